@@ -1,0 +1,142 @@
+/*
+ * nedy.h -- C ABI of the B200-native GF2 Kadanoff-Baym hot path.
+ *
+ * Drop-in boundary for the per-timestep work of tblommel/NEdyson: the
+ * second-Born self-energy (density-fitted, spin-unrestricted and full-U), the
+ * Hartree-Fock mean field, the Dyson time step with its Gregory-weighted history
+ * integrals and Legendre mixed-component convolutions, the polynomial predictor,
+ * the bootstrap and the correlation energy.  Plain C: opaque handles, raw
+ * pointers and sizes; every function returns an nedy_status code and never
+ * throws or exits across the boundary.
+ *
+ * Storage: Green's functions keep the reference's packed layout (reference
+ * src/greens.cpp:34-195), with nao x nao row-major complex128 blocks:
+ *   NEDY_LES  block (i,j), i <= j, at j*(j+1)/2 + i      (column G^<(.,T) contiguous)
+ *   NEDY_RET  block (i,j), j <= i, at i*(i+1)/2 + j      (row G^R(T,.) contiguous)
+ *   NEDY_TV   block (t,m) at t*(ntau+1) + m
+ *   NEDY_MAT  block m
+ * Block indices are 64-bit.  The imaginary-time grid is the ntau+1
+ * Legendre-Gauss-Lobatto nodes tau_m = beta (x_m + 1) / 2 (nedy_collocation_nodes).
+ *
+ * Threading: a context owns one CUDA stream; calls on one context must come from
+ * one host thread at a time (the reference objects are not re-entrant either,
+ * src/dyson.h:26-37).
+ */
+#ifndef NEDY_H
+#define NEDY_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEDY_ABI_VERSION 1
+
+enum nedy_status {
+  NEDY_OK = 0,
+  NEDY_ERR_ARG = 1,      /* bad argument or size (the reference asserts) */
+  NEDY_ERR_CUDA = 2,     /* CUDA runtime error */
+  NEDY_ERR_NOCONV = 3,   /* iteration did not reach its tolerance */
+  NEDY_ERR_TIMEOUT = 4,  /* a bounded device wait gave up */
+  NEDY_ERR_OOM = 5,      /* device allocation failed */
+  NEDY_ERR_STATE = 6,    /* call out of order (e.g. tensor not set) */
+  NEDY_ERR_SINGULAR = 7  /* zero pivot in a Dyson solve */
+};
+
+enum nedy_component { NEDY_LES = 0, NEDY_RET = 1, NEDY_TV = 2, NEDY_MAT = 3 };
+
+typedef struct nedy_ctx nedy_ctx;
+typedef struct nedy_gf nedy_gf;
+typedef struct nedy_buf nedy_buf;
+
+/* Sizes of one simulation: dyson(nt, ntau, nao, k) (reference src/dyson.cpp:25-43),
+ * beta and dt as passed to dyson_step (src/dyson.h:86). */
+typedef struct {
+  int nt, ntau, nao, k;
+  double beta, dt;
+  int device;                 /* CUDA device ordinal */
+  long long workspace_bytes;  /* self-energy chunk budget; 0 = default (4 GiB) */
+} nedy_config;
+
+int nedy_abi_version(void);
+const char *nedy_status_string(int status);
+/* Message of the last failing call on this host thread. */
+const char *nedy_last_error(void);
+
+int nedy_ctx_create(const nedy_config *cfg, nedy_ctx **out);
+int nedy_ctx_destroy(nedy_ctx *ctx);
+int nedy_ctx_synchronize(nedy_ctx *ctx);
+/* Collocation nodes x_m in [-1,1] and weights (ntau+1 values each). */
+int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w);
+
+/* --- Green's functions: green_func(nt, ntau, size1, sig) (src/greens.cpp:34-55) --- */
+int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out);
+int nedy_gf_destroy(nedy_gf *g);
+/* Copy nblocks nao x nao blocks starting at block first_block of a component. */
+int nedy_gf_upload(nedy_gf *g, int component, long long first_block, long long nblocks, const void *host);
+int nedy_gf_download(const nedy_gf *g, int component, long long first_block, long long nblocks, void *host);
+int nedy_gf_device_pointer(const nedy_gf *g, int component, void **dev);
+/* green_func::set_tstp_zero (src/greens.h:76-86) */
+int nedy_gf_set_tstp_zero(nedy_gf *g, int tstp);
+
+/* --- Device buffers (mean-field hmf, density matrices, ...) --- */
+int nedy_buf_create(nedy_ctx *ctx, long long bytes, nedy_buf **out);
+int nedy_buf_destroy(nedy_buf *b);
+int nedy_buf_upload(nedy_buf *b, long long offset, long long bytes, const void *host);
+int nedy_buf_download(const nedy_buf *b, long long offset, long long bytes, void *host);
+int nedy_buf_device_pointer(const nedy_buf *b, void **dev);
+
+/* --- Interaction tensors --- */
+/* Vija: nao x nao x naux row-major real (B^Q_ij).  Replaces the tensors handed to
+ * molGF2SolverDecomp(Vija, Viaj) (src/mol2bSolver.h:103); Viaj is derived. */
+int nedy_set_df_tensor(nedy_ctx *ctx, const double *Vija, int nao, int naux);
+/* U, Uexch: nao^4 row-major real; Uexch(j,l,n,q) = 2 U(j,n,l,q) - U(j,l,n,q).
+ * Replaces molGF2Solver(U, Uexch) (src/mol2bSolver.h:194). */
+int nedy_set_full_tensor(nedy_ctx *ctx, const double *U, const double *Uexch, int nao);
+
+/* --- Self-energy of time row tstp (Sigma is zeroed first, like the reference) --- */
+/* molGF2SolverDecomp::solve(int, GREEN&, GREEN&)          src/mol2bSolver.h:125 */
+int nedy_gf2_decomp_solve(nedy_ctx *ctx, int tstp, nedy_gf *Sigma, const nedy_gf *G);
+/* molGF2SolverSpinDecomp::solve(int, vector<GREEN>&, ...) src/mol2bSolver.h:67 */
+int nedy_gf2_spin_decomp_solve(nedy_ctx *ctx, int tstp, nedy_gf *Sigma_up, nedy_gf *Sigma_dn,
+                               const nedy_gf *G_up, const nedy_gf *G_dn);
+/* molGF2Solver::solve(int, GREEN&, GREEN&)                 src/mol2bSolver.h:204 */
+int nedy_gf2_full_solve(nedy_ctx *ctx, int tstp, nedy_gf *Sigma, const nedy_gf *G);
+
+/* --- Mean field; hmf buffers hold (nt+1) x nao x nao complex blocks --- */
+/* rho = i*sig*G^<(t,t) written at rho_offset (bytes) of a buffer; green_func::get_dm (src/greens.h:68-74) */
+int nedy_get_dm(nedy_ctx *ctx, const nedy_gf *G, int tstp, nedy_buf *rho, long long rho_offset);
+/* molHFSolverDecomp::solve_HF(tstp, hmf, rho)              src/molHFSolver.h:64 */
+int nedy_hf_decomp(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
+/* molHFSolverSpinDecomp::solve_HF; rho2 holds the two spin densities back to back  src/molHFSolver.h:125 */
+int nedy_hf_spin_decomp(nedy_ctx *ctx, int tstp, nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *rho2);
+/* molHFSolver::solve_HF                                    src/molHFSolver.h:31 */
+int nedy_hf_full(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
+
+/* --- Dyson equation --- */
+/* dyson::Extrapolate(int, GREEN&)                          src/dyson.h:114 */
+int nedy_extrapolate(nedy_ctx *ctx, int tstp, nedy_gf *G);
+/* dyson::dyson_step(int, GREEN&, const GREEN&, const cplx*, mu, beta, dt)  src/dyson.h:86.
+ * err3 (optional) receives the ret, tv and les residual norms. */
+int nedy_dyson_step(nedy_ctx *ctx, int tstp, nedy_gf *G, const nedy_gf *Sigma, const nedy_buf *hmf, double mu,
+                    double *err3);
+/* dyson::dyson_start(GREEN&, const GREEN&, const cplx*, mu, beta, dt)   src/dyson.h:58 */
+int nedy_dyson_start(nedy_ctx *ctx, nedy_gf *G, const nedy_gf *Sigma, const nedy_buf *hmf, double mu, double *err);
+/* dyson::energy_conv(int, const GREEN&, const GREEN&, beta, dt)         src/dyson.h:137 */
+int nedy_energy_conv(nedy_ctx *ctx, int tstp, const nedy_gf *Sigma, const nedy_gf *G, double *energy);
+
+/* --- One whole time step of the restricted density-fitted simulation
+ * (DecompSimulation::do_tstp, src/molNEsim_decomp_impl.h:85-104): predictor,
+ * then corr_steps x [rho, hmf(tstp) = h_t + HF(rho), Sigma, dyson_step].
+ * h_t: nao x nao complex one-body Hamiltonian at tstp (h0 plus the drive).
+ * err: residual of the last dyson_step (sum of the three components). */
+int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
+                     double mu, int corr_steps, double *err);
+/* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122). */
+int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
+                          nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
+                          double mu_up, double mu_dn, int corr_steps, double *err);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEDY_H */

@@ -1,0 +1,598 @@
+// C ABI (include/nedy.h): handles, memory, and the public entry points.
+#include "../../include/nedy.h"
+#include "sigma.cuh"
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace nedy;
+
+struct nedy_ctx {
+  Ctx c;
+};
+struct nedy_gf {
+  nedy_ctx *ctx;
+  DevGF g;
+};
+struct nedy_buf {
+  nedy_ctx *ctx;
+  void *p;
+  long long bytes;
+};
+
+namespace nedy {
+
+Arena::~Arena() {
+  for (auto &b : blocks_) cudaFree(b.p);
+}
+size_t Arena::capacity() const {
+  size_t s = 0;
+  for (auto &b : blocks_) s += b.cap;
+  return s;
+}
+void Arena::reset() {
+  if (blocks_.size() > 1) {
+    size_t total = capacity();
+    NEDY_CUDA(cudaDeviceSynchronize());
+    for (auto &b : blocks_) cudaFree(b.p);
+    blocks_.clear();
+    char *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, total);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw CudaError("workspace allocation of " + std::to_string(total) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    blocks_.push_back({p, total, 0});
+  }
+  for (auto &b : blocks_) b.top = 0;
+}
+void *Arena::get(size_t bytes) {
+  size_t need = ((bytes + 255) / 256) * 256;
+  if (need == 0) need = 256;
+  if (!blocks_.empty() && blocks_.back().top + need <= blocks_.back().cap) {
+    Block &b = blocks_.back();
+    void *p = b.p + b.top;
+    b.top += need;
+    return p;
+  }
+  size_t cap = std::max(need, (size_t)64 << 20);
+  char *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, cap);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw CudaError("workspace allocation of " + std::to_string(cap) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  blocks_.push_back({p, cap, need});
+  return p;
+}
+
+Ctx::~Ctx() {
+  auto f = [](void *p) { if (p) cudaFree(p); };
+  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// full-U Hartree-Fock (molHFSolver.cpp:35-56): hmf_ij += sum_kl rho_kl (2 U_ijkl - U_ilkj)
+__global__ void hf_full_kernel(int N, const double *U, const double2 *rho, double2 *h) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= N * N) return;
+  const int i = e / N, j = e - (e / N) * N;
+  double2 acc = czero();
+  for (int k = 0; k < N; k++)
+    for (int l = 0; l < N; l++) {
+      const double u = 2.0 * U[((i64)(i * N + j) * N + k) * N + l] - U[((i64)(i * N + l) * N + k) * N + j];
+      acc = cadd(acc, cscale(rho[k * N + l], u));
+    }
+  h[e] = cadd(h[e], acc);
+}
+void hf_full(Ctx &c, double2 *hmf_T, const double2 *rho) {
+  NEDY_REQUIRE(c.U, "hf_full: U not set");
+  int N = c.u_nao;
+  hf_full_kernel<<<(N * N + 127) / 128, 128, 0, c.stream>>>(N, c.U, rho, hmf_T);
+  NEDY_CHECK_LAUNCH();
+}
+
+} // namespace nedy
+
+namespace {
+thread_local std::string g_err;
+
+template <class F>
+int guard(F &&f) {
+  try {
+    f();
+    return NEDY_OK;
+  } catch (const ArgError &e) {
+    g_err = e.what();
+    if (g_err.find("singular") != std::string::npos) return NEDY_ERR_SINGULAR;
+    return NEDY_ERR_ARG;
+  } catch (const CudaError &e) {
+    g_err = e.what();
+    if (g_err.find("out of memory") != std::string::npos || g_err.find("allocation") != std::string::npos)
+      return NEDY_ERR_OOM;
+    return NEDY_ERR_CUDA;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return NEDY_ERR_STATE;
+  } catch (...) {
+    g_err = "unknown error";
+    return NEDY_ERR_STATE;
+  }
+}
+
+void set_dev(nedy_ctx *ctx) { NEDY_CUDA(cudaSetDevice(ctx->c.device)); }
+
+double2 *comp_ptr(const nedy_gf *g, int comp, i64 &nblocks) {
+  const DevGF &d = g->g;
+  switch (comp) {
+    case NEDY_LES: nblocks = d.nt >= 0 ? d.ntri() : 0; return d.les;
+    case NEDY_RET: nblocks = d.nt >= 0 ? d.ntri() : 0; return d.ret;
+    case NEDY_TV: nblocks = (i64)(d.nt + 1) * (d.ntau + 1); return d.tv;
+    case NEDY_MAT: nblocks = d.ntau + 1; return d.mat;
+  }
+  throw ArgError("unknown component");
+}
+
+double2 *hmf_row(const nedy_buf *b, const nedy_ctx *ctx, int tstp, int nao) {
+  const i64 es = (i64)nao * nao;
+  NEDY_REQUIRE(b && b->bytes >= (i64)(tstp + 1) * es * 16, "hmf buffer too small for tstp");
+  return (double2 *)b->p + (i64)tstp * es;
+}
+} // namespace
+
+extern "C" {
+
+int nedy_abi_version(void) { return NEDY_ABI_VERSION; }
+
+const char *nedy_status_string(int s) {
+  switch (s) {
+    case NEDY_OK: return "ok";
+    case NEDY_ERR_ARG: return "bad argument";
+    case NEDY_ERR_CUDA: return "CUDA error";
+    case NEDY_ERR_NOCONV: return "not converged";
+    case NEDY_ERR_TIMEOUT: return "device wait timed out";
+    case NEDY_ERR_OOM: return "out of device memory";
+    case NEDY_ERR_STATE: return "call out of order";
+    case NEDY_ERR_SINGULAR: return "singular matrix";
+  }
+  return "unknown status";
+}
+
+const char *nedy_last_error(void) { return g_err.c_str(); }
+
+int nedy_ctx_create(const nedy_config *cfg, nedy_ctx **out) {
+  return guard([&] {
+    NEDY_REQUIRE(cfg && out, "null argument");
+    NEDY_REQUIRE(cfg->nt >= cfg->k && cfg->k >= 1 && cfg->ntau >= 2 && cfg->nao >= 1, "bad sizes in nedy_config");
+    NEDY_REQUIRE(cfg->beta > 0 && cfg->dt > 0, "beta and dt must be positive");
+    int ndev = 0;
+    NEDY_CUDA(cudaGetDeviceCount(&ndev));
+    NEDY_REQUIRE(cfg->device >= 0 && cfg->device < ndev, "no such CUDA device");
+    auto *h = new nedy_ctx;
+    Ctx &c = h->c;
+    c.device = cfg->device;
+    c.nt = cfg->nt; c.ntau = cfg->ntau; c.nao = cfg->nao; c.k = cfg->k;
+    c.beta = cfg->beta; c.dt = cfg->dt;
+    if (cfg->workspace_bytes > 0) c.ws_budget = cfg->workspace_bytes;
+    try {
+      NEDY_CUDA(cudaSetDevice(c.device));
+      NEDY_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+      c.W = make_weights(c.k);
+      c.col = make_colloc(c.ntau);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int nedy_ctx_destroy(nedy_ctx *ctx) {
+  return guard([&] {
+    if (!ctx) return;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    delete ctx;
+  });
+}
+
+int nedy_ctx_synchronize(nedy_ctx *ctx) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null context");
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null context");
+    if (x) std::memcpy(x, ctx->c.col.x.data(), sizeof(double) * ctx->c.col.x.size());
+    if (w) std::memcpy(w, ctx->c.col.w.data(), sizeof(double) * ctx->c.col.w.size());
+  });
+}
+
+int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && out, "null argument");
+    NEDY_REQUIRE(nao > 0 && nt >= -1 && ntau >= 0 && sig * sig == 1, "green_func: bad sizes (greens.cpp:35)");
+    set_dev(ctx);
+    auto *g = new nedy_gf;
+    g->ctx = ctx;
+    DevGF &d = g->g;
+    d.nt = nt; d.ntau = ntau; d.nao = nao; d.sig = sig; d.es = (i64)nao * nao;
+    auto alloc = [&](double2 *&p, i64 nblk) {
+      if (nblk <= 0) { p = nullptr; return; }
+      cudaError_t e = cudaMalloc(&p, sizeof(double2) * nblk * d.es);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        throw CudaError(std::string("green_func allocation failed: ") + cudaGetErrorString(e));
+      }
+      NEDY_CUDA(cudaMemset(p, 0, sizeof(double2) * nblk * d.es));
+    };
+    try {
+      alloc(d.mat, ntau + 1);
+      if (nt >= 0) {
+        alloc(d.les, d.ntri());
+        alloc(d.ret, d.ntri());
+        alloc(d.tv, (i64)(nt + 1) * (ntau + 1));
+      }
+    } catch (...) {
+      if (d.mat) cudaFree(d.mat);
+      if (d.les) cudaFree(d.les);
+      if (d.ret) cudaFree(d.ret);
+      if (d.tv) cudaFree(d.tv);
+      delete g;
+      throw;
+    }
+    *out = g;
+  });
+}
+
+int nedy_gf_destroy(nedy_gf *g) {
+  return guard([&] {
+    if (!g) return;
+    set_dev(g->ctx);
+    cudaStreamSynchronize(g->ctx->c.stream);
+    if (g->g.mat) cudaFree(g->g.mat);
+    if (g->g.les) cudaFree(g->g.les);
+    if (g->g.ret) cudaFree(g->g.ret);
+    if (g->g.tv) cudaFree(g->g.tv);
+    delete g;
+  });
+}
+
+int nedy_gf_upload(nedy_gf *g, int comp, long long first, long long nb, const void *host) {
+  return guard([&] {
+    NEDY_REQUIRE(g && host, "null argument");
+    set_dev(g->ctx);
+    i64 tot;
+    double2 *p = comp_ptr(g, comp, tot);
+    NEDY_REQUIRE(first >= 0 && nb >= 0 && first + nb <= tot, "block range out of bounds");
+    NEDY_CUDA(cudaMemcpyAsync(p + first * g->g.es, host, sizeof(double2) * nb * g->g.es, cudaMemcpyHostToDevice,
+                              g->ctx->c.stream));
+    NEDY_CUDA(cudaStreamSynchronize(g->ctx->c.stream));
+    if (comp == NEDY_MAT) g->g.mat_version++;
+  });
+}
+
+int nedy_gf_download(const nedy_gf *g, int comp, long long first, long long nb, void *host) {
+  return guard([&] {
+    NEDY_REQUIRE(g && host, "null argument");
+    set_dev(g->ctx);
+    i64 tot;
+    double2 *p = comp_ptr(g, comp, tot);
+    NEDY_REQUIRE(first >= 0 && nb >= 0 && first + nb <= tot, "block range out of bounds");
+    NEDY_CUDA(cudaMemcpyAsync(host, p + first * g->g.es, sizeof(double2) * nb * g->g.es, cudaMemcpyDeviceToHost,
+                              g->ctx->c.stream));
+    NEDY_CUDA(cudaStreamSynchronize(g->ctx->c.stream));
+  });
+}
+
+int nedy_gf_device_pointer(const nedy_gf *g, int comp, void **dev) {
+  return guard([&] {
+    NEDY_REQUIRE(g && dev, "null argument");
+    i64 tot;
+    *dev = comp_ptr(g, comp, tot);
+  });
+}
+
+int nedy_gf_set_tstp_zero(nedy_gf *g, int tstp) {
+  return guard([&] {
+    NEDY_REQUIRE(g, "null argument");
+    const DevGF &d = g->g;
+    NEDY_REQUIRE(tstp >= -1 && tstp <= d.nt, "tstp out of range");
+    set_dev(g->ctx);
+    cudaStream_t s = g->ctx->c.stream;
+    if (tstp == -1) {
+      NEDY_CUDA(cudaMemsetAsync(d.mat, 0, sizeof(double2) * (d.ntau + 1) * d.es, s));
+      g->g.mat_version++;
+    } else {
+      NEDY_CUDA(cudaMemsetAsync(d.retptr(tstp, 0), 0, sizeof(double2) * (tstp + 1) * d.es, s));
+      NEDY_CUDA(cudaMemsetAsync(d.lesptr(0, tstp), 0, sizeof(double2) * (tstp + 1) * d.es, s));
+      NEDY_CUDA(cudaMemsetAsync(d.tvptr(tstp, 0), 0, sizeof(double2) * (d.ntau + 1) * d.es, s));
+    }
+  });
+}
+
+int nedy_buf_create(nedy_ctx *ctx, long long bytes, nedy_buf **out) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && out && bytes > 0, "bad argument");
+    set_dev(ctx);
+    auto *b = new nedy_buf;
+    b->ctx = ctx;
+    b->bytes = bytes;
+    cudaError_t e = cudaMalloc(&b->p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      delete b;
+      throw CudaError(std::string("buffer allocation failed: ") + cudaGetErrorString(e));
+    }
+    NEDY_CUDA(cudaMemset(b->p, 0, bytes));
+    *out = b;
+  });
+}
+
+int nedy_buf_destroy(nedy_buf *b) {
+  return guard([&] {
+    if (!b) return;
+    set_dev(b->ctx);
+    cudaStreamSynchronize(b->ctx->c.stream);
+    cudaFree(b->p);
+    delete b;
+  });
+}
+
+int nedy_buf_upload(nedy_buf *b, long long off, long long bytes, const void *host) {
+  return guard([&] {
+    NEDY_REQUIRE(b && host && off >= 0 && bytes >= 0 && off + bytes <= b->bytes, "buffer range out of bounds");
+    set_dev(b->ctx);
+    NEDY_CUDA(cudaMemcpyAsync((char *)b->p + off, host, bytes, cudaMemcpyHostToDevice, b->ctx->c.stream));
+    NEDY_CUDA(cudaStreamSynchronize(b->ctx->c.stream));
+  });
+}
+
+int nedy_buf_download(const nedy_buf *b, long long off, long long bytes, void *host) {
+  return guard([&] {
+    NEDY_REQUIRE(b && host && off >= 0 && bytes >= 0 && off + bytes <= b->bytes, "buffer range out of bounds");
+    set_dev(b->ctx);
+    NEDY_CUDA(cudaMemcpyAsync(host, (char *)b->p + off, bytes, cudaMemcpyDeviceToHost, b->ctx->c.stream));
+    NEDY_CUDA(cudaStreamSynchronize(b->ctx->c.stream));
+  });
+}
+
+int nedy_buf_device_pointer(const nedy_buf *b, void **dev) {
+  return guard([&] {
+    NEDY_REQUIRE(b && dev, "null argument");
+    *dev = b->p;
+  });
+}
+
+int nedy_set_df_tensor(nedy_ctx *ctx, const double *Vija, int nao, int naux) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && Vija && nao > 0 && naux > 0, "bad argument");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    const size_t n = (size_t)nao * nao * naux;
+    std::vector<double> viaj(n), vaij(n), vmbq(n);
+    for (int i = 0; i < nao; i++)
+      for (int j = 0; j < nao; j++)
+        for (int a = 0; a < naux; a++) {
+          const double v = Vija[((size_t)i * nao + j) * naux + a];
+          viaj[((size_t)i * naux + a) * nao + j] = v;   // Viaj(i,a,j) = Vija(i,j,a)
+          vaij[((size_t)a * nao + i) * nao + j] = v;    // Vaij(a,i,j)
+          vmbq[((size_t)j * naux + a) * nao + i] = v;   // Vmbq(m=j, b=a, q=i) = V^b_qm
+        }
+    auto put = [&](double *&d, const double *h) {
+      if (d) cudaFree(d);
+      NEDY_CUDA(cudaMalloc(&d, sizeof(double) * n));
+      NEDY_CUDA(cudaMemcpy(d, h, sizeof(double) * n, cudaMemcpyHostToDevice));
+    };
+    put(c.Vija, Vija);
+    put(c.Viaj, viaj.data());
+    put(c.Vaij, vaij.data());
+    put(c.Vmbq, vmbq.data());
+    c.df_nao = nao;
+    c.df_naux = naux;
+  });
+}
+
+int nedy_set_full_tensor(nedy_ctx *ctx, const double *U, const double *Uexch, int nao) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && U && Uexch && nao > 0, "bad argument");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    const size_t n = (size_t)nao * nao * nao * nao;
+    if (c.U) cudaFree(c.U);
+    if (c.Uexch) cudaFree(c.Uexch);
+    NEDY_CUDA(cudaMalloc(&c.U, sizeof(double) * n));
+    NEDY_CUDA(cudaMalloc(&c.Uexch, sizeof(double) * n));
+    NEDY_CUDA(cudaMemcpy(c.U, U, sizeof(double) * n, cudaMemcpyHostToDevice));
+    NEDY_CUDA(cudaMemcpy(c.Uexch, Uexch, sizeof(double) * n, cudaMemcpyHostToDevice));
+    c.u_nao = nao;
+  });
+}
+
+int nedy_gf2_decomp_solve(nedy_ctx *ctx, int tstp, nedy_gf *Sigma, const nedy_gf *G) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && Sigma && G, "null argument");
+    set_dev(ctx);
+    DevGF *S[1] = {&Sigma->g};
+    const DevGF *Gs[1] = {&G->g};
+    sigma_df(ctx->c, tstp, 1, S, Gs);
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int nedy_gf2_spin_decomp_solve(nedy_ctx *ctx, int tstp, nedy_gf *Su, nedy_gf *Sd, const nedy_gf *Gu,
+                               const nedy_gf *Gd) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && Su && Sd && Gu && Gd, "null argument");
+    set_dev(ctx);
+    DevGF *S[2] = {&Su->g, &Sd->g};
+    const DevGF *Gs[2] = {&Gu->g, &Gd->g};
+    sigma_df(ctx->c, tstp, 2, S, Gs);
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int nedy_gf2_full_solve(nedy_ctx *ctx, int tstp, nedy_gf *Sigma, const nedy_gf *G) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && Sigma && G, "null argument");
+    set_dev(ctx);
+    sigma_full(ctx->c, tstp, Sigma->g, G->g);
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int nedy_get_dm(nedy_ctx *ctx, const nedy_gf *G, int tstp, nedy_buf *rho, long long off) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G && rho, "null argument");
+    NEDY_REQUIRE(tstp >= 0 && tstp <= G->g.nt, "tstp out of range");
+    const i64 es = G->g.es;
+    NEDY_REQUIRE(off >= 0 && off % 16 == 0 && off + es * 16 <= rho->bytes, "rho buffer too small");
+    set_dev(ctx);
+    get_dm(ctx->c, G->g, tstp, (double2 *)((char *)rho->p + off));
+  });
+}
+
+int nedy_hf_decomp(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && hmf && rho, "null argument");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    c.ws.reset();
+    double2 *h[1] = {hmf_row(hmf, ctx, tstp, c.df_nao)};
+    NEDY_REQUIRE(rho->bytes >= (i64)c.df_nao * c.df_nao * 16, "rho buffer too small");
+    hf_decomp(c, 1, h, (const double2 *)rho->p);
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int nedy_hf_spin_decomp(nedy_ctx *ctx, int tstp, nedy_buf *hu, nedy_buf *hd, const nedy_buf *rho2) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && hu && hd && rho2, "null argument");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    c.ws.reset();
+    double2 *h[2] = {hmf_row(hu, ctx, tstp, c.df_nao), hmf_row(hd, ctx, tstp, c.df_nao)};
+    NEDY_REQUIRE(rho2->bytes >= 2LL * c.df_nao * c.df_nao * 16, "rho buffer too small");
+    hf_decomp(c, 2, h, (const double2 *)rho2->p);
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int nedy_hf_full(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && hmf && rho, "null argument");
+    set_dev(ctx);
+    hf_full(ctx->c, hmf_row(hmf, ctx, tstp, ctx->c.u_nao), (const double2 *)rho->p);
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int nedy_extrapolate(nedy_ctx *ctx, int tstp, nedy_gf *G) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G, "null argument");
+    set_dev(ctx);
+    extrapolate(ctx->c, tstp, G->g);
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+  });
+}
+
+int nedy_dyson_step(nedy_ctx *ctx, int tstp, nedy_gf *G, const nedy_gf *Sigma, const nedy_buf *hmf, double mu,
+                    double *err3) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G && Sigma && hmf, "null argument");
+    set_dev(ctx);
+    hmf_row(hmf, ctx, G->g.nt, G->g.nao);
+    double e[3];
+    dyson_step(ctx->c, tstp, G->g, Sigma->g, (const double2 *)hmf->p, mu, e);
+    NEDY_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    if (err3) { err3[0] = e[0]; err3[1] = e[1]; err3[2] = e[2]; }
+  });
+}
+
+int nedy_dyson_start(nedy_ctx *ctx, nedy_gf *G, const nedy_gf *Sigma, const nedy_buf *hmf, double mu, double *err) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G && Sigma && hmf, "null argument");
+    set_dev(ctx);
+    hmf_row(hmf, ctx, ctx->c.k, G->g.nao);
+    double e = dyson_start(ctx->c, G->g, Sigma->g, (const double2 *)hmf->p, mu);
+    if (err) *err = e;
+  });
+}
+
+int nedy_energy_conv(nedy_ctx *ctx, int tstp, const nedy_gf *Sigma, const nedy_gf *G, double *energy) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && Sigma && G && energy, "null argument");
+    set_dev(ctx);
+    *energy = energy_conv(ctx->c, tstp, Sigma->g, G->g);
+  });
+}
+
+int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const nedy_buf *h_t,
+                     double mu, int corr_steps, double *err) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G && S && hmf && h_t, "null argument");
+    NEDY_REQUIRE(corr_steps >= 1, "corr_steps must be >= 1");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    const int N = G->g.nao;
+    const i64 es = (i64)N * N;
+    NEDY_REQUIRE(h_t->bytes >= es * 16, "h_t buffer too small");
+    double2 *hT = hmf_row(hmf, ctx, tstp, N);
+    hmf_row(hmf, ctx, G->g.nt, N);
+    extrapolate(c, tstp, G->g);
+    double e[3] = {0, 0, 0};
+    for (int it = 0; it < corr_steps; it++) {
+      c.ws.reset();
+      double2 *rho = c.ws.alloc<double2>(es);
+      get_dm(c, G->g, tstp, rho);
+      NEDY_CUDA(cudaMemcpyAsync(hT, h_t->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      double2 *h[1] = {hT};
+      hf_decomp(c, 1, h, rho);
+      DevGF *Ss[1] = {&S->g};
+      const DevGF *Gs[1] = {&G->g};
+      sigma_df(c, tstp, 1, Ss, Gs);
+      dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
+    }
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    if (err) *err = e[0] + e[1] + e[2];
+  });
+}
+
+int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *Gu, nedy_gf *Gd, nedy_gf *Su, nedy_gf *Sd,
+                          nedy_buf *hu, nedy_buf *hd, const nedy_buf *htu, const nedy_buf *htd, double mu_up,
+                          double mu_dn, int corr_steps, double *err) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && Gu && Gd && Su && Sd && hu && hd && htu && htd, "null argument");
+    NEDY_REQUIRE(corr_steps >= 1, "corr_steps must be >= 1");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    const int N = Gu->g.nao;
+    const i64 es = (i64)N * N;
+    double2 *hT[2] = {hmf_row(hu, ctx, tstp, N), hmf_row(hd, ctx, tstp, N)};
+    extrapolate(c, tstp, Gu->g);
+    extrapolate(c, tstp, Gd->g);
+    double eu[3] = {0, 0, 0}, ed[3] = {0, 0, 0};
+    for (int it = 0; it < corr_steps; it++) {
+      c.ws.reset();
+      double2 *rho = c.ws.alloc<double2>(2 * es);
+      get_dm(c, Gu->g, tstp, rho);
+      get_dm(c, Gd->g, tstp, rho + es);
+      NEDY_CUDA(cudaMemcpyAsync(hT[0], htu->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      NEDY_CUDA(cudaMemcpyAsync(hT[1], htd->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      hf_decomp(c, 2, hT, rho);
+      DevGF *Ss[2] = {&Su->g, &Sd->g};
+      const DevGF *Gs[2] = {&Gu->g, &Gd->g};
+      sigma_df(c, tstp, 2, Ss, Gs);
+      dyson_step(c, tstp, Gu->g, Su->g, (const double2 *)hu->p, mu_up, eu);
+      dyson_step(c, tstp, Gd->g, Sd->g, (const double2 *)hd->p, mu_dn, ed);
+    }
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    if (err) *err = eu[0] + eu[1] + eu[2] + ed[0] + ed[1] + ed[2];
+  });
+}
+
+} // extern "C"

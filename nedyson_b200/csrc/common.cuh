@@ -1,0 +1,51 @@
+// Shared device/host helpers of the B200 GF2 engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <stdexcept>
+
+namespace nedy {
+
+using i64 = long long;
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string &m) : std::runtime_error(m) {}
+};
+struct ArgError : std::runtime_error {
+  explicit ArgError(const std::string &m) : std::runtime_error(m) {}
+};
+
+#define NEDY_CUDA(call)                                                                        \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      throw ::nedy::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " @ " +     \
+                              __FILE__ + ":" + std::to_string(__LINE__));                      \
+  } while (0)
+
+#define NEDY_CHECK_LAUNCH() NEDY_CUDA(cudaGetLastError())
+
+#define NEDY_REQUIRE(cond, msg)                                                                \
+  do {                                                                                         \
+    if (!(cond)) throw ::nedy::ArgError(std::string(msg));                                     \
+  } while (0)
+
+// complex helpers on double2 (x = re, y = im)
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
+
+// packed-triangle indices of the reference storage (greens.cpp:177-185)
+__host__ __device__ __forceinline__ i64 les_idx(i64 i, i64 j) { return j * (j + 1) / 2 + i; }  // i <= j
+__host__ __device__ __forceinline__ i64 ret_idx(i64 i, i64 j) { return i * (i + 1) / 2 + j; }  // j <= i
+
+inline unsigned cdiv(i64 a, i64 b) { return (unsigned)((a + b - 1) / b); }
+
+} // namespace nedy

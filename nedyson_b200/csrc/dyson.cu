@@ -1,0 +1,934 @@
+// Dyson time step, its history integrals, the predictor, the bootstrap, the HF
+// mean field and the energy -- device side.
+//
+//   dyson_step_ret : reference src/dyson_step.h:7-127
+//   dyson_step_tv  : reference src/dyson_step.h:130-169 (+ Ctv_tstp / CTV1, dyson_integrals.h:80-116, 254-324)
+//   dyson_step_les : reference src/dyson_step.h:171-326 (+ Cles2 / Cles3, dyson_integrals.h:336-461)
+//   Extrapolate    : reference src/dyson.cpp:47-117
+//   dyson_start    : reference src/dyson_boot.h:6-230
+//   energy_conv    : reference src/dyson_integrals.h:24-70
+//   HF             : reference src/molHFSolver.cpp:81-110, 203-239, 35-56
+//
+// Layout: every history sum is one (grouped) FP64 GEMM over packed blocks.  The
+// sequential Volterra sweeps use the cached inverses of the time-local matrices
+// M(t') = (i bd0/dt + mu) - hmf(t') - dt*w0*Sig^R(t',t'): for t' < T they no longer
+// change, so each step is a single block product instead of an LU solve.
+#include "sigma.cuh"
+#include <cmath>
+#include <algorithm>
+
+namespace nedy {
+namespace {
+
+constexpr int TPB = 256;
+
+inline unsigned nblk(i64 n, int tpb = TPB) { return (unsigned)std::min<i64>((n + tpb - 1) / tpb, 65535LL * 16); }
+
+#define GRID_STRIDE(i, n) for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < (n); i += (i64)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------------------------
+// Gauss-Jordan with partial pivoting, one CTA per system, in global memory.
+// A: n x n (destroyed), B: n x nrhs (overwritten by X = A^-1 B).  status[b] = 1 on a zero pivot.
+__global__ void gj_kernel(int n, int nrhs, double2 *A, i64 sA, double2 *B, i64 sB, int *status) {
+  double2 *a = A + blockIdx.x * sA;
+  double2 *b = B + blockIdx.x * sB;
+  __shared__ double sval[TPB];
+  __shared__ int sidx[TPB];
+  __shared__ double2 fac[1024];
+  const int tid = threadIdx.x;
+  for (int c = 0; c < n; c++) {
+    // pivot search
+    double best = -1.0;
+    int bi = c;
+    for (int r = c + tid; r < n; r += blockDim.x) {
+      double v = hypot(a[(i64)r * n + c].x, a[(i64)r * n + c].y);
+      if (v > best) { best = v; bi = r; }
+    }
+    sval[tid] = best;
+    sidx[tid] = bi;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (tid < s && sval[tid + s] > sval[tid]) { sval[tid] = sval[tid + s]; sidx[tid] = sidx[tid + s]; }
+      __syncthreads();
+    }
+    const int p = sidx[0];
+    if (sval[0] == 0.0) {
+      if (tid == 0 && status) status[blockIdx.x] = 1;
+      return;
+    }
+    if (p != c) {
+      for (int j = tid; j < n; j += blockDim.x) {
+        double2 t = a[(i64)c * n + j]; a[(i64)c * n + j] = a[(i64)p * n + j]; a[(i64)p * n + j] = t;
+      }
+      for (int j = tid; j < nrhs; j += blockDim.x) {
+        double2 t = b[(i64)c * nrhs + j]; b[(i64)c * nrhs + j] = b[(i64)p * nrhs + j]; b[(i64)p * nrhs + j] = t;
+      }
+    }
+    __syncthreads();
+    const double2 piv = a[(i64)c * n + c];
+    const double dd = piv.x * piv.x + piv.y * piv.y;
+    const double2 inv = make_double2(piv.x / dd, -piv.y / dd);
+    __syncthreads();
+    for (int j = tid; j < n; j += blockDim.x) a[(i64)c * n + j] = cmul(a[(i64)c * n + j], inv);
+    for (int j = tid; j < nrhs; j += blockDim.x) b[(i64)c * nrhs + j] = cmul(b[(i64)c * nrhs + j], inv);
+    __syncthreads();
+    // elimination factors (column c of the other rows), processed in slabs of 1024 rows
+    for (int r0 = 0; r0 < n; r0 += 1024) {
+      const int rn = min(1024, n - r0);
+      for (int r = tid; r < rn; r += blockDim.x) fac[r] = (r0 + r == c) ? czero() : a[(i64)(r0 + r) * n + c];
+      __syncthreads();
+      const int w = n + nrhs;
+      for (i64 idx = tid; idx < (i64)rn * w; idx += blockDim.x) {
+        const int r = (int)(idx / w), j = (int)(idx - (i64)r * w);
+        const double2 f = fac[r];
+        if (f.x == 0.0 && f.y == 0.0) continue;
+        if (j < n) {
+          if (j == c) continue;
+          a[(i64)(r0 + r) * n + j] = csub(a[(i64)(r0 + r) * n + j], cmul(f, a[(i64)c * n + j]));
+        } else {
+          const int jj = j - n;
+          b[(i64)(r0 + r) * nrhs + jj] = csub(b[(i64)(r0 + r) * nrhs + jj], cmul(f, b[(i64)c * nrhs + jj]));
+        }
+      }
+      __syncthreads();
+      for (int r = tid; r < rn; r += blockDim.x)
+        if (r0 + r != c) a[(i64)(r0 + r) * n + c] = czero();
+      __syncthreads();
+    }
+  }
+}
+
+void gj(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB) {
+  int *st = c.ws.alloc<int>(nb);
+  NEDY_CUDA(cudaMemsetAsync(st, 0, sizeof(int) * nb, c.stream));
+  gj_kernel<<<nb, TPB, 0, c.stream>>>(n, nrhs, A, sA, B, sB, st);
+  NEDY_CHECK_LAUNCH();
+  c.pending_status.push_back({st, nb});
+}
+
+// ---------------------------------------------------------------------------------
+// M(t') = (i bd0/dt + mu) I - hmf(t') - dt w0 Sig^R(t',t')  for t' = t0 + b; B = I
+__global__ void build_M_kernel(int N, int nb, int t0, const double2 *hmf, DevGF S, double bd0, double mu, double dt,
+                               double w0, double2 *Mout, double2 *Iout) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * nb) {
+    const int b = (int)(idx / es), e = (int)(idx - (i64)b * es);
+    const int i = e / N, j = e - (e / N) * N;
+    const int t = t0 + b;
+    const double2 h = hmf[(i64)t * es + e];
+    const double2 s = S.retptr(t, t)[e];
+    double2 m = make_double2(-h.x - dt * w0 * s.x, -h.y - dt * w0 * s.y);
+    if (i == j) { m.x += mu; m.y += bd0 / dt; }
+    Mout[idx] = m;
+    Iout[idx] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Retarded start block (dyson_step.h:26-71): M (kN x kN) and Q (kN x N)
+__global__ void ret_start_kernel(int N, int k, int T, DevGF G, DevGF S, const double2 *hmf, const double *pdiff,
+                                 const double *greg, int greg_ld, double mu, double dt, double2 *M, double2 *Q) {
+  const i64 es = (i64)N * N;
+  const int kn = k * N;
+  // M: element (r, c) with r = (n-1)*N + i, c = (l-1)*N + j for n, l in 1..k
+  GRID_STRIDE(idx, (i64)kn * kn + (i64)kn * N) {
+    if (idx < (i64)kn * kn) {
+      const int r = (int)(idx / kn), cc = (int)(idx - (i64)r * kn);
+      const int n = r / N + 1, i = r % N, l = cc / N + 1, j = cc % N;
+      // derivative: -(-i/dt) pdiff(n,l) I  = +(i/dt) pdiff
+      double2 m = make_double2(0.0, 0.0);
+      if (i == j) m.y += pdiff[n * (k + 1) + l] / dt;
+      if (l == n) {
+        const double2 h = hmf[(i64)(T - n) * es + (i64)j * N + i];  // hmf^T
+        m.x -= h.x; m.y -= h.y;
+        if (i == j) m.x += mu;
+      }
+      const double w = dt * greg[n * greg_ld + l];
+      if (T - l >= T - n) {  // l <= n: -dt w Sig^R(T-l, T-n)^T
+        const double2 s = S.retptr(T - l, T - n)[(i64)j * N + i];
+        m.x -= w * s.x; m.y -= w * s.y;
+      } else {  // +dt w conj(Sig^R(T-n, T-l))
+        const double2 s = S.retptr(T - n, T - l)[(i64)i * N + j];
+        m.x += w * s.x; m.y -= w * s.y;
+      }
+      M[idx] = m;
+    } else {
+      const i64 q = idx - (i64)kn * kn;
+      const int r = (int)(q / N), j = (int)(q - (i64)r * N);
+      const int n = r / N + 1, i = r % N;
+      // Q_n = (-i/dt) pdiff(n,0) G^R(T,T)^T + dt w(n,0) (G^R(T,T) Sig^R(T,T-n))^T
+      const double2 *g = G.retptr(T, T);
+      double2 v = make_double2(0.0, 0.0);
+      const double2 gt = g[(i64)j * N + i];
+      const double pd = pdiff[n * (k + 1)] / dt;
+      v.x += pd * gt.y;  // (-i) * gt * pd
+      v.y -= pd * gt.x;
+      double2 acc = czero();  // (G S)^T[i][j] = (G S)[j][i] = sum_c G[j][c] S[c][i]
+      const double2 *s = S.retptr(T, T - n);
+      for (int c2 = 0; c2 < N; c2++) acc = cadd(acc, cmul(g[(i64)j * N + c2], s[(i64)c2 * N + i]));
+      const double w = dt * greg[n * greg_ld];
+      v.x += w * acc.x; v.y += w * acc.y;
+      Q[q] = v;
+    }
+  }
+}
+
+// G^R(T, T-l-1) = X_l^T for l < k, and the error norm contribution
+__global__ void ret_start_store(int N, int k, int T, DevGF G, const double2 *X, double *err) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * k) {
+    const int l = (int)(idx / es), e = (int)(idx - (i64)l * es);
+    const int i = e / N, j = e - (e / N) * N;
+    double2 *dst = G.retptr(T, T - l - 1) + e;
+    const double2 v = X[(i64)l * es + (i64)j * N + i];
+    const double2 d = csub(*dst, v);
+    atomicAdd(&err[l], d.x * d.x + d.y * d.y);
+    *dst = v;
+  }
+}
+
+// One retarded Volterra step (dyson_step.h:88-106): Qh = dt Q_n + sum_l bd(l)(-i/dt) G^R(T,T-n+l);
+// G^R(T,T-n) = Qh * Minv(T-n).  One CTA per output row.
+__global__ void ret_step_kernel(int N, int k, int T, int n, DevGF G, const double2 *Q, const double2 *Minv,
+                                const double *bd, double dt, double *err) {
+  extern __shared__ double2 row[];
+  const i64 es = (i64)N * N;
+  const int i = blockIdx.x;
+  for (int c = threadIdx.x; c < N; c += blockDim.x) {
+    double2 v = cscale(Q[(i64)n * es + (i64)i * N + c], dt);
+    for (int l = 1; l <= k + 1; l++) {
+      const double2 g = G.retptr(T, T - n + l)[(i64)i * N + c];
+      const double f = bd[l] / dt;
+      v.x += f * g.y;  // (-i) f g
+      v.y -= f * g.x;
+    }
+    row[c] = v;
+  }
+  __syncthreads();
+  const double2 *Mi = Minv + (i64)(T - n) * es;
+  for (int j = threadIdx.x; j < N; j += blockDim.x) {
+    double2 acc = czero();
+    for (int c = 0; c < N; c++) acc = cadd(acc, cmul(row[c], Mi[(i64)c * N + j]));
+    double2 *dst = G.retptr(T, T - n) + (i64)i * N + j;
+    const double2 d = csub(*dst, acc);
+    atomicAdd(&err[n], d.x * d.x + d.y * d.y);
+    *dst = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// tv: derivative history terms  out += -(i/dt) bd(l) G^tv(T-l, .)
+__global__ void tv_bd_kernel(i64 n, int k, int T, DevGF G, const double *bd, double dt, double2 *out) {
+  GRID_STRIDE(idx, n) {
+    double2 v = out[idx];
+    for (int l = 1; l <= k + 1; l++) {
+      const double2 g = G.tvptr(T - l, 0)[idx];
+      const double f = bd[l] / dt;
+      v.x += f * g.y;
+      v.y -= f * g.x;
+    }
+    out[idx] = v;
+  }
+}
+
+// per-block squared difference norms: err[b] = ||A_b - B_b||^2 (accumulated)
+__global__ void diffnorm_kernel(int N, int nb, const double2 *A, const double2 *B, double *err) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * nb) {
+    const int b = (int)(idx / es);
+    const double2 d = csub(A[idx], B[idx]);
+    atomicAdd(&err[b], d.x * d.x + d.y * d.y);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// les helpers
+// G^<(0,n) = -G^tv(n,0)^+ ; err
+__global__ void les_init_kernel(int N, int n, DevGF G, double2 *X0, double *err) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(e, es) {
+    const int i = (int)(e / N), j = (int)(e - (e / N) * N);
+    const double2 t = G.tvptr(n, 0)[(i64)j * N + i];
+    const double2 v = make_double2(-t.x, t.y);
+    double2 *dst = G.lesptr(0, n) + e;
+    const double2 d = csub(*dst, v);
+    atomicAdd(err, d.x * d.x + d.y * d.y);
+    *dst = v;
+    X0[e] = v;
+  }
+}
+
+// NTT_j = sig * i * G^tv(n, ntau-j)^+   (dyson_integrals.h:424-425) ; UB = sum_j u_j NTT_j
+__global__ void ntt_kernel(int N, int ntau, int n, DevGF G, int sig, double2 *ntt) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * (ntau + 1)) {
+    const int j = (int)(idx / es), e = (int)(idx - (i64)j * es);
+    const int a = e / N, b = e - (e / N) * N;
+    const double2 g = G.tvptr(n, ntau - j)[(i64)b * N + a];  // conj transpose
+    // sig * i * conj(g)
+    ntt[idx] = make_double2(sig * g.y, sig * g.x);
+  }
+}
+// B''_j = (beta/2) (w_j NTT_j + ctop u_j UB),  UB = sum_i u_i NTT_i (one CTA per element column chunk)
+__global__ void lesser_weights_kernel(int N, int ntau, const double2 *ntt, const double *w, const double *u,
+                                      double ctop, double beta, double2 *out) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(e, es) {
+    double2 ub = czero();
+    for (int i = 0; i <= ntau; i++) ub = cadd(ub, cscale(ntt[(i64)i * es + e], u[i]));
+    for (int j = 0; j <= ntau; j++) {
+      double2 v = cadd(cscale(ntt[(i64)j * es + e], w[j]), cscale(ub, ctop * u[j]));
+      out[(i64)j * es + e] = cscale(v, 0.5 * beta);
+    }
+  }
+}
+// X_j = dt w(n,j) G^R(n,j)^+  (dyson_integrals.h:355-362, m = n >= j)
+__global__ void cles2_x_kernel(int N, int n, DevGF G, const double *gregrow, double dt, double2 *X) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * (n + 1)) {
+    const int j = (int)(idx / es), e = (int)(idx - (i64)j * es);
+    const int a = e / N, b = e - (e / N) * N;
+    const double2 g = G.retptr(n, j)[(i64)b * N + a];
+    const double f = dt * gregrow[j];
+    X[idx] = make_double2(f * g.x, -f * g.y);
+  }
+}
+
+// Lesser start block (dyson_step.h:217-252): M (kN x kN); Q_m (m=1..k) gets the G^<(0,n) terms.
+__global__ void les_start_kernel(int N, int k, int n, DevGF G, DevGF S, const double2 *hmf, const double *pdiff,
+                                 const double *greg, int greg_ld, double mu, double dt, const double2 *Qmain,
+                                 double2 *M, double2 *Q) {
+  const i64 es = (i64)N * N;
+  const int kn = k * N;
+  GRID_STRIDE(idx, (i64)kn * kn + (i64)kn * N) {
+    if (idx < (i64)kn * kn) {
+      const int r = (int)(idx / kn), cc = (int)(idx - (i64)r * kn);
+      const int m = r / N + 1, i = r % N, l = cc / N + 1, j = cc % N;
+      double2 v = czero();
+      if (i == j) v.y += pdiff[m * (k + 1) + l] / dt;  // (i/dt) pdiff
+      if (m == l) {
+        const double2 h = hmf[(i64)l * es + (i64)i * N + j];
+        v.x -= h.x; v.y -= h.y;
+        if (i == j) v.x += mu;
+      }
+      const double w = dt * greg[m * greg_ld + l];
+      if (m >= l) {
+        const double2 s = S.retptr(m, l)[(i64)i * N + j];
+        v.x -= w * s.x; v.y -= w * s.y;
+      } else {
+        const double2 s = S.retptr(l, m)[(i64)j * N + i];  // adjoint
+        v.x += w * s.x; v.y -= w * s.y;
+      }
+      M[idx] = v;
+    } else {
+      const i64 q = idx - (i64)kn * kn;
+      const int r = (int)(q / N), j = (int)(q - (i64)r * N);
+      const int m = r / N + 1, i = r % N;
+      // Q_m -= (i/dt) pdiff(m,0) G^<(0,n) ; Q_m += dt w(m,0) Sig^R(m,0) G^<(0,n)
+      const double2 *g0 = G.lesptr(0, n);
+      double2 v = Qmain[(i64)m * es + (i64)i * N + j];
+      const double pd = pdiff[m * (k + 1)] / dt;
+      const double2 gij = g0[(i64)i * N + j];
+      v.x += pd * gij.y;  // -(i pd) g
+      v.y -= pd * gij.x;
+      double2 acc = czero();
+      const double2 *s = S.retptr(m, 0);
+      for (int c2 = 0; c2 < N; c2++) acc = cadd(acc, cmul(s[(i64)i * N + c2], g0[(i64)c2 * N + j]));
+      const double w = dt * greg[m * greg_ld];
+      v.x += w * acc.x; v.y += w * acc.y;
+      Q[q] = v;  // packed (kN x N) right-hand side for rows m = 1..k
+    }
+  }
+}
+
+// One lesser Volterra step (dyson_step.h:257-280): Qh = Q_m - sum_l (i/dt) bd(l) X_{m-l}; X_m = Minv(m) Qh
+__global__ void les_step_kernel(int N, int k, int m, const double2 *Q, double2 *X, const double2 *Minv,
+                                const double *bd, double dt) {
+  extern __shared__ double2 col[];
+  const i64 es = (i64)N * N;
+  const int j = blockIdx.x;  // output column
+  for (int c = threadIdx.x; c < N; c += blockDim.x) {
+    double2 v = Q[(i64)m * es + (i64)c * N + j];
+    for (int l = 1; l <= k + 1; l++) {
+      const double2 x = X[(i64)(m - l) * es + (i64)c * N + j];
+      const double f = bd[l] / dt;
+      v.x += f * x.y;  // -(i f) x
+      v.y -= f * x.x;
+    }
+    col[c] = v;
+  }
+  __syncthreads();
+  const double2 *Mi = Minv + (i64)m * es;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double2 acc = czero();
+    for (int c = 0; c < N; c++) acc = cadd(acc, cmul(Mi[(i64)i * N + c], col[c]));
+    X[(i64)m * es + (i64)i * N + j] = acc;
+  }
+}
+
+// Diagonal G^<(n,n) (dyson_step.h:284-310), one CTA.
+__global__ void les_diag_kernel(int N, int k, int n, DevGF G, DevGF S, const double2 *hmf, const double *ex,
+                                const double *bd, double wnn, double mu, double dt, const double2 *Q, double2 *X) {
+  extern __shared__ double2 sm[];
+  const i64 es = (i64)N * N;
+  double2 *xn = sm, *qn = sm + es;
+  for (int e = threadIdx.x; e < es; e += blockDim.x) {
+    double2 v = czero();
+    for (int jj = 0; jj <= k; jj++) v = cadd(v, cscale(G.lesptr(n - jj - 1, n - jj - 1)[e], ex[jj]));
+    xn[e] = v;
+  }
+  __syncthreads();
+  const double2 *sr = S.retptr(n, n);
+  const double2 *h = hmf + (i64)n * es;
+  for (int e = threadIdx.x; e < es; e += blockDim.x) {
+    const int i = e / N, j = e - (e / N) * N;
+    double2 acc = Q[(i64)n * es + e];
+    double2 a1 = czero(), a2 = czero();
+    for (int c = 0; c < N; c++) {
+      a1 = cadd(a1, cmul(sr[(i64)i * N + c], xn[(i64)c * N + j]));
+      double2 hm = h[(i64)i * N + c];
+      if (c == i) hm.x -= mu;
+      a2 = cadd(a2, cmul(hm, xn[(i64)c * N + j]));
+    }
+    acc = cadd(acc, cadd(cscale(a1, dt * wnn), a2));
+    qn[e] = acc;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < es; e += blockDim.x) {
+    const int i = e / N, j = e - (e / N) * N;
+    const double2 a = qn[e], b = qn[(i64)j * N + i];
+    // -i (Q + Q^+)
+    const double2 s = make_double2(a.x + b.x, a.y - b.y);
+    double2 v = make_double2(s.y, -s.x);
+    for (int l = 1; l <= k + 1; l++) v = csub(v, cscale(G.lesptr(n - l, n - l)[e], bd[l] / dt));
+    X[(i64)n * es + e] = cscale(v, dt / bd[0]);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Extrapolate (dyson.cpp:47-117)
+__global__ void extrap_tv_kernel(int N, int k, int n, DevGF G, const double *exw) {
+  const i64 tot = (i64)N * N * (G.ntau + 1);
+  GRID_STRIDE(idx, tot) {
+    double2 v = czero();
+    for (int j = 0; j <= k; j++) v = cadd(v, cscale(G.tvptr(n - j - 1, 0)[idx], exw[j]));
+    G.tvptr(n, 0)[idx] = v;
+  }
+}
+__global__ void extrap_ret_kernel(int N, int k, int n, DevGF G, const double *exw) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * (n + 1)) {
+    const int col = (int)(idx / es), e = (int)(idx - (i64)col * es);  // G^R(n, col)
+    const int i = e / N, j = e - (e / N) * N;
+    double2 v = czero();
+    if (col > k) {  // col = n - l with l < n - k
+      const int l = n - col;
+      for (int jj = 0; jj <= k; jj++) v = cadd(v, cscale(G.retptr(n - jj - 1, n - l - jj - 1)[e], exw[jj]));
+    } else {
+      const int l = col;
+      const int jcut = (l <= n - k - 1) ? k : (n - l - 1);
+      for (int jj = 0; jj <= jcut; jj++) v = cadd(v, cscale(G.retptr(n - jj - 1, l)[e], exw[jj]));
+      for (int jj = jcut + 1; jj <= k; jj++) {
+        const double2 a = G.retptr(l, n - jj - 1)[(i64)j * N + i];
+        v.x -= exw[jj] * a.x;
+        v.y += exw[jj] * a.y;
+      }
+    }
+    G.retptr(n, col)[e] = v;
+  }
+}
+__global__ void extrap_les_kernel(int N, int k, int n, DevGF G, const double *exw) {
+  const i64 es = (i64)N * N;
+  GRID_STRIDE(idx, es * (n + 1)) {
+    const int l = (int)(idx / es), e = (int)(idx - (i64)l * es);  // G^<(l, n)
+    const int i = e / N, j = e - (e / N) * N;
+    double2 v = czero();
+    if (l == 0) {
+      const double2 t = G.tvptr(n, 0)[(i64)j * N + i];
+      v = make_double2(-t.x, t.y);
+    } else if (l <= k) {
+      const int jcut = (k > n - l - 1) ? (n - l - 1) : k;
+      for (int jj = 0; jj <= jcut; jj++) v = cadd(v, cscale(G.lesptr(l, n - 1 - jj)[e], exw[jj]));
+      for (int jj = jcut + 1; jj <= k; jj++) {
+        const double2 a = G.lesptr(n - 1 - jj, l)[(i64)j * N + i];
+        v.x -= exw[jj] * a.x;
+        v.y += exw[jj] * a.y;
+      }
+    } else {
+      for (int jj = 0; jj <= k; jj++) v = cadd(v, cscale(G.lesptr(l - jj - 1, n - jj - 1)[e], exw[jj]));
+    }
+    G.lesptr(l, n)[e] = v;
+  }
+}
+
+// rho = i sig G^<(T,T)
+__global__ void dm_kernel(int N, int T, DevGF G, double2 *rho) {
+  GRID_STRIDE(e, (i64)N * N) {
+    const double2 g = G.lesptr(T, T)[e];
+    rho[e] = make_double2(-G.sig * g.y, G.sig * g.x);
+  }
+}
+
+__global__ void set_diag_kernel(int N, double2 *blk, double2 v) {
+  GRID_STRIDE(e, (i64)N * N) {
+    const int i = (int)(e / N), j = (int)(e - (e / N) * N);
+    blk[e] = i == j ? v : czero();
+  }
+}
+
+__global__ void add_kernel(i64 n, const double2 *a, double2 *out) {
+  GRID_STRIDE(i, n) out[i] = cadd(out[i], a[i]);
+}
+
+[[maybe_unused]] double *dev_table(Ctx &c, const std::vector<double> &h) {
+  double *d = c.ws.alloc<double>((i64)h.size());
+  NEDY_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, c.stream));
+  return d;
+}
+
+double sum_dev(Ctx &c, const double *d, int n, bool sqrt_each) {
+  std::vector<double> h(n);
+  NEDY_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+  NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  double s = 0;
+  for (double v : h) s += sqrt_each ? std::sqrt(v) : v;
+  return s;
+}
+
+} // namespace
+
+// ===================================================================================
+void gj_public(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB) { gj(c, n, nrhs, nb, A, sA, B, sB); }
+
+void check_status(Ctx &c) {
+  for (auto &p : c.pending_status) {
+    std::vector<int> h(p.second);
+    NEDY_CUDA(cudaMemcpyAsync(h.data(), p.first, sizeof(int) * p.second, cudaMemcpyDeviceToHost, c.stream));
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    for (int v : h)
+      if (v) {
+        c.pending_status.clear();
+        throw ArgError("singular matrix in a Dyson solve");
+      }
+  }
+  c.pending_status.clear();
+}
+
+void ensure_tables(Ctx &c) {
+  if (c.greg && c.greg_n == c.nt) return;
+  int n = c.nt + 1;
+  std::vector<double> g((size_t)n * n, 0.0), gt((size_t)n * n, 0.0);
+  for (int a = 0; a < n; a++) {
+    int top = std::max(a, c.k);
+    for (int j = 0; j <= top && j < n; j++) {
+      double w = c.W.gregory(a, j);
+      g[(size_t)a * n + j] = w;
+      gt[(size_t)j * n + a] = w;
+    }
+  }
+  if (c.greg) cudaFree(c.greg);
+  NEDY_CUDA(cudaMalloc(&c.greg, sizeof(double) * 2 * (size_t)n * n));
+  c.gregT = c.greg + (size_t)n * n;
+  NEDY_CUDA(cudaMemcpy(c.greg, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice));
+  NEDY_CUDA(cudaMemcpy(c.gregT, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice));
+  std::vector<double> small;
+  small.insert(small.end(), c.W.poly_diff.begin(), c.W.poly_diff.end());
+  small.insert(small.end(), c.W.bd.begin(), c.W.bd.end());
+  small.insert(small.end(), c.W.ex.begin(), c.W.ex.end());
+  small.insert(small.end(), c.col.w.begin(), c.col.w.end());
+  small.insert(small.end(), c.col.u.begin(), c.col.u.end());
+  if (c.small) cudaFree(c.small);
+  NEDY_CUDA(cudaMalloc(&c.small, sizeof(double) * small.size()));
+  NEDY_CUDA(cudaMemcpy(c.small, small.data(), sizeof(double) * small.size(), cudaMemcpyHostToDevice));
+  c.d_pdiff = c.small;
+  c.d_bd = c.d_pdiff + c.W.poly_diff.size();
+  c.d_ex = c.d_bd + c.W.bd.size();
+  c.d_w = c.d_ex + c.W.ex.size();
+  c.d_u = c.d_w + c.col.w.size();
+  c.greg_n = c.nt;
+}
+
+void update_minv(Ctx &c, const DevGF &Sig, const double2 *hmf, double mu, int t0, int t1) {
+  int N = Sig.nao, nb = t1 - t0 + 1;
+  if (nb <= 0) return;
+  i64 es = (i64)N * N;
+  double2 *M = c.ws.alloc<double2>(es * nb);
+  double2 *Mi = c.Minv + (i64)t0 * es;
+  build_M_kernel<<<nblk(es * nb), TPB, 0, c.stream>>>(N, nb, t0, hmf, Sig, c.W.bd[0], mu, c.dt, c.W.omega(0), M, Mi);
+  NEDY_CHECK_LAUNCH();
+  gj(c, N, N, nb, M, es, Mi, es);
+}
+
+void ensure_minv(Ctx &c, int N) {
+  if (c.Minv && c.Minv_cap >= (c.nt + 1) && c.Minv_nao == N) return;
+  if (c.Minv) cudaFree(c.Minv);
+  NEDY_CUDA(cudaMalloc(&c.Minv, sizeof(double2) * (size_t)(c.nt + 1) * N * N));
+  c.Minv_cap = c.nt + 1;
+  c.Minv_nao = N;
+}
+
+void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
+  const int N = G.nao, np = G.ntau + 1;
+  const i64 es = (i64)N * N;
+  if (c.mixK && c.mixK_src == G.mat && c.mixK_ver == G.mat_version && c.mixK_nao == N) return;
+  build_mixing_eval(c.col);
+  const int Q2 = 2 * c.col.Q;
+  if (c.mixK && c.mixK_nao != N) { cudaFree(c.mixK); c.mixK = nullptr; }
+  if (!c.mixK) NEDY_CUDA(cudaMalloc(&c.mixK, sizeof(double2) * (size_t)np * np * es));
+  // sign of the antiperiodic extension folded into the first half of EB
+  std::vector<double> EBs(c.col.EB);
+  for (int m = 0; m < np; m++)
+    for (int q = 0; q < c.col.Q; q++)
+      for (int j = 0; j < np; j++) EBs[((size_t)m * Q2 + q) * np + j] *= (double)G.sig;
+  const int chunk = std::max(1, (int)std::min<i64>(np, (i64)(2LL << 30) / (sizeof(double2) * Q2 * es)));
+  double *dEA = nullptr, *dEB = nullptr;
+  double2 *BB = nullptr;
+  NEDY_CUDA(cudaMalloc(&dEA, sizeof(double) * c.col.EA.size()));
+  NEDY_CUDA(cudaMalloc(&dEB, sizeof(double) * EBs.size()));
+  NEDY_CUDA(cudaMalloc(&BB, sizeof(double2) * (size_t)chunk * Q2 * es));
+  NEDY_CUDA(cudaMemcpy(dEA, c.col.EA.data(), sizeof(double) * c.col.EA.size(), cudaMemcpyHostToDevice));
+  NEDY_CUDA(cudaMemcpy(dEB, EBs.data(), sizeof(double) * EBs.size(), cudaMemcpyHostToDevice));
+  for (int m0 = 0; m0 < np; m0 += chunk) {
+    int nm = std::min(chunk, np - m0);
+    {  // BB[m] = EB[m] (2Q x np) * G^M (np x N^2)
+      GemmArgs g;
+      g.M = Q2; g.N = (int)es; g.K = np; g.nb1 = nm;
+      g.A = rowmajor(dEB + (size_t)m0 * Q2 * np, np); g.A.bs1 = (i64)Q2 * np; g.a_cplx = false;
+      g.B = rowmajor(G.mat, es);
+      g.C = rowmajor(BB, es); g.C.bs1 = (i64)Q2 * es;
+      gemm(g, c.stream);
+    }
+    {  // K[m] = (beta/2) EA[m] (np x 2Q) * BB[m]
+      GemmArgs g;
+      g.M = np; g.N = (int)es; g.K = Q2; g.nb1 = nm;
+      g.A = rowmajor(dEA + (size_t)m0 * np * Q2, Q2); g.A.bs1 = (i64)np * Q2; g.a_cplx = false;
+      g.B = rowmajor(BB, es); g.B.bs1 = (i64)Q2 * es;
+      g.C = rowmajor(c.mixK + (size_t)m0 * np * es, es); g.C.bs1 = (i64)np * es;
+      g.alpha = make_double2(0.5 * c.beta, 0.0);
+      gemm(g, c.stream);
+    }
+  }
+  NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  cudaFree(dEA);
+  cudaFree(dEB);
+  cudaFree(BB);
+  c.mixK_src = G.mat;
+  c.mixK_ver = G.mat_version;
+  c.mixK_nao = N;
+}
+
+// out[m] (+)= sum_i A_i K[m][i]   (A_i = tv blocks of one time row), out in [m][a][b] layout
+static void mixing_gemm(Ctx &c, int N, int np, const double2 *Arow, const double2 *K, double2 *out, bool real_only,
+                        double2 beta) {
+  const i64 es = (i64)N * N;
+  GemmArgs g;
+  g.M = N; g.N = (int)(np * N); g.K = (int)(np * N);
+  g.A.p = Arow; g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1;
+  g.B.p = K; g.B.rdiv = N; g.B.rs_hi = es; g.B.rs_lo = N; g.B.cdiv = N; g.B.cs_hi = (i64)np * es; g.B.cs_lo = 1;
+  g.C.p = out; g.C.rs_lo = N; g.C.cdiv = N; g.C.cs_hi = es; g.C.cs_lo = 1;
+  g.beta = beta;
+  (void)real_only;
+  gemm(g, c.stream);
+}
+
+// ===================================================================================
+void extrapolate(Ctx &c, int n, DevGF &G) {
+  NEDY_REQUIRE(n > c.k && n <= G.nt, "extrapolate: need k < n <= nt");
+  ensure_tables(c);
+  const int N = G.nao, k = c.k;
+  const i64 es = (i64)N * N;
+  extrap_tv_kernel<<<nblk(es * (G.ntau + 1)), TPB, 0, c.stream>>>(N, k, n, G, c.d_ex);
+  extrap_ret_kernel<<<nblk(es * (n + 1)), TPB, 0, c.stream>>>(N, k, n, G, c.d_ex);
+  extrap_les_kernel<<<nblk(es * (n + 1)), TPB, 0, c.stream>>>(N, k, n, G, c.d_ex);
+  NEDY_CHECK_LAUNCH();
+}
+
+void get_dm(Ctx &c, const DevGF &G, int T, double2 *rho) {
+  dm_kernel<<<nblk((i64)G.nao * G.nao), TPB, 0, c.stream>>>(G.nao, T, G, rho);
+  NEDY_CHECK_LAUNCH();
+}
+
+void hf_decomp(Ctx &c, int nspin, double2 *const *hmf_T, const double2 *rho) {
+  NEDY_REQUIRE(c.Vija, "hf: density-fitted tensor not set");
+  const int N = c.df_nao, A = c.df_naux;
+  const i64 es = (i64)N * N;
+  double2 *rt = c.ws.alloc<double2>(es);
+  double2 *Xa = c.ws.alloc<double2>(A);
+  double2 *T1 = c.ws.alloc<double2>(es * A);
+  // total density for the Hartree term
+  NEDY_CUDA(cudaMemcpyAsync(rt, rho, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+  if (nspin == 2) {
+    add_kernel<<<nblk(es), TPB, 0, c.stream>>>(es, rho + es, rt);
+    NEDY_CHECK_LAUNCH();
+  }
+  {  // Xa = rho_flat (1 x N^2) * Vija (N^2 x A)
+    GemmArgs g;
+    g.M = 1; g.N = A; g.K = (int)es;
+    g.A = rowmajor(rt, es);
+    g.B = rowmajor(c.Vija, A); g.b_cplx = false;
+    g.C = rowmajor(Xa, A);
+    gemm(g, c.stream);
+  }
+  for (int s = 0; s < nspin; s++) {
+    {  // hmf_flat += f * Vija (N^2 x A) * Xa (A x 1)
+      GemmArgs g;
+      g.M = (int)es; g.N = 1; g.K = A;
+      g.A = rowmajor(c.Vija, A); g.a_cplx = false;
+      g.B = rowmajor(Xa, 1);
+      g.C = rowmajor(hmf_T[s], 1);
+      g.alpha = make_double2(nspin == 1 ? 2.0 : 1.0, 0.0);
+      g.beta = make_double2(1.0, 0.0);
+      gemm(g, c.stream);
+    }
+    const double2 *rs = rho + (nspin == 2 ? s * es : 0);
+    {  // T1[(i,a)][k] = sum_l Viaj[(i,a)][l] rho[k][l]
+      GemmArgs g;
+      g.M = N * A; g.N = N; g.K = N;
+      g.A = rowmajor(c.Viaj, N); g.a_cplx = false;
+      g.B = transposed(rs, N);
+      g.C = rowmajor(T1, N);
+      gemm(g, c.stream);
+    }
+    {  // hmf -= T1 (N x (a,k)) * Vaij ((a,k) x j)
+      GemmArgs g;
+      g.M = N; g.N = N; g.K = N * A;
+      g.A = rowmajor(T1, (i64)N * A);
+      g.B = rowmajor(c.Vaij, N); g.b_cplx = false;
+      g.C = rowmajor(hmf_T[s], N);
+      g.alpha = make_double2(-1.0, 0.0);
+      g.beta = make_double2(1.0, 0.0);
+      gemm(g, c.stream);
+    }
+  }
+}
+
+// ===================================================================================
+static double dyson_ret(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *hmf, double mu) {
+  const int N = G.nao, k = c.k, kn = k * N, ld = c.nt + 1;
+  const i64 es = (i64)N * N;
+  const double dt = c.dt;
+  double *err = c.ws.alloc<double>(T + 1);
+  NEDY_CUDA(cudaMemsetAsync(err, 0, sizeof(double) * (T + 1), c.stream));
+  set_diag_kernel<<<nblk(es), TPB, 0, c.stream>>>(N, G.retptr(T, T), make_double2(0.0, -1.0));
+  double2 *M = c.ws.alloc<double2>((i64)kn * kn);
+  double2 *Qs = c.ws.alloc<double2>((i64)kn * N);
+  ret_start_kernel<<<nblk((i64)kn * kn + (i64)kn * N), TPB, 0, c.stream>>>(N, k, T, G, S, hmf, c.d_pdiff, c.greg, ld,
+                                                                             mu, dt, M, Qs);
+  NEDY_CHECK_LAUNCH();
+  gj(c, kn, N, 1, M, 0, Qs, 0);
+  ret_start_store<<<nblk(es * k), TPB, 0, c.stream>>>(N, k, T, G, Qs, err + 1);
+  NEDY_CHECK_LAUNCH();
+  if (T <= k) return sum_dev(c, err, T + 1, true);
+  double2 *Q = c.ws.alloc<double2>((i64)(T + 1) * es);
+  NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * (T + 1) * es, c.stream));
+  // Q_n = sum_{l<=k} w(n,l) G^R(T,T-l) Sig^R(T-l,T-n),  n = k+1..T
+  for (int l = 0; l <= k; l++) {
+    GemmArgs g;
+    g.M = N; g.N = N; g.K = N; g.nb1 = T - k;
+    g.A = rowmajor(G.retptr(T, T - l), N);
+    g.B = rowmajor(S.retptr(T - l, T - (k + 1)), N); g.B.bs1 = -es;
+    g.C = rowmajor(Q + (i64)(k + 1) * es, N); g.C.bs1 = es;
+    g.bscale = c.gregT + (i64)l * ld + (k + 1);
+    g.beta = make_double2(1.0, 0.0);
+    gemm(g, c.stream);
+  }
+  const int smem = N * sizeof(double2);
+  for (int n = k + 1; n <= T; n++) {
+    ret_step_kernel<<<N, std::min(N, 256), smem, c.stream>>>(N, k, T, n, G, Q, c.Minv, c.d_bd, dt, err);
+    NEDY_CHECK_LAUNCH();
+    if (n < T) {  // push G^R(T,T-n) into Q_m, m = n+1..T
+      GemmArgs g;
+      g.M = N; g.N = N; g.K = N; g.nb1 = T - n;
+      g.A = rowmajor(G.retptr(T, T - n), N);
+      g.B = rowmajor(S.retptr(T - n, T - n - 1), N); g.B.bs1 = -es;
+      g.C = rowmajor(Q + (i64)(n + 1) * es, N); g.C.bs1 = es;
+      g.bscale = c.gregT + (i64)n * ld + (n + 1);
+      g.beta = make_double2(1.0, 0.0);
+      gemm(g, c.stream);
+    }
+  }
+  return sum_dev(c, err, T + 1, true);
+}
+
+static double dyson_tv(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *hmf, double mu) {
+  const int N = G.nao, np = G.ntau + 1, ld = c.nt + 1;
+  const i64 es = (i64)N * N, row = (i64)np * es;
+  double2 *old = c.ws.alloc<double2>(row);
+  double2 *ctv = c.ws.alloc<double2>(row);
+  NEDY_CUDA(cudaMemcpyAsync(old, G.tvptr(T, 0), sizeof(double2) * row, cudaMemcpyDeviceToDevice, c.stream));
+  // mixing: int_0^beta Sig^tv(T,tau') G^M(tau' - tau_m)
+  mixing_gemm(c, N, np, S.tvptr(T, 0), c.mixK, ctv, false, czero());
+  // CTV1: sum_{j<T} dt w(T,j) Sig^R(T,j) G^tv(j, .)   (the j = T term multiplies G^tv(T,.) = 0)
+  if (T > 0) {
+    GemmArgs g;
+    g.M = N; g.N = (int)(np * N); g.K = T * N;
+    g.A.p = S.retptr(T, 0); g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1;
+    g.B.p = G.tvptr(0, 0); g.B.rdiv = N; g.B.rs_hi = row; g.B.rs_lo = N; g.B.cdiv = N; g.B.cs_hi = es; g.B.cs_lo = 1;
+    g.C.p = ctv; g.C.rs_lo = N; g.C.cdiv = N; g.C.cs_hi = es; g.C.cs_lo = 1;
+    g.kscale = c.greg + (i64)T * ld; g.kdiv = N;
+    g.alpha = make_double2(c.dt, 0.0);
+    g.beta = make_double2(1.0, 0.0);
+    gemm(g, c.stream);
+  }
+  tv_bd_kernel<<<nblk(row), TPB, 0, c.stream>>>(row, c.k, T, G, c.d_bd, c.dt, ctv);
+  NEDY_CHECK_LAUNCH();
+  // M(T) and its inverse
+  update_minv(c, S, hmf, mu, T, T);
+  {  // G^tv(T, m) = Minv(T) ctv_m
+    GemmArgs g;
+    g.M = N; g.N = (int)(np * N); g.K = N;
+    g.A = rowmajor(c.Minv + (i64)T * es, N);
+    g.B.p = ctv; g.B.rs_lo = N; g.B.cdiv = N; g.B.cs_hi = es; g.B.cs_lo = 1;
+    g.C.p = G.tvptr(T, 0); g.C.rs_lo = N; g.C.cdiv = N; g.C.cs_hi = es; g.C.cs_lo = 1;
+    gemm(g, c.stream);
+  }
+  double *err = c.ws.alloc<double>(np);
+  NEDY_CUDA(cudaMemsetAsync(err, 0, sizeof(double) * np, c.stream));
+  diffnorm_kernel<<<nblk(row), TPB, 0, c.stream>>>(N, np, old, G.tvptr(T, 0), err);
+  NEDY_CHECK_LAUNCH();
+  return sum_dev(c, err, np, true);
+}
+
+static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *hmf, double mu) {
+  const int N = G.nao, k = c.k, kn = k * N, np = G.ntau + 1, ld = c.nt + 1;
+  const i64 es = (i64)N * N;
+  const double dt = c.dt;
+  double *err = c.ws.alloc<double>(n + 2);
+  NEDY_CUDA(cudaMemsetAsync(err, 0, sizeof(double) * (n + 2), c.stream));
+  double2 *X = c.ws.alloc<double2>((i64)(n + 1) * es);
+  double2 *Q = c.ws.alloc<double2>((i64)(n + 1) * es);
+  NEDY_CUDA(cudaMemsetAsync(X, 0, sizeof(double2) * (n + 1) * es, c.stream));
+  NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * (n + 1) * es, c.stream));
+  les_init_kernel<<<nblk(es), TPB, 0, c.stream>>>(N, n, G, X, err + n + 1);
+  NEDY_CHECK_LAUNCH();
+  // Cles3: Q_p += int Sig^tv(p,tau) [sig i G^tv(n,beta-tau)^+] dtau   (p = 0..n)
+  {
+    double2 *ntt = c.ws.alloc<double2>((i64)np * es);
+    double2 *Bw = c.ws.alloc<double2>((i64)np * es);
+    ntt_kernel<<<nblk(es * np), TPB, 0, c.stream>>>(N, G.ntau, n, G, G.sig, ntt);
+    lesser_weights_kernel<<<nblk(es), TPB, 0, c.stream>>>(N, G.ntau, ntt, c.d_w, c.d_u, c.col.ctop, c.beta, Bw);
+    NEDY_CHECK_LAUNCH();
+    GemmArgs g;
+    g.M = (n + 1) * N; g.N = N; g.K = np * N;
+    g.A.p = S.tvptr(0, 0); g.A.rdiv = N; g.A.rs_hi = (i64)np * es; g.A.rs_lo = N;
+    g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1;
+    g.B = rowmajor(Bw, N);
+    g.C = rowmajor(Q, N);
+    g.beta = make_double2(1.0, 0.0);
+    gemm(g, c.stream);
+  }
+  // Cles2 with X_j = dt w(n,j) G^R(n,j)^+
+  {
+    double2 *Xc = c.ws.alloc<double2>((i64)(n + 1) * es);
+    cles2_x_kernel<<<nblk(es * (n + 1)), TPB, 0, c.stream>>>(N, n, G, c.greg + (i64)n * ld, dt, Xc);
+    NEDY_CHECK_LAUNCH();
+    std::vector<i64> offA(n + 1), offC(n + 1), offB(n + 1);
+    std::vector<int> Mv(n + 1), Kv(n + 1);
+    for (int p = 0; p <= n; p++) {
+      offA[p] = les_idx(0, p) * es;
+      offC[p] = (i64)p * es;
+      offB[p] = (i64)p * es;
+      Mv[p] = (p + 1) * N;
+      Kv[p] = p * N;
+    }
+    i64 *dOffA = c.ws.alloc<i64>(n + 1), *dOffB = c.ws.alloc<i64>(n + 1), *dOffC = c.ws.alloc<i64>(n + 1);
+    int *dM = c.ws.alloc<int>(n + 1), *dK = c.ws.alloc<int>(n + 1);
+    NEDY_CUDA(cudaMemcpyAsync(dOffA, offA.data(), sizeof(i64) * (n + 1), cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dOffB, offB.data(), sizeof(i64) * (n + 1), cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dOffC, offC.data(), sizeof(i64) * (n + 1), cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dM, Mv.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dK, Kv.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream));
+    {  // part 1: Q_p -= sum_{j<p} Sig^<(j,p)^+ X_j     (group p: K = p N)
+      GemmArgs g;
+      g.M = N; g.N = N; g.K = n * N; g.nb1 = n + 1;
+      g.A.p = S.les; g.A.rs_lo = 1; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = N;
+      g.conjA = true;
+      g.B = rowmajor(Xc, N);
+      g.C = rowmajor(Q, N);
+      g.goffA = dOffA; g.goffC = dOffC; g.gK = dK;
+      g.alpha = make_double2(-1.0, 0.0);
+      g.beta = make_double2(1.0, 0.0);
+      gemm(g, c.stream);
+    }
+    {  // part 2: Q_p += sum_{j>=p} Sig^<(p,j) X_j        (group j: rows (p,a), p <= j)
+      GemmArgs g;
+      g.M = (n + 1) * N; g.N = N; g.K = N; g.nb1 = n + 1;
+      g.A = rowmajor(S.les, N);
+      g.B = rowmajor(Xc, N);
+      g.C = rowmajor(Q, N);
+      g.goffA = dOffA; g.goffB = dOffB; g.gM = dM;
+      g.atomic = true;
+      gemm(g, c.stream);
+    }
+  }
+  // start block m = 1..k
+  {
+    double2 *M = c.ws.alloc<double2>((i64)kn * kn);
+    double2 *Qs = c.ws.alloc<double2>((i64)kn * N);
+    les_start_kernel<<<nblk((i64)kn * kn + (i64)kn * N), TPB, 0, c.stream>>>(N, k, n, G, S, hmf, c.d_pdiff, c.greg,
+                                                                              ld, mu, dt, Q, M, Qs);
+    NEDY_CHECK_LAUNCH();
+    gj(c, kn, N, 1, M, 0, Qs, 0);
+    NEDY_CUDA(cudaMemcpyAsync(X + es, Qs, sizeof(double2) * kn * N, cudaMemcpyDeviceToDevice, c.stream));
+  }
+  // sequential m = k+1 .. n-1, then the diagonal
+  const int LC = 8;  // blocks per split-K chunk of the pull sums
+  for (int m = k + 1; m <= n; m++) {
+    // Q_m += sum_{l<m} dt w(m,l) Sig^R(m,l) X_l   (split-K over l in chunks of LC blocks, atomics)
+    for (int part = 0; part < 2; part++) {
+      const int nfull = m / LC, rem = m - nfull * LC;
+      const int nb = part == 0 ? nfull : (rem > 0 ? 1 : 0);
+      if (nb == 0) continue;
+      const int l0 = part == 0 ? 0 : nfull * LC;
+      GemmArgs g;
+      g.M = N; g.N = N; g.K = (part == 0 ? LC : rem) * N; g.nb1 = nb;
+      g.A.p = S.retptr(m, l0); g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1; g.A.bs1 = LC * es;
+      g.B = rowmajor(X + (i64)l0 * es, N); g.B.bs1 = LC * es;
+      g.C = rowmajor(Q + (i64)m * es, N);
+      g.kscale = c.greg + (i64)m * ld + l0; g.kdiv = N; g.kscale_bs1 = LC;
+      g.alpha = make_double2(dt, 0.0);
+      g.atomic = true;
+      gemm(g, c.stream);
+    }
+    if (m < n) {
+      les_step_kernel<<<N, std::min(N, 256), N * sizeof(double2), c.stream>>>(N, k, m, Q, X, c.Minv, c.d_bd, dt);
+      NEDY_CHECK_LAUNCH();
+    }
+  }
+  {
+    const double wnn = c.W.gregory(n, n);
+    static int attr_set = 0;
+    if (!attr_set) {
+      NEDY_CUDA(cudaFuncSetAttribute(les_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr_set = 1;
+    }
+    NEDY_REQUIRE(2 * es * (i64)sizeof(double2) <= 200 * 1024, "dyson_step: nao too large for the diagonal kernel");
+    les_diag_kernel<<<1, 256, 2 * es * sizeof(double2), c.stream>>>(N, k, n, G, S, hmf, c.d_ex, c.d_bd, wnn, mu, dt,
+                                                                   Q, X);
+    NEDY_CHECK_LAUNCH();
+  }
+  diffnorm_kernel<<<nblk((i64)(n + 1) * es), TPB, 0, c.stream>>>(N, n + 1, G.lesptr(0, n), X, err);
+  NEDY_CHECK_LAUNCH();
+  NEDY_CUDA(cudaMemcpyAsync(G.lesptr(1, n), X + es, sizeof(double2) * n * es, cudaMemcpyDeviceToDevice, c.stream));
+  return sum_dev(c, err, n + 2, true);
+}
+
+void dyson_step(Ctx &c, int n, DevGF &G, const DevGF &Sig, const double2 *hmf, double mu, double *err) {
+  NEDY_REQUIRE(n > c.k && n <= G.nt, "dyson_step: need k < n <= nt");
+  NEDY_REQUIRE(G.nao == Sig.nao && G.ntau == Sig.ntau && G.nt == Sig.nt && G.sig == Sig.sig,
+               "dyson_step: G and Sigma shapes differ");
+  NEDY_REQUIRE(G.nt == c.nt && G.ntau == c.ntau, "dyson_step: G does not match the context sizes");
+  ensure_tables(c);
+  ensure_mixing_kernel(c, G);
+  ensure_minv(c, G.nao);
+  c.ws.reset();
+  // time-local inverses for t' < n (final) -- recomputed each call, they are cheap and batched
+  update_minv(c, Sig, hmf, mu, 0, n - 1);
+  double e1 = dyson_ret(c, n, G, Sig, hmf, mu);
+  double e2 = dyson_tv(c, n, G, Sig, hmf, mu);
+  double e3 = dyson_les(c, n, G, Sig, hmf, mu);
+  check_status(c);
+  if (err) { err[0] = e1; err[1] = e2; err[2] = e3; }
+}
+
+} // namespace nedy

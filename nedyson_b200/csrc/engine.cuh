@@ -1,0 +1,98 @@
+// Device-side objects of the B200 GF2 engine: Green's functions in the
+// reference's packed layout, the workspace arena and the engine context.
+#pragma once
+#include "common.cuh"
+#include "gemm_f64.cuh"
+#include <vector>
+#include <memory>
+
+namespace nedy {
+
+// Contour Green's function resident in HBM, same packing as the reference
+// (greens.cpp:34-195): les column T, ret row T and tv row T are contiguous.
+struct DevGF {
+  int nt = 0, ntau = 0, nao = 0, sig = -1;
+  i64 es = 0;
+  double2 *les = nullptr, *ret = nullptr, *tv = nullptr, *mat = nullptr;
+  unsigned long long mat_version = 0;  // bumped whenever G^M is written
+  i64 ntri() const { return (i64)(nt + 1) * (nt + 2) / 2; }
+  __host__ __device__ double2 *lesptr(i64 i, i64 j) const { return les + les_idx(i, j) * es; }
+  __host__ __device__ double2 *retptr(i64 i, i64 j) const { return ret + ret_idx(i, j) * es; }
+  __host__ __device__ double2 *tvptr(i64 i, i64 m) const { return tv + (i * (ntau + 1) + m) * es; }
+  __host__ __device__ double2 *matptr(i64 m) const { return mat + m * es; }
+};
+
+// Bump allocator for per-call workspace.  A request that does not fit opens a
+// further device block (live pointers stay valid); at the next reset() the blocks
+// are merged into one of the combined size, so steady-state calls allocate nothing.
+class Arena {
+ public:
+  ~Arena();
+  void reset();
+  void *get(size_t bytes);
+  template <class T> T *alloc(i64 n) { return (T *)get(sizeof(T) * (size_t)n); }
+  size_t capacity() const;
+
+ private:
+  struct Block { char *p; size_t cap, top; };
+  std::vector<Block> blocks_;
+};
+
+// Calculus weights (host tables) -- the restatement of Integration::Integrator
+// lives in weights.cpp.
+struct Weights {
+  int k = 0;
+  std::vector<double> poly_interp, poly_diff, poly_integ, bd, start, Omega, ex;
+  double gregory(int n, int j) const;
+  double omega(int j) const { return Omega[(size_t)k * (k + 1) + j]; }
+  double pdiff(int m, int l) const { return poly_diff[(size_t)m * (k + 1) + l]; }
+  double pinterp(int a, int l) const { return poly_interp[(size_t)a * (k + 1) + l]; }
+};
+Weights make_weights(int k);
+
+// Legendre-Gauss-Lobatto collocation on [0, beta] (collocation.cpp).
+struct Colloc {
+  int ntau = 0;
+  std::vector<double> x, w, u;  // nodes, weights, top-mode coefficients
+  double ctop = 0;
+  std::vector<double> EA, EB;  // per node m: evaluation matrices of the mixing quadrature
+  int Q = 0;
+};
+Colloc make_colloc(int ntau);
+void build_mixing_eval(Colloc &c);
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nt = 0, ntau = 0, nao = 0, k = 5;
+  double beta = 1.0, dt = 0.01;
+  Arena ws;
+  i64 ws_budget = 4LL << 30;  // bytes the self-energy may use for chunk intermediates
+  std::vector<std::pair<int *, int>> pending_status;  // device status words of batched solves
+  // Gregory weights w(n, j) for n, j <= nt (row-major and transposed), small tables
+  double *greg = nullptr, *gregT = nullptr;
+  int greg_n = -1;
+  double *small = nullptr, *d_pdiff = nullptr, *d_bd = nullptr, *d_ex = nullptr, *d_w = nullptr, *d_u = nullptr;
+  Weights W;
+  Colloc col;
+  // density-fitted interaction, several layouts (real, row-major)
+  int df_nao = 0, df_naux = 0;
+  double *Vija = nullptr;  // [i][j][a]
+  double *Viaj = nullptr;  // [i][a][j]
+  double *Vaij = nullptr;  // [a][i][j]
+  double *Vmbq = nullptr;  // [m][b][q] = V^b_qm
+  // full U (N^4 real) and the exchange combination Uexch
+  int u_nao = 0;
+  double *U = nullptr, *Uexch = nullptr;
+  // mixing kernel K[m][i] (nao x nao) of the current G^M, keyed by (G^M pointer, version)
+  double2 *mixK = nullptr;
+  const double2 *mixK_src = nullptr;
+  unsigned long long mixK_ver = ~0ULL;
+  int mixK_nao = 0;
+  // inverses of the time-local Dyson matrices M(t') = (i bd0/dt + mu) - hmf(t') - dt w0 Sig^R(t',t')
+  double2 *Minv = nullptr;
+  int Minv_cap = 0, Minv_nao = 0;
+  ~Ctx();
+};
+
+} // namespace nedy

@@ -1,0 +1,34 @@
+// Hot-path entry points of the engine (device work enqueued on ctx.stream).
+#pragma once
+#include "engine.cuh"
+
+namespace nedy {
+
+// molGF2SolverDecomp::solve (nspin = 1) / molGF2SolverSpinDecomp::solve (nspin = 2)
+void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G);
+// molGF2Solver::solve (full U_ijkl, restricted)
+void sigma_full(Ctx &c, int T, DevGF &Sig, const DevGF &G);
+
+// hmf(T) += HF(rho); hmf points at the nao x nao block of time T.
+// molHFSolverDecomp::solve_HF (nspin = 1) / molHFSolverSpinDecomp::solve_HF (nspin = 2: rho[2], hmf[2])
+void hf_decomp(Ctx &c, int nspin, double2 *const *hmf_T, const double2 *rho);
+// molHFSolver::solve_HF (full U)
+void hf_full(Ctx &c, double2 *hmf_T, const double2 *rho);
+// rho = i*sig*G^<(T,T) (greens.h:68-74), device to device
+void get_dm(Ctx &c, const DevGF &G, int T, double2 *rho);
+
+// dyson::Extrapolate (dyson.cpp:47-117)
+void extrapolate(Ctx &c, int n, DevGF &G);
+// dyson::dyson_step (dyson_step.h:329-382); hmf: (nt+1) x nao x nao on the device.
+// Returns the sum of the three component errors (ret, tv, les) when err != nullptr.
+void dyson_step(Ctx &c, int n, DevGF &G, const DevGF &Sig, const double2 *hmf, double mu, double *err);
+// dyson::dyson_start (dyson_boot.h:195-230)
+double dyson_start(Ctx &c, DevGF &G, const DevGF &Sig, const double2 *hmf, double mu);
+// dyson::energy_conv (dyson_integrals.h:24-70)
+double energy_conv(Ctx &c, int T, const DevGF &Sig, const DevGF &G);
+// Mixing kernel of G^M (rebuilt when G^M changes)
+void ensure_mixing_kernel(Ctx &c, const DevGF &G);
+// Cached inverse of the time-local Dyson matrix for times [t0, t1] (after their rows are final)
+void update_minv(Ctx &c, const DevGF &Sig, const double2 *hmf, double mu, int t0, int t1);
+
+} // namespace nedy

@@ -1,0 +1,344 @@
+// Density-fitted second-Born (GF2) self-energy for one time row T, restricted and
+// spin-unrestricted.  Replaces molGF2SolverDecomp::solve
+// (reference src/mol2bSolver_decomp_impl.h:412-429) and
+// molGF2SolverSpinDecomp::solve (src/mol2bSolver_spin_decomp_impl.h:436-466).
+//
+// Every slice (t' <= T for the lesser / retarded rows, every tau point for the
+// mixed row) is the same trilinear map of three nao x nao blocks (X, Y, Z):
+//   bubble   B(X,Y,Z) = f * sum_ab Tr[V^a Z V^b Y] V^a X V^b      (f = 2 restricted)
+//   exchange E(X,Y,Z) = sum_ab V^a X V^b Y V^a Z V^b
+//   Sigma    = B - E
+// with (reference loops :431-670)
+//   lesser   (X,Y,Z) = (L, R - L^+, L)                 L = G^<(t',T), R = G^R(T,t')
+//   mixed    (X,Y,Z) = (G^tv(T,tau), -sig G^tv(T,ntau-tau)^+, G^tv(T,tau))
+//   retarded T(R, L, R-L^+) + T(L^+, R^+, L^+) - T(L^+, L, R)
+// The retarded exchange is evaluated as two "units" exactly like the reference
+// (src/mol2bSolver_decomp_impl.h:293-402): M = (-L^+) V (L - R^+) with Z = R, and
+// M = R V L + (-L^+) V R^+ with Z = R - L^+.
+//
+// Each contraction is a batched FP64 GEMM over the slices of a chunk; the N^4
+// exchange intermediate S_{(l,n),(q,j)} lives only in a chunk-sized workspace.
+#include "engine.cuh"
+#include "sigma.cuh"
+
+namespace nedy {
+namespace {
+
+enum PrepMode { PREP_LES = 0, PREP_TV = 1, PREP_RET = 2 };
+
+// Per-slice derived blocks.  out[k][s] for k = 0..nout-1, each N x N.
+//  LES: out0 = R - L^+                              (G^>(T,t'))
+//  TV : out0 = -sig * Gv^+                          (G^lceil)
+//  RET: out0 = L^+, out1 = R^+, out2 = R - L^+, out3 = L - R^+
+__global__ void prep_kernel(int mode, int N, int nsl, const double2 *L0, i64 Ls, const double2 *R0, i64 Rs,
+                            double sgn, double2 *out, i64 out_stride) {
+  const i64 es = (i64)N * N;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < es * nsl; idx += (i64)gridDim.x * blockDim.x) {
+    const int s = (int)(idx / es);
+    const int e = (int)(idx - (i64)s * es);
+    const int i = e / N, j = e - (e / N) * N;
+    if (mode == PREP_LES) {
+      double2 r = R0[s * Rs + e];
+      double2 lt = L0[s * Ls + (i64)j * N + i];
+      out[s * es + e] = make_double2(r.x - lt.x, r.y + lt.y);
+    } else if (mode == PREP_TV) {
+      // L0 points at the mirrored node G^tv(T, ntau - tau0 - s), R0 unused; Ls < 0 walks back.
+      double2 g = L0[s * Ls + (i64)j * N + i];
+      out[s * es + e] = make_double2(sgn * g.x, -sgn * g.y);
+    } else {
+      double2 l = L0[s * Ls + e], lt = L0[s * Ls + (i64)j * N + i];
+      double2 r = R0[s * Rs + e], rt = R0[s * Rs + (i64)j * N + i];
+      (void)l;
+      out[0 * out_stride + s * es + e] = make_double2(lt.x, -lt.y);            // L^+
+      out[1 * out_stride + s * es + e] = make_double2(rt.x, -rt.y);            // R^+
+      out[2 * out_stride + s * es + e] = make_double2(r.x - lt.x, r.y + lt.y); // R - L^+
+      out[3 * out_stride + s * es + e] = make_double2(l.x - rt.x, l.y + rt.y); // L - R^+
+    }
+  }
+}
+
+struct Blocks {  // a batch of N x N blocks, block s at p + s * stride (elements)
+  const double2 *p;
+  i64 stride;
+};
+
+View blk(Blocks b, int N) {
+  View v = rowmajor(b.p, N);
+  v.bs1 = b.stride;
+  return v;
+}
+View blkT(Blocks b, int N) {
+  View v = transposed(b.p, N);
+  v.bs1 = b.stride;
+  return v;
+}
+
+struct DF {
+  Ctx &c;
+  int N, A, nsl;
+  i64 es, NA, N2A;
+  cudaStream_t s;
+  DF(Ctx &cx, int nsl_) : c(cx), N(cx.df_nao), A(cx.df_naux), nsl(nsl_), s(cx.stream) {
+    es = (i64)N * N;
+    NA = (i64)N * A;
+    N2A = es * A;
+  }
+  // VZ[s] = Viaj (NA x N) * Z_s   -> layout [n][a][q] = (V^a Z)_nq
+  void VZ(Blocks Z, double2 *out) {
+    GemmArgs g;
+    g.M = (int)NA; g.N = N; g.K = N; g.nb1 = nsl;
+    g.A = rowmajor(c.Viaj, N); g.a_cplx = false;
+    g.B = blk(Z, N);
+    g.C = rowmajor(out, N); g.C.bs1 = N2A;
+    gemm(g, s);
+  }
+  // VYt[s] = Y_s^T * Vmbq  -> layout [n][b][q] = (V^b Y)_qn
+  void VYt(Blocks Y, double2 *out) {
+    GemmArgs g;
+    g.M = N; g.N = (int)NA; g.K = N; g.nb1 = nsl;
+    g.A = blkT(Y, N);
+    g.B = rowmajor(c.Vmbq, NA); g.b_cplx = false;
+    g.C = rowmajor(out, NA); g.C.bs1 = N2A;
+    gemm(g, s);
+  }
+  // P[s] (+)= sign * sum_{(n,q)} VZ[s][n][a][q] * VYt[s][n][b][q]
+  void P(const double2 *vz, const double2 *vyt, double2 *P, double sign, bool acc) {
+    GemmArgs g;
+    g.M = A; g.N = A; g.K = (int)es; g.nb1 = nsl;
+    g.A.p = vz; g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = NA; g.A.cs_lo = 1; g.A.bs1 = N2A;
+    g.B.p = vyt; g.B.rdiv = N; g.B.rs_hi = NA; g.B.rs_lo = 1; g.B.cs_lo = N; g.B.bs1 = N2A;
+    g.C = rowmajor(P, A); g.C.bs1 = (i64)A * A;
+    g.alpha = make_double2(sign, 0);
+    g.beta = make_double2(acc ? 1.0 : 0.0, 0);
+    gemm(g, s);
+  }
+  // W[s] = P[s] * Vaij  -> [a][(k,j)]
+  void W(const double2 *P, double2 *W) {
+    GemmArgs g;
+    g.M = A; g.N = (int)es; g.K = A; g.nb1 = nsl;
+    g.A = rowmajor(P, A); g.A.bs1 = (i64)A * A;
+    g.B = rowmajor(c.Vaij, es); g.b_cplx = false;
+    g.C = rowmajor(W, es); g.C.bs1 = N2A;
+    gemm(g, s);
+  }
+  // Sigma_s += f * VZ(X)[s] (N x NA) * W[s] (NA x N)
+  void SigB(const double2 *vzx, const double2 *W, Blocks Sig, double f) {
+    GemmArgs g;
+    g.M = N; g.N = N; g.K = (int)NA; g.nb1 = nsl;
+    g.A = rowmajor(vzx, NA); g.A.bs1 = N2A;
+    g.B = rowmajor(W, N); g.B.bs1 = N2A;
+    g.C = blk(Sig, N);
+    g.alpha = make_double2(f, 0);
+    g.beta = make_double2(1.0, 0);
+    gemm(g, s);
+  }
+  // M[s] (+)= alpha * X_s (N x N) * VY[s] (N x (b,n))   -> [l][b][n]
+  void Mx(Blocks X, const double2 *vy, double2 *M, double alpha, bool acc) {
+    GemmArgs g;
+    g.M = N; g.N = (int)NA; g.K = N; g.nb1 = nsl;
+    g.A = blk(X, N);
+    g.B = rowmajor(vy, NA); g.B.bs1 = N2A;
+    g.C = rowmajor(M, NA); g.C.bs1 = N2A;
+    g.alpha = make_double2(alpha, 0);
+    g.beta = make_double2(acc ? 1.0 : 0.0, 0);
+    gemm(g, s);
+  }
+  // Exchange for units u0..u0+nu-1 of this chunk: Sigma_u -= sum_{l,a} V^a_il Q[l][j][a]
+  //   S[u][(l,n)][(q,j)] = sum_b M[u][l][b][n] V^b_qj ;  Q[u][j][l][a] = sum_{(n,q)} S[u][l][(n,q)][j] VZ(Z)[u][n][a][q]
+  void Exch(int nu, const double2 *M, const double2 *vzz, Blocks Sig, double2 *S, double2 *Q) {
+    {
+      GemmArgs g;
+      g.M = (int)es; g.N = (int)es; g.K = A; g.nb1 = nu;
+      g.A.p = M; g.A.rdiv = N; g.A.rs_hi = NA; g.A.rs_lo = 1; g.A.cs_lo = N; g.A.bs1 = N2A;
+      g.B = rowmajor(c.Vaij, es); g.b_cplx = false;
+      g.C = rowmajor(S, es); g.C.bs1 = es * es;
+      gemm(g, s);
+    }
+    {
+      GemmArgs g;
+      g.M = N; g.N = A; g.K = (int)es; g.nb1 = nu; g.nb2 = N;
+      g.A.p = S; g.A.rs_lo = 1; g.A.cs_lo = N; g.A.bs1 = es * es; g.A.bs2 = es * N;
+      g.B.p = vzz; g.B.rdiv = N; g.B.rs_hi = NA; g.B.rs_lo = 1; g.B.cs_lo = N; g.B.bs1 = N2A; g.B.bs2 = 0;
+      g.C.p = Q; g.C.rs_lo = NA; g.C.cs_lo = 1; g.C.bs1 = N2A; g.C.bs2 = A;
+      gemm(g, s);
+    }
+    {
+      GemmArgs g;
+      g.M = N; g.N = N; g.K = (int)NA; g.nb1 = nu;
+      g.A = rowmajor(c.Vija, NA); g.a_cplx = false;
+      g.B.p = Q; g.B.rs_lo = 1; g.B.cs_lo = NA; g.B.bs1 = N2A;
+      g.C = blk(Sig, N);
+      g.alpha = make_double2(-1.0, 0);
+      g.beta = make_double2(1.0, 0);
+      gemm(g, s);
+    }
+  }
+};
+
+void prep(Ctx &c, int mode, int nsl, const double2 *L0, i64 Ls, const double2 *R0, i64 Rs, double sgn,
+          double2 *out, i64 out_stride) {
+  int N = c.df_nao;
+  i64 tot = (i64)N * N * nsl;
+  int th = 256;
+  unsigned bl = (unsigned)std::min<i64>((tot + th - 1) / th, 65535LL * 8);
+  prep_kernel<<<bl, th, 0, c.stream>>>(mode, N, nsl, L0, Ls, R0, Rs, sgn, out, out_stride);
+  NEDY_CHECK_LAUNCH();
+}
+
+} // namespace
+
+// Chunk sizes: slices per chunk and exchange units per S buffer, from the workspace budget.
+static void chunking(const Ctx &c, int &chunk, int &sub) {
+  i64 N = c.df_nao, A = c.df_naux;
+  i64 n2a = N * N * A * 16;  // bytes of one [n][a][q] intermediate
+  i64 n4 = N * N * N * N * 16;
+  i64 budget = c.ws_budget;
+  // per slice (retarded, the largest): 5 VZ/VYt + 3 VY + 2 M + Q + 2 P/W + prep
+  i64 per = 13 * n2a + 2 * A * A * 16;
+  sub = (int)std::max<i64>(1, std::min<i64>(16, (budget / 3) / n4));
+  chunk = (int)std::max<i64>(1, std::min<i64>(64, (budget - sub * n4) / std::max<i64>(per, 1)));
+  if (chunk < sub) sub = chunk;
+}
+
+void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G) {
+  NEDY_REQUIRE(c.Vija != nullptr, "sigma_df: density-fitted tensor not set");
+  NEDY_REQUIRE(nspin == 1 || nspin == 2, "sigma_df: nspin must be 1 or 2");
+  const int N = c.df_nao, A = c.df_naux;
+  for (int s = 0; s < nspin; s++) {
+    NEDY_REQUIRE(G[s]->nao == N && Sig[s]->nao == N, "sigma_df: nao mismatch");
+    NEDY_REQUIRE(T >= 0 && T <= G[s]->nt && T <= Sig[s]->nt, "sigma_df: tstp out of range");
+    NEDY_REQUIRE(G[s]->ntau == Sig[s]->ntau && G[s]->sig == Sig[s]->sig, "sigma_df: shape mismatch");
+  }
+  const i64 es = (i64)N * N, N2A = es * A, NA = (i64)N * A;
+  const int ntau = G[0]->ntau, sig = G[0]->sig;
+  const double fb = nspin == 1 ? 2.0 : 1.0;
+  // set_tstp_zero (greens.h:76-86)
+  for (int s = 0; s < nspin; s++) {
+    NEDY_CUDA(cudaMemsetAsync(Sig[s]->retptr(T, 0), 0, sizeof(double2) * (T + 1) * es, c.stream));
+    NEDY_CUDA(cudaMemsetAsync(Sig[s]->lesptr(0, T), 0, sizeof(double2) * (T + 1) * es, c.stream));
+    NEDY_CUDA(cudaMemsetAsync(Sig[s]->tvptr(T, 0), 0, sizeof(double2) * (ntau + 1) * es, c.stream));
+  }
+  int chunk, sub;
+  chunking(c, chunk, sub);
+
+  // ---------------- lesser and mixed rows: one bubble unit + one exchange unit per slice
+  for (int kind = 0; kind < 2; kind++) {
+    const int nslices = kind == 0 ? T + 1 : ntau + 1;
+    for (int t0 = 0; t0 < nslices; t0 += chunk) {
+      const int nsl = std::min(chunk, nslices - t0);
+      c.ws.reset();
+      DF d(c, nsl);
+      double2 *Yb[2], *VZ[2], *VYt[2];
+      Blocks X[2];
+      for (int s = 0; s < nspin; s++) {
+        Yb[s] = c.ws.alloc<double2>(nsl * es);
+        if (kind == 0) {
+          X[s] = {G[s]->lesptr(t0, T), es};
+          prep(c, PREP_LES, nsl, G[s]->lesptr(t0, T), es, G[s]->retptr(T, t0), es, 0, Yb[s], 0);
+        } else {
+          X[s] = {G[s]->tvptr(T, t0), es};
+          prep(c, PREP_TV, nsl, G[s]->tvptr(T, ntau - t0), -es, nullptr, 0, -(double)sig, Yb[s], 0);
+        }
+        VZ[s] = c.ws.alloc<double2>(nsl * N2A);
+        VYt[s] = c.ws.alloc<double2>(nsl * N2A);
+        d.VZ(X[s], VZ[s]);
+        d.VYt({Yb[s], es}, VYt[s]);
+      }
+      double2 *P = c.ws.alloc<double2>((i64)nsl * A * A);
+      double2 *Wb = c.ws.alloc<double2>(nsl * N2A);
+      for (int s = 0; s < nspin; s++) d.P(VZ[s], VYt[s], P, 1.0, s > 0);
+      d.W(P, Wb);
+      for (int s = 0; s < nspin; s++) {
+        Blocks out = kind == 0 ? Blocks{Sig[s]->lesptr(t0, T), es} : Blocks{Sig[s]->tvptr(T, t0), es};
+        d.SigB(VZ[s], Wb, out, fb);
+      }
+      // exchange (per spin): M = X V Y, Z = X
+      double2 *VY = c.ws.alloc<double2>(nsl * N2A);
+      double2 *M = c.ws.alloc<double2>(nsl * N2A);
+      double2 *Q = c.ws.alloc<double2>(nsl * N2A);
+      double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
+      for (int s = 0; s < nspin; s++) {
+        d.VZ({Yb[s], es}, VY);
+        d.Mx(X[s], VY, M, 1.0, false);
+        Blocks out = kind == 0 ? Blocks{Sig[s]->lesptr(t0, T), es} : Blocks{Sig[s]->tvptr(T, t0), es};
+        for (int u0 = 0; u0 < nsl; u0 += sub) {
+          int nu = std::min(sub, nsl - u0);
+          d.Exch(nu, M + u0 * N2A, VZ[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
+        }
+      }
+    }
+  }
+
+  // ---------------- retarded row: two bubble units + two exchange units per slice
+  for (int t0 = 0; t0 <= T; t0 += chunk) {
+    const int nsl = std::min(chunk, T + 1 - t0);
+    c.ws.reset();
+    DF d(c, nsl);
+    double2 *D[2];  // per spin: 4 derived blocks per slice (L^+, R^+, R-L^+, L-R^+)
+    Blocks L[2], R[2], Lh[2], Rh[2], Zd[2], Y1[2];
+    double2 *vzZd[2], *vzLh[2], *vzR[2], *vytL[2], *vytRh[2];
+    for (int s = 0; s < nspin; s++) {
+      D[s] = c.ws.alloc<double2>(4 * nsl * es);
+      prep(c, PREP_RET, nsl, G[s]->lesptr(t0, T), es, G[s]->retptr(T, t0), es, 0, D[s], nsl * es);
+      L[s] = {G[s]->lesptr(t0, T), es};
+      R[s] = {G[s]->retptr(T, t0), es};
+      Lh[s] = {D[s], es};
+      Rh[s] = {D[s] + nsl * es, es};
+      Zd[s] = {D[s] + 2 * nsl * es, es};
+      Y1[s] = {D[s] + 3 * nsl * es, es};
+      vzZd[s] = c.ws.alloc<double2>(nsl * N2A);
+      vzLh[s] = c.ws.alloc<double2>(nsl * N2A);
+      vzR[s] = c.ws.alloc<double2>(nsl * N2A);
+      vytL[s] = c.ws.alloc<double2>(nsl * N2A);
+      vytRh[s] = c.ws.alloc<double2>(nsl * N2A);
+      d.VZ(Zd[s], vzZd[s]);
+      d.VZ(Lh[s], vzLh[s]);
+      d.VZ(R[s], vzR[s]);
+      d.VYt(L[s], vytL[s]);
+      d.VYt(Rh[s], vytRh[s]);
+    }
+    double2 *PA = c.ws.alloc<double2>((i64)nsl * A * A);
+    double2 *PB = c.ws.alloc<double2>((i64)nsl * A * A);
+    for (int s = 0; s < nspin; s++) {
+      d.P(vzZd[s], vytL[s], PA, 1.0, s > 0);
+      d.P(vzLh[s], vytRh[s], PB, 1.0, s > 0);
+      d.P(vzR[s], vytL[s], PB, -1.0, true);
+    }
+    double2 *WA = c.ws.alloc<double2>(nsl * N2A);
+    double2 *WB = c.ws.alloc<double2>(nsl * N2A);
+    d.W(PA, WA);
+    d.W(PB, WB);
+    for (int s = 0; s < nspin; s++) {
+      Blocks out = {Sig[s]->retptr(T, t0), es};
+      d.SigB(vzR[s], WA, out, fb);
+      d.SigB(vzLh[s], WB, out, fb);
+    }
+    // exchange units per spin
+    double2 *VY = c.ws.alloc<double2>(nsl * N2A);
+    double2 *M = c.ws.alloc<double2>(nsl * N2A);
+    double2 *Q = c.ws.alloc<double2>(nsl * N2A);
+    double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
+    for (int s = 0; s < nspin; s++) {
+      Blocks out = {Sig[s]->retptr(T, t0), es};
+      // unit 1: M = (-L^+) V (L - R^+), Z = R
+      d.VZ(Y1[s], VY);
+      d.Mx(Lh[s], VY, M, -1.0, false);
+      for (int u0 = 0; u0 < nsl; u0 += sub) {
+        int nu = std::min(sub, nsl - u0);
+        d.Exch(nu, M + u0 * N2A, vzR[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
+      }
+      // unit 2: M = R V L + (-L^+) V R^+, Z = R - L^+
+      d.VZ(L[s], VY);
+      d.Mx(R[s], VY, M, 1.0, false);
+      d.VZ(Rh[s], VY);
+      d.Mx(Lh[s], VY, M, -1.0, true);
+      for (int u0 = 0; u0 < nsl; u0 += sub) {
+        int nu = std::min(sub, nsl - u0);
+        d.Exch(nu, M + u0 * N2A, vzZd[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
+      }
+    }
+  }
+  (void)NA;
+}
+
+} // namespace nedy

@@ -1,0 +1,153 @@
+"""Seeded synthetic inputs and the equilibrium starting state.
+
+The reference reads molecular integrals from HDF5 and obtains its equilibrium
+state from the external gfmol Matsubara solver; here both come from seeded
+random numbers and a Hartree-Fock equilibrium, identical for the CUDA path and
+for the CPU oracle:
+
+* h0: symmetric N(0,1) matrix, upper half of the spectrum shifted so the gap at
+  half filling is >= ``gap``;
+* B^Q: symmetric N(0,1) matrices scaled so that ||U||_F = ``u_norm`` with
+  U_ijkl = sum_Q B^Q_ij B^Q_kl; Vija[i, j, Q] = B^Q_ij;
+* D: symmetric N(0,1) dipole matrix; drives E(t) gated to exactly 0 for
+  t <= k*dt (the bootstrap assumes a time-translation-invariant start,
+  reference src/molNEsim.cpp:38-49);
+* equilibrium: self-consistent restricted HF Fock matrix F and chemical
+  potential mu at mid-gap; G^M(tau) and the first k+1 time steps of G are the
+  free Green's function of F (G0_from_h0, reference src/dyson_free.h:226-297).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .greens import HostGF
+
+
+@dataclass
+class Problem:
+    nao: int
+    naux: int
+    h0: np.ndarray
+    Vija: np.ndarray
+    D: np.ndarray
+    seed: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def U(self):
+        return np.einsum("ija,kla->ijkl", self.Vija, self.Vija)
+
+    @property
+    def Uexch(self):
+        # Uexch(j,l,n,q) = 2 U(j,n,l,q) - U(j,l,n,q)   (reference tests/mol2bSolver-test.cpp:229-237)
+        U = self.U
+        return 2 * U.transpose(0, 2, 1, 3) - U
+
+
+def make_problem(nao: int, naux: int, seed: int, gap: float = 0.5, u_norm: float = 0.5) -> Problem:
+    rng = np.random.default_rng(seed)
+    a = rng.normal(size=(nao, nao))
+    h0 = 0.5 * (a + a.T)
+    w, v = np.linalg.eigh(h0)
+    nocc = nao // 2
+    if 0 < nocc < nao:
+        g = w[nocc] - w[nocc - 1]
+        if g < gap:
+            w[nocc:] += gap - g
+    h0 = (v * w) @ v.T
+    h0 = 0.5 * (h0 + h0.T)
+    B = rng.normal(size=(naux, nao, nao))
+    B = 0.5 * (B + B.transpose(0, 2, 1))
+    # ||U||_F^2 = sum_{QP} (tr B^Q B^P)^2  (B symmetric)
+    gram = np.einsum("qij,pij->qp", B, B)
+    nrm = math.sqrt((gram ** 2).sum())
+    B *= math.sqrt(u_norm / nrm)
+    Vija = np.ascontiguousarray(B.transpose(1, 2, 0))
+    d = rng.normal(size=(nao, nao))
+    D = 0.5 * (d + d.T)
+    return Problem(nao, naux, h0, Vija, D, seed)
+
+
+def drive(kind: str, t: float, k: int, dt: float, **kw) -> float:
+    """Amplitude E(t) of the external field along D, 0 for t <= k*dt."""
+    if t <= k * dt + 1e-12:
+        return 0.0
+    if kind == "sin":
+        return kw.get("E0", 0.1) * math.sin(kw.get("omega", 2.0) * t)
+    if kind == "gauss":
+        E0, t0, s = kw.get("E0", 0.05), kw.get("t0", 2.0), kw.get("sigma", 0.5)
+        return E0 * math.exp(-0.5 * ((t - t0) / s) ** 2)
+    if kind == "none":
+        return 0.0
+    raise ValueError(kind)
+
+
+def fermi(beta, w):
+    x = beta * np.asarray(w, float)
+    out = np.empty_like(x)
+    big = np.abs(x) > 100
+    out[big] = np.where(x[big] > 0, 0.0, 1.0)
+    out[~big] = 1.0 / (1.0 + np.exp(x[~big]))
+    return out
+
+
+def fermi_exp(beta, tau, w):
+    w = np.asarray(w, float)
+    return np.where(w < 0, np.exp(w * tau) * fermi(beta, w), np.exp((tau - beta) * w) * fermi(beta, -w))
+
+
+def hf_fock(p: Problem, rho: np.ndarray) -> np.ndarray:
+    """h0 + 2J - K for the restricted density rho (molHFSolverDecomp::solve_HF, molHFSolver.cpp:81-110)."""
+    V = p.Vija
+    X = np.einsum("kl,kla->a", rho, V)
+    J = np.einsum("ija,a->ij", V, X)
+    K = np.einsum("ila,kl,kja->ij", V, rho, V)
+    return p.h0 + 2 * J - K
+
+
+def hf_equilibrium(p: Problem, beta: float, iters: int = 200, tol: float = 1e-13):
+    """Self-consistent restricted HF at inverse temperature beta, mu at mid-gap."""
+    N = p.nao
+    nocc = N // 2
+    F = p.h0.astype(complex)
+    mu = 0.0
+    for _ in range(iters):
+        w, v = np.linalg.eigh(F)
+        mu = 0.5 * (w[nocc - 1] + w[nocc]) if 0 < nocc < N else float(w.mean())
+        rho = (v * fermi(beta, w - mu)) @ v.conj().T
+        Fn = hf_fock(p, rho)
+        d = np.abs(Fn - F).max()
+        F = Fn
+        if d < tol:
+            break
+    F = 0.5 * (F + F.conj().T)
+    return F.real.copy(), mu
+
+
+def g0_from_h0(G: HostGF, x: np.ndarray, mu: float, H0: np.ndarray, beta: float, dt: float, k: int,
+               with_matsubara: bool = True):
+    """Free Green's function of a constant Hamiltonian (dyson::G0_from_h0, reference src/dyson_free.h:226-297),
+    fermions (sig = -1); fills G^M (optional), G^tv(0..k,.), G^R and G^< on [0,k]^2."""
+    N = G.nao
+    Hmu = mu * np.eye(N) - H0
+    ev, U = np.linalg.eigh(Hmu)
+    evm = -ev
+    Udt = (U * np.exp(1j * dt * ev)) @ U.conj().T
+    Ut = [np.eye(N, dtype=complex)]
+    for n in range(1, k + 1):
+        Ut.append(Ut[-1] @ Udt)
+    taus = beta / 2.0 * (np.asarray(x) + 1.0)
+    for m, tau in enumerate(taus):
+        if with_matsubara:
+            G.mat[m] = -(U * fermi_exp(beta, tau, ev)) @ U.conj().T
+        core = (U * fermi_exp(beta, tau, evm)) @ U.conj().T
+        for n in range(k + 1):
+            G.tv[n, m] = 1j * Ut[n] @ core
+    val = (U * fermi(beta, evm)) @ U.conj().T
+    for m in range(k + 1):
+        for n in range(m + 1):
+            G.retblk(m, n)[:] = -1j * Ut[m] @ Ut[n].conj().T
+            G.lesblk(n, m)[:] = 1j * Ut[n] @ val @ Ut[m].conj().T

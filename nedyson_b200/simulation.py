@@ -1,0 +1,78 @@
+"""Simulation drivers over the engine (host orchestration of the C ABI).
+
+``DecompSimulation`` mirrors the reference's restricted density-fitted driver
+(src/molNEsim_decomp_impl.h): ``free_gf`` + ``do_boot`` (:62-82) + ``do_tstp``
+(:85-104); ``DecompSpinSimulation`` the unrestricted one
+(src/molNEsim_decomp_spin_impl.h:70-122).  The equilibrium state is the
+Hartree-Fock one of ``inputs.hf_equilibrium`` (the reference takes it from the
+external gfmol solver), and the external drive E(t) D is added to h0 inside
+h(t), gated to zero during the bootstrap window.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import api
+from .greens import HostGF
+from .inputs import Problem, drive, g0_from_h0, hf_equilibrium
+
+
+class DecompSimulation:
+    def __init__(self, p: Problem, nt: int, ntau: int, beta: float, dt: float, k: int = 5,
+                 corr_steps: int = 5, drive_kind: str = "none", drive_kw: dict | None = None, device: int = 0,
+                 workspace_bytes: int = 0):
+        self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k
+        self.corr_steps = corr_steps
+        self.drive_kind, self.drive_kw = drive_kind, dict(drive_kw or {})
+        self.ctx = api.Context(nt, ntau, p.nao, k, beta, dt, device, workspace_bytes)
+        self.x, self.w = self.ctx.collocation()
+        N = p.nao
+        self.G = api.green_func(self.ctx, nt, ntau, N, -1)
+        self.Sigma = api.green_func(self.ctx, nt, ntau, N, -1)
+        self.solver = api.molGF2SolverDecomp(self.ctx, p.Vija)
+        self.dyson = api.dyson(self.ctx)
+        self.hmf = api.hmf_buffer(self.ctx, N)
+        self.ht = api.DeviceBuffer(self.ctx, N * N * 16)
+        self.F, self.mu = hf_equilibrium(p, beta)
+        self.boot_err = None
+
+    def h_of_t(self, t: int) -> np.ndarray:
+        E = drive(self.drive_kind, t * self.dt, self.k, self.dt, **self.drive_kw)
+        return (self.p.h0 + E * self.p.D).astype(np.complex128)
+
+    def initial_state(self) -> HostGF:
+        g = HostGF(self.nt, self.ntau, self.p.nao, -1)
+        g0_from_h0(g, self.x, self.mu, self.F, self.beta, self.dt, self.k)
+        return g
+
+    def free_gf(self):
+        self.G.from_host(self.initial_state())
+        hm = np.zeros((self.nt + 1, self.p.nao, self.p.nao), np.complex128)
+        hm[: self.k + 1] = self.F
+        self.hmf.upload(hm)
+
+    def do_boot(self, max_iter: int = 50, tol: float = 1e-12) -> float:
+        err = None
+        for _ in range(max_iter + 1):
+            for t in range(self.k + 1):
+                self.solver.solve(t, self.Sigma, self.G)
+            err = self.dyson.dyson_start(self.G, self.Sigma, self.hmf, self.mu)
+            if err < tol:
+                break
+        self.boot_err = err
+        return err
+
+    def do_tstp(self, t: int) -> float:
+        self.ht.upload(self.h_of_t(t))
+        import ctypes as C
+        from ._lib import check, lib
+        e = C.c_double()
+        check(lib().nedy_decomp_tstp(self.ctx.h, t, self.G.h, self.Sigma.h, self.hmf.h, self.ht.h, self.mu,
+                                     self.corr_steps, C.byref(e)))
+        return e.value
+
+    def run(self, nt: int | None = None, boot_iter: int = 50, boot_tol: float = 1e-12):
+        self.free_gf()
+        self.do_boot(boot_iter, boot_tol)
+        for t in range(self.k + 1, (nt if nt is not None else self.nt) + 1):
+            self.do_tstp(t)

@@ -1,0 +1,54 @@
+"""Oracle-side simulation driver used by the parity tests (test infrastructure).
+
+Same initial state and the same do_boot / do_tstp sequence as
+``nedyson_b200.simulation.DecompSimulation`` (reference
+src/molNEsim_decomp_impl.h:62-104), on the CPU oracle.
+"""
+import numpy as np
+
+from oracle import pyoracle as po
+from nedyson_b200.greens import HostGF
+from nedyson_b200.inputs import Problem, drive, g0_from_h0, hf_equilibrium
+
+
+class OracleDecompSim:
+    def __init__(self, p: Problem, nt, ntau, beta, dt, k=5, corr_steps=5, drive_kind="none", drive_kw=None):
+        self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k
+        self.corr_steps = corr_steps
+        self.drive_kind, self.drive_kw = drive_kind, dict(drive_kw or {})
+        self.dy = po.Dyson(nt, ntau, p.nao, k)
+        self.df = po.DF(p.Vija)
+        self.x, _ = po.colloc_nodes(ntau)
+        self.F, self.mu = hf_equilibrium(p, beta)
+        self.G = HostGF(nt, ntau, p.nao, -1)
+        self.S = HostGF(nt, ntau, p.nao, -1)
+        self.hmf = np.zeros((nt + 1, p.nao, p.nao), np.complex128)
+
+    def h_of_t(self, t):
+        E = drive(self.drive_kind, t * self.dt, self.k, self.dt, **self.drive_kw)
+        return (self.p.h0 + E * self.p.D).astype(np.complex128)
+
+    def free_gf(self):
+        g0_from_h0(self.G, self.x, self.mu, self.F, self.beta, self.dt, self.k)
+        self.hmf[: self.k + 1] = self.F
+
+    def do_boot(self, max_iter=50, tol=1e-12):
+        err = None
+        for _ in range(max_iter + 1):
+            for t in range(self.k + 1):
+                self.df.solve(t, self.S, self.G)
+            err = self.dy.dyson_start(self.G, self.S, self.hmf, self.mu, self.beta, self.dt)
+            if err < tol:
+                break
+        return err
+
+    def do_tstp(self, t):
+        self.dy.extrapolate(t, self.G)
+        e = None
+        for _ in range(self.corr_steps):
+            rho = self.G.get_dm(t)
+            self.hmf[t] = self.h_of_t(t)
+            self.df.hf(self.hmf[t], rho)
+            self.df.solve(t, self.S, self.G)
+            e, _ = self.dy.dyson_step(t, self.G, self.S, self.hmf, self.mu, self.beta, self.dt)
+        return e
