@@ -1,0 +1,421 @@
+#!/usr/bin/env python
+"""GF2 Kadanoff-Baym time steps per second at nao=64, naux=256 (plain FP64 path).
+
+One "step" is one full time step T of the restricted density-fitted GF2
+simulation (DecompSimulation::do_tstp, reference src/molNEsim_decomp_impl.h:85-104):
+the polynomial predictor followed by corr_steps x [density matrix, HF mean
+field, GF2 self-energy row T, Dyson step row T], through the C ABI.
+
+Workload: nao=64, naux=256, ntau=256, beta=20, k=5, dt=0.01, 5 corrector
+iterations, steps T = t0+W ... t0+W+K-1 on a synthetic pre-evolved state (the
+free propagation of the Hartree-Fock Fock matrix on rows 0..t0-1, a scaled copy
+of it as the self-energy history; seeded inputs, no dataset).  The history
+arrays (GBs) are far larger than L2, so no explicit flush is needed.
+
+Multi-GPU: one independent trajectory per GPU (replicas, no collective);
+value = total time steps of all ranks / max-over-ranks time.
+
+--impl reference times the CPU restatement of the reference solver (oracle/)
+on the host cores on a bounded sample and reports the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "GF2 timesteps/s, nao=64 naux=256: plain FP64 vs split+predictor at 1e-8"
+
+
+def flops_sigma(T, N, A, ntau):
+    """Algorithmic flops of one GF2 self-energy row (reference contraction order)."""
+    nt1 = ntau + 1
+    return (T + 1) * (128 * N**3 * A + 44 * A * A * N * N + 36 * N**4 * A) + \
+        nt1 * (36 * N**3 * A + 12 * A * A * N * N + 12 * N**4 * A)
+
+
+def flops_dyson(T, N, ntau):
+    """Flops of one Dyson step (history integrals, sweeps, mixing with the tau kernel)."""
+    nt1 = ntau + 1
+    return 8 * N**3 * (T * (T + 1) / 2 + (T + 1) ** 2 + T * T / 2 + 2 * (T + 1) * nt1 + nt1 + nt1 * nt1)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--nao", type=int, default=64)
+    ap.add_argument("--naux", type=int, default=256)
+    ap.add_argument("--ntau", type=int, default=256)
+    ap.add_argument("--t0", type=int, default=100)
+    ap.add_argument("--corr", type=int, default=5)
+    ap.add_argument("--beta", type=float, default=20.0)
+    ap.add_argument("--dt", type=float, default=0.01)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed
+class Dist:
+    def __init__(self, n):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU sample (oracle)
+def cpu_sample(args, target_seconds=20.0):
+    """Time the CPU restatement of the reference on a bounded sample and scale to one step at T.
+
+    Sample: one GF2 self-energy row at (nao, naux) with small T_s / ntau_s (enough slices for
+    every core), and one Dyson step at T_d = 24, ntau_d = 16; each is scaled to the bench
+    step by the flop models above (time per flop assumed constant)."""
+    from oracle import pyoracle as po
+    from nedyson_b200.greens import HostGF
+    from nedyson_b200.inputs import make_problem, hf_equilibrium, free_history
+    # every OpenMP thread holds one nao^4 exchange intermediate (268 MB at nao = 64): cap the threads
+    cores = min(os.cpu_count() or 1, 32)
+    po.set_threads(cores)
+    N, A = args.nao, args.naux
+    p = make_problem(N, A, args.seed)
+    rng = np.random.default_rng(1)
+    ntau_s = 8
+    T_s = max(2, (cores - ntau_s - 1 + 1) // 2)
+    G = HostGF(T_s, ntau_s, N, -1)
+    for a in (G.les, G.ret, G.tv):
+        a[:] = 0.05 * (rng.uniform(-1, 1, a.shape) + 1j * rng.uniform(-1, 1, a.shape))
+    S = HostGF(T_s, ntau_s, N, -1)
+    df = po.DF(p.Vija)
+    t0 = time.perf_counter()
+    df.solve(T_s, S, G)
+    ts = time.perf_counter() - t0
+    rate_s = flops_sigma(T_s, N, A, ntau_s) / ts
+    # Dyson sample
+    T_d, ntau_d = 24, 16
+    F, mu = hf_equilibrium(p, args.beta)
+    x, _ = po.colloc_nodes(ntau_d)
+    Gd = HostGF(T_d, ntau_d, N, -1)
+    les, ret, tv, mat = free_history(T_d, T_d + 1, ntau_d, x, mu, F, args.beta, args.dt)
+    Gd.les[:] = les
+    Gd.ret[:] = ret
+    Gd.tv[:] = tv
+    Gd.mat[:] = mat
+    Sd = HostGF(T_d, ntau_d, N, -1)
+    Sd.les[:] = 0.02 * les
+    Sd.ret[:] = 0.02 * ret
+    Sd.tv[:] = 0.02 * tv
+    hmf = np.repeat(F[None].astype(complex), T_d + 1, axis=0)
+    dy = po.Dyson(T_d, ntau_d, N, 5)
+    dy.mixing(Sd.tv[0], Gd.mat, args.beta, -1.0)  # builds the tau kernel outside the timing
+    t0 = time.perf_counter()
+    dy.dyson_step(T_d, Gd, Sd, hmf, mu, args.beta, args.dt)
+    td = time.perf_counter() - t0
+    rate_d = flops_dyson(T_d, N, ntau_d) / td
+    return dict(cores=cores, T_s=T_s, ntau_s=ntau_s, sigma_s=ts, rate_sigma=rate_s, T_d=T_d, ntau_d=ntau_d,
+                dyson_s=td, rate_dyson=rate_d)
+
+
+def cpu_step_seconds(smp, T, args):
+    return args.corr * (flops_sigma(T, args.nao, args.naux, args.ntau) / smp["rate_sigma"] +
+                        flops_dyson(T, args.nao, args.ntau) / smp["rate_dyson"])
+
+
+def cpu_baseline_obj(smp, value, args):
+    return {"value": value, "unit": "timesteps/s", "cores": smp["cores"], "kind": "port",
+            "sample": (f"oracle (C++ restatement, OpenMP over slices, OpenBLAS) timed on one GF2 self-energy row "
+                       f"at nao={args.nao}, naux={args.naux}, T={smp['T_s']}, ntau={smp['ntau_s']} "
+                       f"({smp['sigma_s']:.2f} s, {smp['rate_sigma'] / 1e9:.1f} GFLOP/s) and one Dyson step at "
+                       f"T={smp['T_d']}, ntau={smp['ntau_d']} ({smp['dyson_s']:.2f} s, "
+                       f"{smp['rate_dyson'] / 1e9:.1f} GFLOP/s), scaled by the flop model to one "
+                       f"{args.corr}-iteration step at T={args.t0 + args.warmup}, ntau={args.ntau}")}
+
+
+# ------------------------------------------------------------------ peaks
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_gemm_peak(device: int) -> float:
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s), burst: torch.matmul float64 8192^3, best of 5."""
+    import torch
+    dev = torch.device(f"cuda:{device}")
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2 * n**3 / best / 1e12
+
+
+# ------------------------------------------------------------------ engine arm
+def run_engine(args, dist: Dist):
+    import torch
+    from nedyson_b200 import api
+    from nedyson_b200._lib import LES, RET, TV, MAT, check, lib
+    from nedyson_b200.greens import tri
+    from nedyson_b200.inputs import make_problem, hf_equilibrium, free_history, drive
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    N, A, ntau, K, W = args.nao, args.naux, args.ntau, args.steps, args.warmup
+    t_first = args.t0
+    nt = t_first + W + K
+    p = make_problem(N, A, args.seed + dist.rank)
+    F, mu = hf_equilibrium(p, args.beta)
+    ctx = api.Context(nt, ntau, N, 5, args.beta, args.dt, device=dev)
+    x, _ = ctx.collocation()
+    G = api.green_func(ctx, nt, ntau, N, -1)
+    S = api.green_func(ctx, nt, ntau, N, -1)
+    les, ret, tv, mat = free_history(nt, t_first, ntau, x, mu, F, args.beta, args.dt)
+    G.upload(LES, 0, les)
+    G.upload(RET, 0, ret)
+    G.upload(TV, 0, tv)
+    G.upload(MAT, 0, mat)
+    S.upload(LES, 0, 0.02 * les)
+    S.upload(RET, 0, 0.02 * ret)
+    S.upload(TV, 0, 0.02 * tv)
+    del les, ret, tv
+    solver = api.molGF2SolverDecomp(ctx, p.Vija)
+    hm = np.zeros((nt + 1, N, N), np.complex128)
+    hm[:t_first] = F
+    hmf = api.hmf_buffer(ctx, N, hm)
+    # one-body Hamiltonian of every step, resident on the device (drive: 0.1 sin(2t) along D)
+    hts = [api.DeviceBuffer.from_array(ctx, (p.h0 + drive("sin", t * args.dt, 5, args.dt) * p.D).astype(np.complex128))
+           for t in range(nt + 1)]
+    # pinned host buffers for the end-to-end pass: h(t) in, new G row out
+    row_blocks = 2 * (nt + 1) + (ntau + 1)
+    h_host = torch.empty((N, N), dtype=torch.complex128).pin_memory()
+    row_host = torch.empty((row_blocks, N, N), dtype=torch.complex128).pin_memory()
+    ht_e2e = api.DeviceBuffer(ctx, N * N * 16)
+    sp = C.c_void_p()
+    check(lib().nedy_ctx_stream(ctx.h, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device(f"cuda:{dev}"))
+
+    def step(t):
+        e = C.c_double()
+        check(lib().nedy_decomp_tstp(ctx.h, t, G.h, S.h, hmf.h, hts[t].h, mu, args.corr, C.byref(e)))
+        return e.value
+
+    for t in range(t_first, t_first + W):
+        step(t)
+    ctx.synchronize()
+    check(lib().nedy_ctx_set_timing(ctx.h, 1))
+    clocks = Clocks(dev) if dist.rank == 0 else None
+    n0 = lib().nedy_launch_count()
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    T_timed = list(range(t_first + W, t_first + W + K))
+    for t in T_timed:
+        step(t)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    secs = e0.elapsed_time(e1) / 1e3
+    launches = int(lib().nedy_launch_count() - n0)
+    ms4 = (C.c_double * 4)()
+    check(lib().nedy_ctx_phase_times(ctx.h, ms4))
+    check(lib().nedy_ctx_set_timing(ctx.h, 0))
+    clk = clocks.stop() if clocks else None
+    secs_max = dist.max(secs)
+
+    # end-to-end pass through the C ABI with host buffers: re-run the last timed step T_e
+    # (rows are recomputed in place), copying h(T_e) from pinned host memory in and the new
+    # G row (les column, ret row, tv row) back out, all inside the timed region.
+    T_e = T_timed[-1]
+    hval = (p.h0 + drive("sin", T_e * args.dt, 5, args.dt) * p.D).astype(np.complex128)
+    h_host.copy_(torch.from_numpy(hval))
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    ee0.record(stream)
+    check(lib().nedy_buf_upload(ht_e2e.h, 0, N * N * 16, C.c_void_p(h_host.data_ptr())))
+    e = C.c_double()
+    check(lib().nedy_decomp_tstp(ctx.h, T_e, G.h, S.h, hmf.h, ht_e2e.h, mu, args.corr, C.byref(e)))
+    base = row_host.data_ptr()
+    es = N * N * 16
+    check(lib().nedy_gf_download(G.h, LES, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base)))
+    check(lib().nedy_gf_download(G.h, RET, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base + (T_e + 1) * es)))
+    check(lib().nedy_gf_download(G.h, TV, T_e * (ntau + 1), ntau + 1, C.c_void_p(base + 2 * (T_e + 1) * es)))
+    ee1.record(stream)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    e2e_secs = dist.max(ee0.elapsed_time(ee1) / 1e3)
+    h2d = N * N * 16
+    d2h = (2 * (T_e + 1) + ntau + 1) * es
+    rowmax = float(np.abs(row_host.numpy()).max())
+
+    out = dict(secs=secs_max, launches=launches, phase_ms=list(ms4), clocks=clk, T=T_timed, e2e_secs=e2e_secs,
+               h2d=h2d, d2h=d2h, rowmax=rowmax, err=e.value)
+    ctx.close()
+    return out
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    K, W = args.steps, args.warmup
+    cfg = {"workload": f"restricted density-fitted GF2 time step, nao={args.nao} naux={args.naux} ntau={args.ntau} "
+                       f"beta={args.beta} k=5 dt={args.dt}, {args.corr} corrector iterations, steps T={args.t0 + W}.."
+                       f"{args.t0 + W + K - 1} on a pre-evolved synthetic state",
+           "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "t_window": [args.t0 + W, args.t0 + W + K - 1],
+           "corr_steps": args.corr, "precision": "fp64", "predictor": "polynomial extrapolation (k=5)",
+           "l2": "inputs (G, Sigma histories) larger than L2; no flush needed",
+           "parallelism": f"replicas x{dist.world}"}
+    if args.impl == "reference":
+        if dist.rank != 0:
+            dist.close()
+            return
+        samples = []
+        for i in range(W + K):
+            smp = cpu_sample(args)
+            if i >= W:
+                samples.append(smp)
+        T_mid = args.t0 + W
+        step_s = float(np.mean([cpu_step_seconds(s, T_mid, args) for s in samples]))
+        value = 1.0 / step_s
+        line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": 0, "steps": K, "warmup": W,
+                "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "complex128", "data": "synthetic (seeded)", "config": cfg, "impl": "reference",
+                "cpu_baseline": cpu_baseline_obj(samples[-1], value, args),
+                "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        dist.close()
+        return
+
+    r = run_engine(args, dist)
+    total_steps = K * dist.world
+    value = total_steps / r["secs"]
+    T_mid = r["T"][len(r["T"]) // 2]
+    # roofline of the dominant kernel (the self-energy row): algorithmic flops / device time
+    sig_ms = r["phase_ms"][2]
+    sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau) for t in r["T"]) * args.corr
+    achieved = sig_flops / (sig_ms / 1e3) / 1e12 if sig_ms > 0 else None
+    peaks, src = measured_peaks()
+    line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": dist.world, "steps": K, "warmup": W,
+            "ms_per_step": r["secs"] / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "complex128", "data": "synthetic (seeded random h0, B^Q, dipole; free-propagation history)",
+            "config": cfg}
+    if dist.rank == 0:
+        fp64 = fp64_gemm_peak(dist.local)
+        line["roofline"] = {"bound": "tensor", "kernel": "GF2 self-energy row (FP64 DMMA GEMM chain)",
+                            "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                            "frac": (achieved / fp64) if achieved else None, "traffic": None,
+                            "peak_source": "measured: cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU",
+                            "bf16_peak_tflops": peaks.get("bf16_tflops"), "bf16_peak_source": src,
+                            "algorithmic_flops_per_step": flops_sigma(T_mid, args.nao, args.naux, args.ntau) * args.corr}
+        line["phase_ms"] = {"predictor": r["phase_ms"][0], "mean_field": r["phase_ms"][1],
+                            "self_energy": r["phase_ms"][2], "dyson": r["phase_ms"][3]}
+        line["clocks"] = r["clocks"]
+        line["gpu_launches"] = r["launches"]
+        line["e2e"] = {"value": dist.world / r["e2e_secs"], "unit": "timesteps/s", "h2d_bytes_per_step": r["h2d"],
+                       "d2h_bytes_per_step": r["d2h"]}
+        if dist.world == 1 and not args.no_cpu_baseline:
+            smp = cpu_sample(args)
+            v = 1.0 / cpu_step_seconds(smp, T_mid, args)
+            line["cpu_baseline"] = cpu_baseline_obj(smp, v, args)
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -65,6 +65,14 @@ const char *nedy_last_error(void);
 int nedy_ctx_create(const nedy_config *cfg, nedy_ctx **out);
 int nedy_ctx_destroy(nedy_ctx *ctx);
 int nedy_ctx_synchronize(nedy_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), e.g. to record events around calls. */
+int nedy_ctx_stream(nedy_ctx *ctx, void **stream);
+/* Per-phase device timing of nedy_decomp_tstp / nedy_decomp_spin_tstp (CUDA events):
+ * ms4 = accumulated milliseconds of predictor, mean field, self-energy, Dyson step. */
+int nedy_ctx_set_timing(nedy_ctx *ctx, int on);
+int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
+/* Number of engine kernel launches issued by this process so far. */
+unsigned long long nedy_launch_count(void);
 /* Collocation nodes x_m in [-1,1] and weights (ntau+1 values each). */
 int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w);
 

@@ -39,6 +39,10 @@ SIGNATURES = {
     "nedy_ctx_destroy": ([_P], _I),
     "nedy_ctx_synchronize": ([_P], _I),
     "nedy_collocation_nodes": ([_P, _DP, _DP], _I),
+    "nedy_ctx_stream": ([_P, _PP], _I),
+    "nedy_ctx_set_timing": ([_P, _I], _I),
+    "nedy_ctx_phase_times": ([_P, _DP], _I),
+    "nedy_launch_count": ([], C.c_ulonglong),
     "nedy_gf_create": ([_P, _I, _I, _I, _I, _PP], _I),
     "nedy_gf_destroy": ([_P], _I),
     "nedy_gf_upload": ([_P, _I, _LL, _LL, _P], _I),

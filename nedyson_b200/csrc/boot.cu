@@ -283,6 +283,7 @@ double energy_conv(Ctx &c, int T, const DevGF &Sig, const DevGF &G) {
   double *out = c.ws.alloc<double>(4);
   NEDY_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * 4, c.stream));
   energy_hist_kernel<<<top + 1, TPB, 0, c.stream>>>(N, T, top, Sig, G, c.greg + (i64)T * (c.nt + 1), out);
+  NEDY_CHECK_LAUNCH();
   energy_tv_kernel<<<nblk((i64)N * N), TPB, 0, c.stream>>>(N, T, Sig, G, c.d_w, c.d_u, c.col.ctop, out);
   NEDY_CHECK_LAUNCH();
   double h[4];

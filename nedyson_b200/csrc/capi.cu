@@ -22,6 +22,35 @@ struct nedy_buf {
 
 namespace nedy {
 
+unsigned long long g_launches = 0;
+
+// Optional per-phase device timing of the whole-step entry points (CUDA events
+// on the engine stream): predictor, mean field, self-energy, Dyson step.
+struct PhaseTimer {
+  Ctx &c;
+  std::vector<std::pair<int, cudaEvent_t>> marks;
+  explicit PhaseTimer(Ctx &cx) : c(cx) {}
+  void mark(int phase) {
+    if (!c.timing) return;
+    cudaEvent_t e;
+    NEDY_CUDA(cudaEventCreate(&e));
+    NEDY_CUDA(cudaEventRecord(e, c.stream));
+    marks.push_back({phase, e});
+  }
+  // phase p runs from its mark to the next mark
+  void collect() {
+    if (!c.timing || marks.empty()) return;
+    NEDY_CUDA(cudaEventSynchronize(marks.back().second));
+    for (size_t i = 0; i + 1 < marks.size(); i++) {
+      float ms = 0;
+      NEDY_CUDA(cudaEventElapsedTime(&ms, marks[i].second, marks[i + 1].second));
+      if (marks[i].first >= 0 && marks[i].first < 4) c.phase_ms[marks[i].first] += ms;
+    }
+    for (auto &m : marks) cudaEventDestroy(m.second);
+    marks.clear();
+  }
+};
+
 Arena::~Arena() {
   for (auto &b : blocks_) cudaFree(b.p);
 }
@@ -176,7 +205,7 @@ int nedy_ctx_create(const nedy_config *cfg, nedy_ctx **out) {
     if (cfg->workspace_bytes > 0) c.ws_budget = cfg->workspace_bytes;
     try {
       NEDY_CUDA(cudaSetDevice(c.device));
-      NEDY_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+      NEDY_CUDA(cudaStreamCreate(&c.stream));
       c.W = make_weights(c.k);
       c.col = make_colloc(c.ntau);
     } catch (...) {
@@ -203,6 +232,30 @@ int nedy_ctx_synchronize(nedy_ctx *ctx) {
   });
 }
 
+int nedy_ctx_stream(nedy_ctx *ctx, void **stream) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && stream, "null argument");
+    *stream = (void *)ctx->c.stream;
+  });
+}
+
+int nedy_ctx_set_timing(nedy_ctx *ctx, int on) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null context");
+    ctx->c.timing = on != 0;
+    for (double &v : ctx->c.phase_ms) v = 0;
+  });
+}
+
+int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && ms4, "null argument");
+    for (int i = 0; i < 4; i++) ms4[i] = ctx->c.phase_ms[i];
+  });
+}
+
+unsigned long long nedy_launch_count(void) { return g_launches; }
+
 int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w) {
   return guard([&] {
     NEDY_REQUIRE(ctx, "null context");
@@ -228,7 +281,7 @@ int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **
         p = nullptr;
         throw CudaError(std::string("green_func allocation failed: ") + cudaGetErrorString(e));
       }
-      NEDY_CUDA(cudaMemset(p, 0, sizeof(double2) * nblk * d.es));
+      memset_sync(p, sizeof(double2) * nblk * d.es, ctx->c.stream);
     };
     try {
       alloc(d.mat, ntau + 1);
@@ -328,7 +381,7 @@ int nedy_buf_create(nedy_ctx *ctx, long long bytes, nedy_buf **out) {
       delete b;
       throw CudaError(std::string("buffer allocation failed: ") + cudaGetErrorString(e));
     }
-    NEDY_CUDA(cudaMemset(b->p, 0, bytes));
+    memset_sync(b->p, bytes, ctx->c.stream);
     *out = b;
   });
 }
@@ -386,7 +439,7 @@ int nedy_set_df_tensor(nedy_ctx *ctx, const double *Vija, int nao, int naux) {
     auto put = [&](double *&d, const double *h) {
       if (d) cudaFree(d);
       NEDY_CUDA(cudaMalloc(&d, sizeof(double) * n));
-      NEDY_CUDA(cudaMemcpy(d, h, sizeof(double) * n, cudaMemcpyHostToDevice));
+      h2d_sync(d, h, sizeof(double) * n, c.stream);
     };
     put(c.Vija, Vija);
     put(c.Viaj, viaj.data());
@@ -407,8 +460,8 @@ int nedy_set_full_tensor(nedy_ctx *ctx, const double *U, const double *Uexch, in
     if (c.Uexch) cudaFree(c.Uexch);
     NEDY_CUDA(cudaMalloc(&c.U, sizeof(double) * n));
     NEDY_CUDA(cudaMalloc(&c.Uexch, sizeof(double) * n));
-    NEDY_CUDA(cudaMemcpy(c.U, U, sizeof(double) * n, cudaMemcpyHostToDevice));
-    NEDY_CUDA(cudaMemcpy(c.Uexch, Uexch, sizeof(double) * n, cudaMemcpyHostToDevice));
+    h2d_sync(c.U, U, sizeof(double) * n, c.stream);
+    h2d_sync(c.Uexch, Uexch, sizeof(double) * n, c.stream);
     c.u_nao = nao;
   });
 }
@@ -543,10 +596,13 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
     NEDY_REQUIRE(h_t->bytes >= es * 16, "h_t buffer too small");
     double2 *hT = hmf_row(hmf, ctx, tstp, N);
     hmf_row(hmf, ctx, G->g.nt, N);
+    PhaseTimer pt(c);
+    pt.mark(0);
     extrapolate(c, tstp, G->g);
     double e[3] = {0, 0, 0};
     for (int it = 0; it < corr_steps; it++) {
       c.ws.reset();
+      pt.mark(1);
       double2 *rho = c.ws.alloc<double2>(es);
       get_dm(c, G->g, tstp, rho);
       NEDY_CUDA(cudaMemcpyAsync(hT, h_t->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
@@ -554,10 +610,14 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
       hf_decomp(c, 1, h, rho);
       DevGF *Ss[1] = {&S->g};
       const DevGF *Gs[1] = {&G->g};
+      pt.mark(2);
       sigma_df(c, tstp, 1, Ss, Gs);
+      pt.mark(3);
       dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
     }
+    pt.mark(-1);
     NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    pt.collect();
     if (err) *err = e[0] + e[1] + e[2];
   });
 }
@@ -573,11 +633,14 @@ int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *Gu, nedy_gf *Gd, ned
     const int N = Gu->g.nao;
     const i64 es = (i64)N * N;
     double2 *hT[2] = {hmf_row(hu, ctx, tstp, N), hmf_row(hd, ctx, tstp, N)};
+    PhaseTimer pt(c);
+    pt.mark(0);
     extrapolate(c, tstp, Gu->g);
     extrapolate(c, tstp, Gd->g);
     double eu[3] = {0, 0, 0}, ed[3] = {0, 0, 0};
     for (int it = 0; it < corr_steps; it++) {
       c.ws.reset();
+      pt.mark(1);
       double2 *rho = c.ws.alloc<double2>(2 * es);
       get_dm(c, Gu->g, tstp, rho);
       get_dm(c, Gd->g, tstp, rho + es);
@@ -586,11 +649,15 @@ int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *Gu, nedy_gf *Gd, ned
       hf_decomp(c, 2, hT, rho);
       DevGF *Ss[2] = {&Su->g, &Sd->g};
       const DevGF *Gs[2] = {&Gu->g, &Gd->g};
+      pt.mark(2);
       sigma_df(c, tstp, 2, Ss, Gs);
+      pt.mark(3);
       dyson_step(c, tstp, Gu->g, Su->g, (const double2 *)hu->p, mu_up, eu);
       dyson_step(c, tstp, Gd->g, Sd->g, (const double2 *)hd->p, mu_dn, ed);
     }
+    pt.mark(-1);
     NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    pt.collect();
     if (err) *err = eu[0] + eu[1] + eu[2] + ed[0] + ed[1] + ed[2];
   });
 }

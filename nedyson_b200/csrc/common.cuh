@@ -25,7 +25,14 @@ struct ArgError : std::runtime_error {
                               __FILE__ + ":" + std::to_string(__LINE__));                      \
   } while (0)
 
-#define NEDY_CHECK_LAUNCH() NEDY_CUDA(cudaGetLastError())
+// Every kernel launch of the engine is followed by NEDY_CHECK_LAUNCH, which also
+// counts it (nedy_launch_count in the C ABI).
+extern unsigned long long g_launches;
+#define NEDY_CHECK_LAUNCH()                                                                    \
+  do {                                                                                         \
+    ++::nedy::g_launches;                                                                      \
+    NEDY_CUDA(cudaGetLastError());                                                             \
+  } while (0)
 
 #define NEDY_REQUIRE(cond, msg)                                                                \
   do {                                                                                         \
@@ -47,5 +54,16 @@ __host__ __device__ __forceinline__ i64 les_idx(i64 i, i64 j) { return j * (j + 
 __host__ __device__ __forceinline__ i64 ret_idx(i64 i, i64 j) { return i * (i + 1) / 2 + j; }  // j <= i
 
 inline unsigned cdiv(i64 a, i64 b) { return (unsigned)((a + b - 1) / b); }
+
+// Host -> device copy / memset ordered on the engine's stream and completed before
+// returning (a pageable cudaMemcpy on the legacy stream may return before its DMA lands).
+inline void h2d_sync(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+  NEDY_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  NEDY_CUDA(cudaStreamSynchronize(s));
+}
+inline void memset_sync(void *dst, size_t bytes, cudaStream_t s) {
+  NEDY_CUDA(cudaMemsetAsync(dst, 0, bytes, s));
+  NEDY_CUDA(cudaStreamSynchronize(s));
+}
 
 } // namespace nedy

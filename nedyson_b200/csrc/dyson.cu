@@ -526,11 +526,11 @@ void ensure_tables(Ctx &c) {
       gt[(size_t)j * n + a] = w;
     }
   }
-  if (c.greg) cudaFree(c.greg);
+  if (c.greg) { NEDY_CUDA(cudaStreamSynchronize(c.stream)); cudaFree(c.greg); }
   NEDY_CUDA(cudaMalloc(&c.greg, sizeof(double) * 2 * (size_t)n * n));
   c.gregT = c.greg + (size_t)n * n;
-  NEDY_CUDA(cudaMemcpy(c.greg, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice));
-  NEDY_CUDA(cudaMemcpy(c.gregT, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice));
+  h2d_sync(c.greg, g.data(), sizeof(double) * g.size(), c.stream);
+  h2d_sync(c.gregT, gt.data(), sizeof(double) * gt.size(), c.stream);
   std::vector<double> small;
   small.insert(small.end(), c.W.poly_diff.begin(), c.W.poly_diff.end());
   small.insert(small.end(), c.W.bd.begin(), c.W.bd.end());
@@ -539,7 +539,7 @@ void ensure_tables(Ctx &c) {
   small.insert(small.end(), c.col.u.begin(), c.col.u.end());
   if (c.small) cudaFree(c.small);
   NEDY_CUDA(cudaMalloc(&c.small, sizeof(double) * small.size()));
-  NEDY_CUDA(cudaMemcpy(c.small, small.data(), sizeof(double) * small.size(), cudaMemcpyHostToDevice));
+  h2d_sync(c.small, small.data(), sizeof(double) * small.size(), c.stream);
   c.d_pdiff = c.small;
   c.d_bd = c.d_pdiff + c.W.poly_diff.size();
   c.d_ex = c.d_bd + c.W.bd.size();
@@ -586,8 +586,8 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
   NEDY_CUDA(cudaMalloc(&dEA, sizeof(double) * c.col.EA.size()));
   NEDY_CUDA(cudaMalloc(&dEB, sizeof(double) * EBs.size()));
   NEDY_CUDA(cudaMalloc(&BB, sizeof(double2) * (size_t)chunk * Q2 * es));
-  NEDY_CUDA(cudaMemcpy(dEA, c.col.EA.data(), sizeof(double) * c.col.EA.size(), cudaMemcpyHostToDevice));
-  NEDY_CUDA(cudaMemcpy(dEB, EBs.data(), sizeof(double) * EBs.size(), cudaMemcpyHostToDevice));
+  h2d_sync(dEA, c.col.EA.data(), sizeof(double) * c.col.EA.size(), c.stream);
+  h2d_sync(dEB, EBs.data(), sizeof(double) * EBs.size(), c.stream);
   for (int m0 = 0; m0 < np; m0 += chunk) {
     int nm = std::min(chunk, np - m0);
     {  // BB[m] = EB[m] (2Q x np) * G^M (np x N^2)
@@ -638,7 +638,9 @@ void extrapolate(Ctx &c, int n, DevGF &G) {
   const int N = G.nao, k = c.k;
   const i64 es = (i64)N * N;
   extrap_tv_kernel<<<nblk(es * (G.ntau + 1)), TPB, 0, c.stream>>>(N, k, n, G, c.d_ex);
+  NEDY_CHECK_LAUNCH();
   extrap_ret_kernel<<<nblk(es * (n + 1)), TPB, 0, c.stream>>>(N, k, n, G, c.d_ex);
+  NEDY_CHECK_LAUNCH();
   extrap_les_kernel<<<nblk(es * (n + 1)), TPB, 0, c.stream>>>(N, k, n, G, c.d_ex);
   NEDY_CHECK_LAUNCH();
 }
@@ -710,6 +712,7 @@ static double dyson_ret(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *
   double *err = c.ws.alloc<double>(T + 1);
   NEDY_CUDA(cudaMemsetAsync(err, 0, sizeof(double) * (T + 1), c.stream));
   set_diag_kernel<<<nblk(es), TPB, 0, c.stream>>>(N, G.retptr(T, T), make_double2(0.0, -1.0));
+  NEDY_CHECK_LAUNCH();
   double2 *M = c.ws.alloc<double2>((i64)kn * kn);
   double2 *Qs = c.ws.alloc<double2>((i64)kn * N);
   ret_start_kernel<<<nblk((i64)kn * kn + (i64)kn * N), TPB, 0, c.stream>>>(N, k, T, G, S, hmf, c.d_pdiff, c.greg, ld,
@@ -806,6 +809,7 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
     double2 *ntt = c.ws.alloc<double2>((i64)np * es);
     double2 *Bw = c.ws.alloc<double2>((i64)np * es);
     ntt_kernel<<<nblk(es * np), TPB, 0, c.stream>>>(N, G.ntau, n, G, G.sig, ntt);
+    NEDY_CHECK_LAUNCH();
     lesser_weights_kernel<<<nblk(es), TPB, 0, c.stream>>>(N, G.ntau, ntt, c.d_w, c.d_u, c.col.ctop, c.beta, Bw);
     NEDY_CHECK_LAUNCH();
     GemmArgs g;

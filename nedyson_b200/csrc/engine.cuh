@@ -92,6 +92,9 @@ struct Ctx {
   // inverses of the time-local Dyson matrices M(t') = (i bd0/dt + mu) - hmf(t') - dt w0 Sig^R(t',t')
   double2 *Minv = nullptr;
   int Minv_cap = 0, Minv_nao = 0;
+  // device time per phase of the whole-step entry points (ms): predictor, mean field, self-energy, Dyson
+  bool timing = false;
+  double phase_ms[4] = {0, 0, 0, 0};
   ~Ctx();
 };
 

@@ -92,8 +92,10 @@ void sigma_full(Ctx &c, int T, DevGF &Sig, const DevGF &G) {
   double2 *D = c.ws.alloc<double2>(3 * nles * es);
   auto nb = [](i64 n) { return (unsigned)std::min<i64>((n + 255) / 256, 65535); };
   full_prep_kernel<<<nb(es * nles), 256, 0, c.stream>>>(0, N, nles, G.lesptr(0, T), es, G.retptr(T, 0), es, 0, H, 0);
+  NEDY_CHECK_LAUNCH();
   full_prep_kernel<<<nb(es * ntv), 256, 0, c.stream>>>(1, N, ntv, G.tvptr(T, ntau), -es, nullptr, 0, -(double)G.sig,
                                                        Hv, 0);
+  NEDY_CHECK_LAUNCH();
   full_prep_kernel<<<nb(es * nles), 256, 0, c.stream>>>(2, N, nles, G.lesptr(0, T), es, G.retptr(T, 0), es, 0, D,
                                                         nles * es);
   NEDY_CHECK_LAUNCH();

@@ -104,7 +104,8 @@ def hf_fock(p: Problem, rho: np.ndarray) -> np.ndarray:
     V = p.Vija
     X = np.einsum("kl,kla->a", rho, V)
     J = np.einsum("ija,a->ij", V, X)
-    K = np.einsum("ila,kl,kja->ij", V, rho, V)
+    Va = np.ascontiguousarray(V.transpose(2, 0, 1))  # V^a_ij
+    K = (Va @ rho.T @ Va).sum(axis=0)                # K_ij = sum_a (V^a rho^T V^a)_ij
     return p.h0 + 2 * J - K
 
 
@@ -151,3 +152,29 @@ def g0_from_h0(G: HostGF, x: np.ndarray, mu: float, H0: np.ndarray, beta: float,
         for n in range(m + 1):
             G.retblk(m, n)[:] = -1j * Ut[m] @ Ut[n].conj().T
             G.lesblk(n, m)[:] = 1j * Ut[n] @ val @ Ut[m].conj().T
+
+
+def free_history(nt: int, t_fill: int, ntau: int, x: np.ndarray, mu: float, F: np.ndarray, beta: float,
+                 dt: float, scale: complex = 1.0):
+    """Free (time-translation-invariant) propagation of the constant Fock matrix F on rows 0..t_fill-1,
+    in packed layout: returns (les_blocks, ret_blocks, tv_rows, mat) where les/ret hold the blocks
+    of the columns / rows 0..t_fill-1 (first tri(t_fill-1) blocks) and tv the rows 0..t_fill-1.
+    Same closed forms as g0_from_h0: G^R(t,t') = -i U(t-t'), G^<(t',t) = i U(t'-t) f,
+    G^tv(t,tau) = i U(t) e(tau), with U(n) = exp(i n dt (mu - F))."""
+    N = F.shape[0]
+    Hmu = mu * np.eye(N) - F
+    ev, V = np.linalg.eigh(Hmu)
+    n = np.arange(t_fill)
+    Ud = np.einsum("ij,nj,kj->nik", V, np.exp(1j * dt * n[:, None] * ev[None, :]), V.conj())  # U(n)
+    fval = (V * fermi(beta, -ev)) @ V.conj().T
+    nb = t_fill * (t_fill + 1) // 2
+    tt = np.repeat(n, n + 1)                     # row / column index of each packed block
+    ss = np.concatenate([np.arange(t + 1) for t in n]) if t_fill > 0 else np.zeros(0, int)
+    ret = -1j * Ud[tt - ss]                      # ret block (t, t') -> U(t - t')
+    les = 1j * np.conj(np.transpose(Ud[tt - ss], (0, 2, 1))) @ fval   # les block (t', t): U(t'-t) f = U(t-t')^+ f
+    taus = beta / 2.0 * (np.asarray(x) + 1.0)
+    core = np.stack([(V * fermi_exp(beta, tau, -ev)) @ V.conj().T for tau in taus])
+    tv = 1j * np.einsum("nij,mjk->nmik", Ud, core)
+    mat = np.stack([-(V * fermi_exp(beta, tau, ev)) @ V.conj().T for tau in taus])
+    return (scale * les).astype(np.complex128), (scale * ret).astype(np.complex128), \
+        (scale * tv).astype(np.complex128), mat.astype(np.complex128)
