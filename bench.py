@@ -346,7 +346,7 @@ def run_engine(args, dist: Dist):
 
     out = dict(secs=secs_max, launches=launches, phase_ms=list(ms4), clocks=clk, T=T_timed, e2e_secs=e2e_secs,
                h2d=h2d, d2h=d2h, rowmax=rowmax, err=e.value)
-    ctx.close()
+    torch.cuda.synchronize(dev)
     return out
 
 
@@ -382,6 +382,7 @@ def main():
         dist.close()
         return
 
+    fp64 = fp64_gemm_peak(dist.local) if dist.rank == 0 else None
     r = run_engine(args, dist)
     total_steps = K * dist.world
     value = total_steps / r["secs"]
@@ -396,7 +397,6 @@ def main():
             "dtype": "complex128", "data": "synthetic (seeded random h0, B^Q, dipole; free-propagation history)",
             "config": cfg}
     if dist.rank == 0:
-        fp64 = fp64_gemm_peak(dist.local)
         line["roofline"] = {"bound": "tensor", "kernel": "GF2 self-energy row (FP64 DMMA GEMM chain)",
                             "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                             "frac": (achieved / fp64) if achieved else None, "traffic": None,
