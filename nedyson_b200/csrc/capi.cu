@@ -2,6 +2,7 @@
 #include "../../include/nedy.h"
 #include "sigma.cuh"
 #include <cstring>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -447,6 +448,12 @@ int nedy_set_df_tensor(nedy_ctx *ctx, const double *Vija, int nao, int naux) {
     put(c.Vmbq, vmbq.data());
     c.df_nao = nao;
     c.df_naux = naux;
+    bool sym = true;
+    for (int i = 0; i < nao && sym; i++)
+      for (int j = 0; j < i && sym; j++)
+        for (int q = 0; q < naux; q++)
+          if (Vija[((size_t)i * nao + j) * naux + q] != Vija[((size_t)j * nao + i) * naux + q]) { sym = false; break; }
+    c.V_sym = sym;
   });
 }
 

@@ -77,6 +77,7 @@ struct Ctx {
   Colloc col;
   // density-fitted interaction, several layouts (real, row-major)
   int df_nao = 0, df_naux = 0;
+  bool V_sym = false;  // every B^Q real symmetric: retarded row from Sigma^> and the lesser row
   double *Vija = nullptr;  // [i][j][a]
   double *Viaj = nullptr;  // [i][a][j]
   double *Vaij = nullptr;  // [a][i][j]

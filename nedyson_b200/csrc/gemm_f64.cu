@@ -1,18 +1,18 @@
 // Batched FP64 / complex128 GEMM on DMMA (mma.sync.aligned.m8n8k4 .f64).  See gemm_f64.cuh.
 //
-// CTA tile 64 x 64 x 16, 4 warps in a 2 x 2 grid, each warp owning a 32 x 32
-// tile = 4 x 4 DMMA fragments.  Complex operands are split into re / im planes
-// in shared memory as they are copied in (cp.async, two-stage pipeline); a
-// complex product is four real DMMAs (re*re - im*im, re*im + im*re).
+// CTA tile BM x 64 x 16 (BM = 128 with 8 warps, or 64 with 4 warps for short M),
+// each warp owning a 32 x 32 tile = 4 x 4 DMMA fragments.  Operands are copied to
+// shared memory with cp.async in a three-stage pipeline, complex values kept
+// interleaved (one 16-byte copy per element, one 16-byte shared load per fragment
+// element); a complex product is four real DMMAs (re*re - im*im, re*im + im*re).
+// Row offsets of the A tile are computed once per CTA; the two-level index split of
+// the views costs one division per element per k-tile only for the split dimension.
 #include "gemm_f64.cuh"
 
 namespace nedy {
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, NT = 128, PAD = 4;
-constexpr int LDA = BM + PAD, LDB = BN + PAD;  // 68 = 4 (mod 16): conflict-free fragment reads
-constexpr int STAGE = 2 * BK * LDA + 2 * BK * LDB;  // doubles per pipeline stage (re+im planes)
-constexpr int SMEM_BYTES = 2 * STAGE * 8;
+constexpr int BN = 64, BK = 16, STAGES = 3;
 
 struct DView {
   const char *p;
@@ -32,6 +32,7 @@ struct Params {
   const int *gM, *gK;
   const double *bscale;
   int atomic;
+  int ksplit, kchunk;  // split-K: z index = batch * ksplit + split, each split covers kchunk of K
   int a_kcontig, b_ncontig;
 };
 
@@ -47,67 +48,108 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void cp_async8(double *dst, const void *src, bool valid) {
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *dst, const void *src, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  int n = valid ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src), "r"(n));
+  int n = valid ? BYTES : 0;
+  if (BYTES == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(n));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(src), "r"(n));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-template <bool AC, bool BC>
-__device__ __forceinline__ void load_tile(const Params &P, const char *Ab, const char *Bb, int m0, int n0, int k0,
-                                          int Mg, int Kg, double *st) {
-  const int tid = threadIdx.x;
-  double *Are = st, *Aim = st + BK * LDA, *Bre = st + 2 * BK * LDA, *Bim = Bre + BK * LDB;
-  const int esA = AC ? 16 : 8, esB = BC ? 16 : 8;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    int m, k;
-    if (P.a_kcontig) { k = tid & 15; m = (tid >> 4) + 8 * i; }
-    else { m = tid & 63; k = (tid >> 6) + 2 * i; }
-    int gm = m0 + m, gk = k0 + k;
-    bool v = gm < Mg && gk < Kg;
-    const char *src = Ab;
-    if (v) src = Ab + (off2(gm, P.A.rdiv, P.A.rs_hi, P.A.rs_lo) + off2(gk, P.A.cdiv, P.A.cs_hi, P.A.cs_lo)) * esA;
-    cp_async8(Are + k * LDA + m, src, v);
-    if (AC) cp_async8(Aim + k * LDA + m, src + 8, v);
-  }
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    int n, k;
-    if (P.b_ncontig) { n = tid & 63; k = (tid >> 6) + 2 * i; }
-    else { k = tid & 15; n = (tid >> 4) + 8 * i; }
-    int gn = n0 + n, gk = k0 + k;
-    bool v = gn < P.N && gk < Kg;
-    const char *src = Bb;
-    if (v) src = Bb + (off2(gk, P.B.rdiv, P.B.rs_hi, P.B.rs_lo) + off2(gn, P.B.cdiv, P.B.cs_hi, P.B.cs_lo)) * esB;
-    cp_async8(Bre + k * LDB + n, src, v);
-    if (BC) cp_async8(Bim + k * LDB + n, src + 8, v);
-  }
-}
+// shared-memory geometry (units: elements of the operand type)
+template <bool C>
+struct Lay {
+  // complex: 16-byte elements, stride = 2 (mod 8) -> conflict-free quarter-warp fragment reads
+  // real:     8-byte elements, stride = 4 (mod 16) -> conflict-free half-warp fragment reads
+  static constexpr int pad = C ? 2 : 4;
+  static constexpr int esz = C ? 16 : 8;
+};
 
-template <bool AC, bool BC>
-__global__ void __launch_bounds__(NT, 2) gemm_kernel(const Params P) {
-  extern __shared__ double smem[];
+template <int BM, bool AC, bool BC>
+struct Smem {
+  static constexpr int LDA = BM + Lay<AC>::pad;
+  static constexpr int LDB = BN + Lay<BC>::pad;
+  static constexpr int ABYTES = BK * LDA * Lay<AC>::esz;
+  static constexpr int BBYTES = BK * LDB * Lay<BC>::esz;
+  static constexpr int STAGE = ABYTES + BBYTES;
+  static constexpr int TOTAL = STAGES * STAGE;
+};
+
+template <int BM, bool AC, bool BC>
+__global__ void __launch_bounds__(BM * 2, (BM == 128 ? 1 : 2)) gemm_kernel(const Params P) {
+  using SM = Smem<BM, AC, BC>;
+  constexpr int NT = BM * 2;            // threads: (BM/32) x 2 warps
+  constexpr int A_PER = BM * BK / NT;   // = 8
+  constexpr int B_PER = BK * BN / NT;   // 8 (BM=64) or 4 (BM=128)
+  extern __shared__ __align__(16) char smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int nb = P.nb1 * P.nb2;
+  const int nb = P.nb1 * P.nb2 * P.ksplit;
   const double sA = P.conjA ? -1.0 : 1.0, sB = P.conjB ? -1.0 : 1.0;
+  const int esA = AC ? 16 : 8, esB = BC ? 16 : 8;
 
-  for (int bz = blockIdx.z; bz < nb; bz += gridDim.z) {
-    const int b1 = bz / P.nb2, b2 = bz - (bz / P.nb2) * P.nb2;
+  for (int bzs = blockIdx.z; bzs < nb; bzs += gridDim.z) {
+    const int bz = bzs / P.ksplit, ks = bzs - bz * P.ksplit;
+    const int b1 = bz / P.nb2, b2 = bz - b1 * P.nb2;
     const int Mg = P.gM ? P.gM[b1] : P.M;
-    const int Kg = P.gK ? P.gK[b1] : P.K;
+    const int Kfull = P.gK ? P.gK[b1] : P.K;
     if (m0 >= Mg) continue;
+    // this split covers k in [kb, kb + Kg) of the full K range
+    const int kb = ks * P.kchunk;
+    const int Kg = max(0, min(Kfull - kb, P.kchunk));
+    if (Kg == 0 && P.ksplit > 1) continue;
     const int ntiles = (Kg + BK - 1) / BK;
     const i64 oA = b1 * P.A.bs1 + b2 * P.A.bs2 + (P.goffA ? P.goffA[b1] : 0);
     const i64 oB = b1 * P.B.bs1 + b2 * P.B.bs2 + (P.goffB ? P.goffB[b1] : 0);
-    const char *Ab = P.A.p + oA * (AC ? 16 : 8);
-    const char *Bb = P.B.p + oB * (BC ? 16 : 8);
+    const char *Ab = P.A.p + oA * esA;
+    const char *Bb = P.B.p + oB * esB;
     const double *ksc = P.kscale ? P.kscale + b1 * P.kscale_bs1 : nullptr;
+
+    // fixed per-thread load coordinates; row (A) / column (B) offsets precomputed
+    const int akc = P.a_kcontig, bnc = P.b_ncontig;
+    auto a_m = [&](int i) { return akc ? (tid / BK) + (NT / BK) * i : tid % BM; };
+    auto a_k = [&](int i) { return akc ? (tid & (BK - 1)) : (tid / BM) + (NT / BM) * i; };
+    auto b_n = [&](int i) { return bnc ? tid % BN : (tid / BK) + (NT / BK) * i; };
+    auto b_k = [&](int i) { return bnc ? (tid / BN) + (NT / BN) * i : (tid & (BK - 1)); };
+    i64 aro[A_PER], bco[B_PER];
+#pragma unroll
+    for (int i = 0; i < A_PER; i++) {
+      const int gm = m0 + a_m(i);
+      aro[i] = gm < Mg ? off2(gm, P.A.rdiv, P.A.rs_hi, P.A.rs_lo) : -1;
+    }
+#pragma unroll
+    for (int i = 0; i < B_PER; i++) {
+      const int gn = n0 + b_n(i);
+      bco[i] = gn < P.N ? off2(gn, P.B.cdiv, P.B.cs_hi, P.B.cs_lo) : -1;
+    }
+
+    auto load = [&](int t, int stage) {
+      char *st = smem + stage * SM::STAGE;
+      char *As = st, *Bs = st + SM::ABYTES;
+      const int k0 = t * BK;
+      const int kg0 = kb + k0;  // absolute k of this tile
+#pragma unroll
+      for (int i = 0; i < A_PER; i++) {
+        const int kk = a_k(i), gk = k0 + kk;
+        const bool v = aro[i] >= 0 && gk < Kg;
+        const char *src = v ? Ab + (aro[i] + off2(kg0 + kk, P.A.cdiv, P.A.cs_hi, P.A.cs_lo)) * esA : Ab;
+        cp_async<AC ? 16 : 8>(As + (kk * SM::LDA + a_m(i)) * esA, src, v);
+      }
+#pragma unroll
+      for (int i = 0; i < B_PER; i++) {
+        const int kk = b_k(i), gk = k0 + kk;
+        const bool v = bco[i] >= 0 && gk < Kg;
+        const char *src = v ? Bb + (off2(kg0 + kk, P.B.rdiv, P.B.rs_hi, P.B.rs_lo) + bco[i]) * esB : Bb;
+        cp_async<BC ? 16 : 8>(Bs + (kk * SM::LDB + b_n(i)) * esB, src, v);
+      }
+    };
+
     double acc_re[4][4][2], acc_im[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; i++)
@@ -117,39 +159,54 @@ __global__ void __launch_bounds__(NT, 2) gemm_kernel(const Params P) {
         acc_im[i][j][0] = acc_im[i][j][1] = 0.0;
       }
 
-    if (ntiles > 0) load_tile<AC, BC>(P, Ab, Bb, m0, n0, 0, Mg, Kg, smem);
-    cp_commit();
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+      if (s < ntiles) load(s, s);
+      cp_commit();
+    }
     for (int t = 0; t < ntiles; t++) {
-      double *st = smem + (t & 1) * STAGE;
-      if (t + 1 < ntiles) {
-        load_tile<AC, BC>(P, Ab, Bb, m0, n0, (t + 1) * BK, Mg, Kg, smem + ((t + 1) & 1) * STAGE);
-        cp_commit();
-        cp_wait<1>();
-      } else {
-        cp_wait<0>();
-      }
+      cp_wait<STAGES - 2>();
       __syncthreads();
-      const double *Are = st, *Aim = st + BK * LDA, *Bre = st + 2 * BK * LDA, *Bim = Bre + BK * LDB;
+      // prefetch tile t + STAGES - 1 into the stage freed at iteration t - 1
+      {
+        const int tn = t + STAGES - 1;
+        if (tn < ntiles) load(tn, tn % STAGES);
+        cp_commit();
+      }
+      const char *st = smem + (t % STAGES) * SM::STAGE;
+      const char *As = st, *Bs = st + SM::ABYTES;
 #pragma unroll
       for (int kk = 0; kk < BK / 4; kk++) {
         const int kr = kk * 4 + (lane & 3);
-        double ks = 1.0;
+        double ksv = 1.0;
         if (ksc) {
-          int gk = t * BK + kr;
-          ks = gk < Kg ? ksc[gk / P.kdiv] : 0.0;
+          const int gk = t * BK + kr;
+          ksv = gk < Kg ? ksc[(kb + gk) / P.kdiv] : 0.0;
         }
         double ar[4], ai[4], br[4], bi[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           const int mm = wm * 32 + i * 8 + (lane >> 2);
-          ar[i] = Are[kr * LDA + mm] * ks;
-          ai[i] = AC ? Aim[kr * LDA + mm] * ks * sA : 0.0;
+          if (AC) {
+            const double2 v = ((const double2 *)As)[kr * SM::LDA + mm];
+            ar[i] = v.x * ksv;
+            ai[i] = v.y * ksv * sA;
+          } else {
+            ar[i] = ((const double *)As)[kr * SM::LDA + mm] * ksv;
+            ai[i] = 0.0;
+          }
         }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
           const int nn = wn * 32 + j * 8 + (lane >> 2);
-          br[j] = Bre[kr * LDB + nn];
-          bi[j] = BC ? Bim[kr * LDB + nn] * sB : 0.0;
+          if (BC) {
+            const double2 v = ((const double2 *)Bs)[kr * SM::LDB + nn];
+            br[j] = v.x;
+            bi[j] = v.y * sB;
+          } else {
+            br[j] = ((const double *)Bs)[kr * SM::LDB + nn];
+            bi[j] = 0.0;
+          }
         }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -163,8 +220,9 @@ __global__ void __launch_bounds__(NT, 2) gemm_kernel(const Params P) {
           }
         }
       }
-      __syncthreads();
     }
+    cp_wait<0>();
+    __syncthreads();
 
     // epilogue: C = alpha * acc + beta * C   (or C += alpha * acc with atomics)
     double2 *Cb = (double2 *)(P.C.p) + (b1 * P.C.bs1 + b2 * P.C.bs2 + (P.goffC ? P.goffC[b1] : 0));
@@ -184,7 +242,7 @@ __global__ void __launch_bounds__(NT, 2) gemm_kernel(const Params P) {
           double2 *dst = Cb + ro + off2(col, P.C.cdiv, P.C.cs_hi, P.C.cs_lo);
           double2 v = make_double2(acc_re[i][j][c], acc_im[i][j][c]);
           double2 o = cmul(alpha, v);
-          if (P.atomic) {
+          if (P.atomic || P.ksplit > 1) {
             atomicAdd(&dst->x, o.x);
             atomicAdd(&dst->y, o.y);
           } else {
@@ -193,6 +251,21 @@ __global__ void __launch_bounds__(NT, 2) gemm_kernel(const Params P) {
           }
         }
     }
+  }
+}
+
+// C(view) = beta * C  (prologue of a split-K launch, whose splits accumulate with atomics)
+__global__ void scale_c_kernel(int M, int N, int nb1, int nb2, DView C, const i64 *goffC, const int *gM, double2 beta) {
+  const i64 tot = (i64)M * N * nb1 * nb2;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < tot; idx += (i64)gridDim.x * blockDim.x) {
+    const i64 b = idx / ((i64)M * N);
+    const int e = (int)(idx - b * M * N);
+    const int r = e / N, c = e - (e / N) * N;
+    const int b1 = (int)(b / nb2), b2 = (int)(b - (i64)b1 * nb2);
+    if (gM && r >= gM[b1]) continue;
+    double2 *dst = (double2 *)C.p + b1 * C.bs1 + b2 * C.bs2 + (goffC ? goffC[b1] : 0) +
+                   off2(r, C.rdiv, C.rs_hi, C.rs_lo) + off2(c, C.cdiv, C.cs_hi, C.cs_lo);
+    *dst = (beta.x == 0.0 && beta.y == 0.0) ? make_double2(0.0, 0.0) : cmul(beta, *dst);
   }
 }
 
@@ -205,18 +278,27 @@ DView dv(const View &v) {
   return d;
 }
 
-template <bool AC, bool BC>
+template <int BM, bool AC, bool BC>
 void launch(const Params &P, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    NEDY_CUDA(cudaFuncSetAttribute(gemm_kernel<AC, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    attr = true;
+  using SM = Smem<BM, AC, BC>;
+  static int attr_dev = -1;
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  if (attr_dev != dev) {
+    NEDY_CUDA(cudaFuncSetAttribute(gemm_kernel<BM, AC, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::TOTAL));
+    attr_dev = dev;
   }
-  int nb = P.nb1 * P.nb2;
+  int nb = P.nb1 * P.nb2 * P.ksplit;
   dim3 grid(cdiv(P.N, BN), cdiv(P.M, BM), (unsigned)(nb < 65535 ? nb : 65535));
   NEDY_REQUIRE(grid.y <= 65535, "gemm: M too large");
-  gemm_kernel<AC, BC><<<grid, NT, SMEM_BYTES, s>>>(P);
+  gemm_kernel<BM, AC, BC><<<grid, BM * 2, SM::TOTAL, s>>>(P);
   NEDY_CHECK_LAUNCH();
+}
+
+template <bool AC, bool BC>
+void launch_bm(const Params &P, cudaStream_t s) {
+  if (P.M >= 128) launch<128, AC, BC>(P, s);
+  else launch<64, AC, BC>(P, s);
 }
 
 } // namespace
@@ -237,10 +319,34 @@ void gemm(const GemmArgs &g, cudaStream_t stream) {
   // loader mapping: walk consecutive threads along the unit-stride direction
   P.a_kcontig = (g.A.cs_lo == 1) ? 1 : 0;
   P.b_ncontig = (g.B.cs_lo == 1) ? 1 : 0;
-  if (g.a_cplx && g.b_cplx) launch<true, true>(P, stream);
-  else if (g.a_cplx) launch<true, false>(P, stream);
-  else if (g.b_cplx) launch<false, true>(P, stream);
-  else launch<false, false>(P, stream);
+  // split-K when the output grid is too small to fill the GPU and K is long
+  P.ksplit = 1;
+  P.kchunk = g.K;
+  {
+    const int bm = g.M >= 128 ? 128 : 64;
+    const i64 ctas = (i64)cdiv(g.N, BN) * cdiv(g.M, bm) * g.nb1 * g.nb2;
+    const i64 target = 2 * 148;
+    if (!g.gK && ctas < target && g.K >= 1024) {
+      int ks = (int)std::min<i64>((target + ctas - 1) / ctas, g.K / 256);
+      if (ks > 1) {
+        int kc = (g.K + ks - 1) / ks;
+        kc = ((kc + BK - 1) / BK) * BK;
+        ks = (g.K + kc - 1) / kc;
+        P.ksplit = ks;
+        P.kchunk = kc;
+      }
+    }
+  }
+  if (P.ksplit > 1 && !g.atomic) {
+    const i64 tot = (i64)g.M * g.N * g.nb1 * g.nb2;
+    scale_c_kernel<<<(unsigned)std::min<i64>((tot + 255) / 256, 65535LL * 8), 256, 0, stream>>>(
+        g.M, g.N, g.nb1, g.nb2, P.C, P.goffC, P.gM, g.beta);
+    NEDY_CHECK_LAUNCH();
+  }
+  if (g.a_cplx && g.b_cplx) launch_bm<true, true>(P, stream);
+  else if (g.a_cplx) launch_bm<true, false>(P, stream);
+  else if (g.b_cplx) launch_bm<false, true>(P, stream);
+  else launch_bm<false, false>(P, stream);
 }
 
 } // namespace nedy

@@ -175,6 +175,23 @@ struct DF {
   }
 };
 
+// out_s += in_s^+ for nb consecutive N x N blocks
+__global__ void adj_add_kernel(int N, int nb, const double2 *in, double2 *out) {
+  const i64 es = (i64)N * N;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < es * nb; idx += (i64)gridDim.x * blockDim.x) {
+    const int b = (int)(idx / es), e = (int)(idx - (i64)b * es);
+    const int i = e / N, j = e - (e / N) * N;
+    const double2 v = in[(i64)b * es + (i64)j * N + i];
+    out[idx] = make_double2(out[idx].x + v.x, out[idx].y - v.y);
+  }
+}
+
+void adj_add(Ctx &c, int N, int nb, const double2 *in, double2 *out) {
+  i64 tot = (i64)N * N * nb;
+  adj_add_kernel<<<(unsigned)std::min<i64>((tot + 255) / 256, 65535LL * 8), 256, 0, c.stream>>>(N, nb, in, out);
+  NEDY_CHECK_LAUNCH();
+}
+
 void prep(Ctx &c, int mode, int nsl, const double2 *L0, i64 Ls, const double2 *R0, i64 Rs, double sgn,
           double2 *out, i64 out_stride) {
   int N = c.df_nao;
@@ -221,52 +238,67 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
   int chunk, sub;
   chunking(c, chunk, sub);
 
-  // ---------------- lesser and mixed rows: one bubble unit + one exchange unit per slice
-  for (int kind = 0; kind < 2; kind++) {
-    const int nslices = kind == 0 ? T + 1 : ntau + 1;
+  // ---------------- lesser and mixed rows: one bubble unit + one exchange unit per slice.
+  // With real symmetric B^Q the retarded row is Sigma^>(T,t') + Sigma^<(t',T)^+ (kind 2), where
+  // Sigma^>(T,t') is the same les-form unit with X = Z = G^>(T,t') = R - L^+ and Y = L.
+  const int nkinds = c.V_sym ? 3 : 2;
+  for (int kind = 0; kind < nkinds; kind++) {
+    const int nslices = kind == 1 ? ntau + 1 : T + 1;
     for (int t0 = 0; t0 < nslices; t0 += chunk) {
       const int nsl = std::min(chunk, nslices - t0);
       c.ws.reset();
       DF d(c, nsl);
-      double2 *Yb[2], *VZ[2], *VYt[2];
-      Blocks X[2];
+      double2 *Hb[2], *VZ[2], *VYt[2];
+      Blocks X[2], Y[2];
       for (int s = 0; s < nspin; s++) {
-        Yb[s] = c.ws.alloc<double2>(nsl * es);
-        if (kind == 0) {
-          X[s] = {G[s]->lesptr(t0, T), es};
-          prep(c, PREP_LES, nsl, G[s]->lesptr(t0, T), es, G[s]->retptr(T, t0), es, 0, Yb[s], 0);
-        } else {
+        Hb[s] = c.ws.alloc<double2>(nsl * es);
+        if (kind == 1) {
           X[s] = {G[s]->tvptr(T, t0), es};
-          prep(c, PREP_TV, nsl, G[s]->tvptr(T, ntau - t0), -es, nullptr, 0, -(double)sig, Yb[s], 0);
+          prep(c, PREP_TV, nsl, G[s]->tvptr(T, ntau - t0), -es, nullptr, 0, -(double)sig, Hb[s], 0);
+          Y[s] = {Hb[s], es};
+        } else {
+          prep(c, PREP_LES, nsl, G[s]->lesptr(t0, T), es, G[s]->retptr(T, t0), es, 0, Hb[s], 0);
+          if (kind == 0) {
+            X[s] = {G[s]->lesptr(t0, T), es};
+            Y[s] = {Hb[s], es};
+          } else {
+            X[s] = {Hb[s], es};
+            Y[s] = {G[s]->lesptr(t0, T), es};
+          }
         }
         VZ[s] = c.ws.alloc<double2>(nsl * N2A);
         VYt[s] = c.ws.alloc<double2>(nsl * N2A);
         d.VZ(X[s], VZ[s]);
-        d.VYt({Yb[s], es}, VYt[s]);
+        d.VYt(Y[s], VYt[s]);
       }
+      auto outb = [&](int s) {
+        return kind == 0 ? Blocks{Sig[s]->lesptr(t0, T), es}
+                         : (kind == 1 ? Blocks{Sig[s]->tvptr(T, t0), es} : Blocks{Sig[s]->retptr(T, t0), es});
+      };
       double2 *P = c.ws.alloc<double2>((i64)nsl * A * A);
       double2 *Wb = c.ws.alloc<double2>(nsl * N2A);
       for (int s = 0; s < nspin; s++) d.P(VZ[s], VYt[s], P, 1.0, s > 0);
       d.W(P, Wb);
-      for (int s = 0; s < nspin; s++) {
-        Blocks out = kind == 0 ? Blocks{Sig[s]->lesptr(t0, T), es} : Blocks{Sig[s]->tvptr(T, t0), es};
-        d.SigB(VZ[s], Wb, out, fb);
-      }
+      for (int s = 0; s < nspin; s++) d.SigB(VZ[s], Wb, outb(s), fb);
       // exchange (per spin): M = X V Y, Z = X
       double2 *VY = c.ws.alloc<double2>(nsl * N2A);
       double2 *M = c.ws.alloc<double2>(nsl * N2A);
       double2 *Q = c.ws.alloc<double2>(nsl * N2A);
       double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
       for (int s = 0; s < nspin; s++) {
-        d.VZ({Yb[s], es}, VY);
+        d.VZ(Y[s], VY);
         d.Mx(X[s], VY, M, 1.0, false);
-        Blocks out = kind == 0 ? Blocks{Sig[s]->lesptr(t0, T), es} : Blocks{Sig[s]->tvptr(T, t0), es};
+        Blocks out = outb(s);
         for (int u0 = 0; u0 < nsl; u0 += sub) {
           int nu = std::min(sub, nsl - u0);
           d.Exch(nu, M + u0 * N2A, VZ[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
         }
       }
     }
+  }
+  if (c.V_sym) {
+    for (int s = 0; s < nspin; s++) adj_add(c, N, T + 1, Sig[s]->lesptr(0, T), Sig[s]->retptr(T, 0));
+    return;
   }
 
   // ---------------- retarded row: two bubble units + two exchange units per slice

@@ -56,6 +56,32 @@ def test_sigma_decomp(nao, naux, nt, ntau):
     cmp_gf(Sd.to_host(), So, 1e-12)
 
 
+@pytest.mark.parametrize("nspin", [1, 2])
+def test_sigma_decomp_symmetric_BQ(nspin):
+    # real symmetric B^Q selects the retarded row Sigma^R = Sigma^>(T,t) + Sigma^<(t,T)^+
+    nao, naux, nt, ntau = 6, 9, 5, 6
+    p = make_problem(nao, naux, seed=40 + nspin)
+    rng = np.random.default_rng(5)
+    G = [rand_gf(rng, nt, ntau, nao) for _ in range(nspin)]
+    So = [HostGF(nt, ntau, nao, -1) for _ in range(nspin)]
+    ctx = api.Context(max(nt, 5), ntau, nao, 5, 1.0, 0.01)
+    Gd = [api.green_func(ctx, nt, ntau, nao, -1).from_host(g) for g in G]
+    Sd = [api.green_func(ctx, nt, ntau, nao, -1) for _ in range(nspin)]
+    df = po.DF(p.Vija)
+    if nspin == 1:
+        s = api.molGF2SolverDecomp(ctx, p.Vija)
+        for t in range(nt + 1):
+            df.solve(t, So[0], G[0])
+            s.solve(t, Sd[0], Gd[0])
+    else:
+        s = api.molGF2SolverSpinDecomp(ctx, p.Vija)
+        for t in range(nt + 1):
+            df.solve_spin(t, So, G)
+            s.solve(t, Sd, Gd)
+    for a, b in zip(Sd, So):
+        cmp_gf(a.to_host(), b, 1e-12)
+
+
 def test_sigma_decomp_chunked_workspace():
     # a small workspace budget forces several slice chunks and exchange sub-chunks
     rng = np.random.default_rng(9)
