@@ -78,6 +78,8 @@ int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w);
 
 /* --- Green's functions: green_func(nt, ntau, size1, sig) (src/greens.cpp:34-55) --- */
 int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out);
+/* Waits for the device; may be called before or after nedy_ctx_destroy of its context
+ * (every other call on the handle needs a live context). */
 int nedy_gf_destroy(nedy_gf *g);
 /* Copy nblocks nao x nao blocks starting at block first_block of a component. */
 int nedy_gf_upload(nedy_gf *g, int component, long long first_block, long long nblocks, const void *host);
@@ -88,6 +90,7 @@ int nedy_gf_set_tstp_zero(nedy_gf *g, int tstp);
 
 /* --- Device buffers (mean-field hmf, density matrices, ...) --- */
 int nedy_buf_create(nedy_ctx *ctx, long long bytes, nedy_buf **out);
+/* Waits for the device; may be called before or after nedy_ctx_destroy. */
 int nedy_buf_destroy(nedy_buf *b);
 int nedy_buf_upload(nedy_buf *b, long long offset, long long bytes, const void *host);
 int nedy_buf_download(const nedy_buf *b, long long offset, long long bytes, void *host);

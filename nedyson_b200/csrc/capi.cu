@@ -1,5 +1,5 @@
 // C ABI (include/nedy.h): handles, memory, and the public entry points.
-#include "../../include/nedy.h"
+#include "handles.cuh"
 #include "sigma.cuh"
 #include <cstring>
 #include <cstdlib>
@@ -7,19 +7,6 @@
 #include <vector>
 
 using namespace nedy;
-
-struct nedy_ctx {
-  Ctx c;
-};
-struct nedy_gf {
-  nedy_ctx *ctx;
-  DevGF g;
-};
-struct nedy_buf {
-  nedy_ctx *ctx;
-  void *p;
-  long long bytes;
-};
 
 namespace nedy {
 
@@ -151,6 +138,11 @@ int guard(F &&f) {
 }
 
 void set_dev(nedy_ctx *ctx) { NEDY_CUDA(cudaSetDevice(ctx->c.device)); }
+} // namespace
+
+int nedy::run_guarded(const std::function<void()> &f) { return guard(f); }
+
+namespace {
 
 double2 *comp_ptr(const nedy_gf *g, int comp, i64 &nblocks) {
   const DevGF &d = g->g;
@@ -272,6 +264,7 @@ int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **
     set_dev(ctx);
     auto *g = new nedy_gf;
     g->ctx = ctx;
+    g->device = ctx->c.device;
     DevGF &d = g->g;
     d.nt = nt; d.ntau = ntau; d.nao = nao; d.sig = sig; d.es = (i64)nao * nao;
     auto alloc = [&](double2 *&p, i64 nblk) {
@@ -306,8 +299,8 @@ int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **
 int nedy_gf_destroy(nedy_gf *g) {
   return guard([&] {
     if (!g) return;
-    set_dev(g->ctx);
-    cudaStreamSynchronize(g->ctx->c.stream);
+    // cudaFree waits for the device; the context may already be gone
+    cudaSetDevice(g->device);
     if (g->g.mat) cudaFree(g->g.mat);
     if (g->g.les) cudaFree(g->g.les);
     if (g->g.ret) cudaFree(g->g.ret);
@@ -375,6 +368,7 @@ int nedy_buf_create(nedy_ctx *ctx, long long bytes, nedy_buf **out) {
     set_dev(ctx);
     auto *b = new nedy_buf;
     b->ctx = ctx;
+    b->device = ctx->c.device;
     b->bytes = bytes;
     cudaError_t e = cudaMalloc(&b->p, bytes);
     if (e != cudaSuccess) {
@@ -390,8 +384,7 @@ int nedy_buf_create(nedy_ctx *ctx, long long bytes, nedy_buf **out) {
 int nedy_buf_destroy(nedy_buf *b) {
   return guard([&] {
     if (!b) return;
-    set_dev(b->ctx);
-    cudaStreamSynchronize(b->ctx->c.stream);
+    cudaSetDevice(b->device);
     cudaFree(b->p);
     delete b;
   });

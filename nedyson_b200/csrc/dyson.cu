@@ -98,11 +98,97 @@ __global__ void gj_kernel(int n, int nrhs, double2 *A, i64 sA, double2 *B, i64 s
   }
 }
 
+// Gauss-Jordan with partial pivoting for ONE large system, spread over many CTAs:
+// CTA g owns the augmented columns [g*cw, (g+1)*cw) of [A | B].  One launch per
+// elimination step c; the pivot index and the pivot column of step c are produced
+// by the launch of step c-1 (by the CTA that owns column c) into buffer c & 1.
+__device__ __forceinline__ double2 &aug(double2 *A, double2 *B, int n, int nrhs, int r, int j) {
+  return j < n ? A[(i64)r * n + j] : B[(i64)r * nrhs + (j - n)];
+}
+
+__device__ void gj_pivot_block(int n, int nrhs, double2 *A, double2 *B, int c, int *piv, double2 *fac) {
+  __shared__ double sval[TPB];
+  __shared__ int sidx[TPB];
+  const int tid = threadIdx.x;
+  double best = -1.0;
+  int bi = c;
+  for (int r = c + tid; r < n; r += blockDim.x) {
+    const double2 v = A[(i64)r * n + c];
+    const double a = hypot(v.x, v.y);
+    if (a > best) { best = a; bi = r; }
+  }
+  sval[tid] = best;
+  sidx[tid] = bi;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (tid < s && sval[tid + s] > sval[tid]) { sval[tid] = sval[tid + s]; sidx[tid] = sidx[tid + s]; }
+    __syncthreads();
+  }
+  if (tid == 0) piv[c & 1] = sidx[0];
+  for (int r = tid; r < n; r += blockDim.x) fac[(i64)(c & 1) * n + r] = A[(i64)r * n + c];
+}
+
+__global__ void gj_first_pivot_kernel(int n, int nrhs, double2 *A, double2 *B, int *piv, double2 *fac) {
+  gj_pivot_block(n, nrhs, A, B, 0, piv, fac);
+}
+
+__global__ void gj_step_kernel(int n, int nrhs, double2 *A, double2 *B, int c, int cw, int *piv, double2 *fac,
+                               int *status) {
+  __shared__ double2 rowc[64];
+  const int j0 = blockIdx.x * cw, W = n + nrhs;
+  const int jn = min(cw, W - j0);
+  if (jn <= 0) return;
+  const int p = piv[c & 1];
+  const double2 *f = fac + (i64)(c & 1) * n;
+  double2 pv = f[p];
+  if (pv.x == 0.0 && pv.y == 0.0) {
+    if (threadIdx.x == 0) *status = 1;
+    pv = make_double2(1.0, 0.0);
+  }
+  const double dd = pv.x * pv.x + pv.y * pv.y;
+  const double2 inv = make_double2(pv.x / dd, -pv.y / dd);
+  // phase 1: swap rows c and p, scale the pivot row
+  for (int jj = threadIdx.x; jj < jn; jj += blockDim.x) {
+    const int j = j0 + jj;
+    const double2 ac = aug(A, B, n, nrhs, c, j), ap = aug(A, B, n, nrhs, p, j);
+    const double2 rc = cmul(ap, inv);
+    rowc[jj] = rc;
+    aug(A, B, n, nrhs, c, j) = rc;
+    if (p != c) aug(A, B, n, nrhs, p, j) = csub(ac, cmul(f[c], rc));
+  }
+  __syncthreads();
+  // phase 2: eliminate the other rows (the factors are the pivot column after the swap)
+  for (i64 idx = threadIdx.x; idx < (i64)n * jn; idx += blockDim.x) {
+    const int r = (int)(idx / jn), jj = (int)(idx - (i64)r * jn);
+    if (r == c || r == p) continue;
+    double2 &x = aug(A, B, n, nrhs, r, j0 + jj);
+    x = csub(x, cmul(f[r], rowc[jj]));
+  }
+  __syncthreads();
+  // the owner of column c+1 prepares the next step
+  const int c1 = c + 1;
+  if (c1 < n && c1 >= j0 && c1 < j0 + jn) gj_pivot_block(n, nrhs, A, B, c1, piv, fac);
+}
+
 void gj(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB) {
   int *st = c.ws.alloc<int>(nb);
   NEDY_CUDA(cudaMemsetAsync(st, 0, sizeof(int) * nb, c.stream));
-  gj_kernel<<<nb, TPB, 0, c.stream>>>(n, nrhs, A, sA, B, sB, st);
-  NEDY_CHECK_LAUNCH();
+  if (nb == 1 && n >= 128) {
+    const int W = n + nrhs;
+    const int cw = std::min(64, std::max(2, (W + 147) / 148));
+    const int G = (W + cw - 1) / cw;
+    int *piv = c.ws.alloc<int>(2);
+    double2 *fac = c.ws.alloc<double2>(2 * (i64)n);
+    gj_first_pivot_kernel<<<1, TPB, 0, c.stream>>>(n, nrhs, A, B, piv, fac);
+    NEDY_CHECK_LAUNCH();
+    for (int col = 0; col < n; col++) {
+      gj_step_kernel<<<G, TPB, 0, c.stream>>>(n, nrhs, A, B, col, cw, piv, fac, st);
+      NEDY_CHECK_LAUNCH();
+    }
+  } else {
+    gj_kernel<<<nb, TPB, 0, c.stream>>>(n, nrhs, A, sA, B, sB, st);
+    NEDY_CHECK_LAUNCH();
+  }
   c.pending_status.push_back({st, nb});
 }
 

@@ -197,7 +197,7 @@ def _state(nao, naux, nt, ntau, beta, dt, k, seed, sigma_scale=0.05):
     return p, G, S, hmf, mu
 
 
-@pytest.mark.parametrize("nao,T", [(3, 6), (3, 9), (5, 14), (16, 20)])
+@pytest.mark.parametrize("nao,T", [(3, 6), (3, 9), (5, 14), (16, 20), (32, 8)])
 def test_dyson_step(nao, T):
     nt, ntau, beta, dt, k = max(T, 12), 12, 4.0, 0.02, 5
     p, G, S, hmf, mu = _state(nao, 4, nt, ntau, beta, dt, k, seed=nao + T)
@@ -215,8 +215,9 @@ def test_dyson_step(nao, T):
     assert abs(eg - eo) <= 1e-8 * max(1.0, abs(eo))
 
 
-def test_dyson_start():
-    nao, nt, ntau, beta, dt, k = 4, 10, 14, 5.0, 0.02, 5
+@pytest.mark.parametrize("nao", [4, 32])
+def test_dyson_start(nao):
+    nt, ntau, beta, dt, k = 10, 14, 5.0, 0.02, 5
     p, G, S, hmf, mu = _state(nao, 4, nt, ntau, beta, dt, k, seed=31)
     ctx = api.Context(nt, ntau, nao, k, beta, dt)
     Gd = api.green_func(ctx, nt, ntau, nao, -1).from_host(G)
