@@ -122,6 +122,23 @@ int nedy_hf_decomp(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
 int nedy_hf_spin_decomp(nedy_ctx *ctx, int tstp, nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *rho2);
 /* molHFSolver::solve_HF                                    src/molHFSolver.h:31 */
 int nedy_hf_full(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
+/* Same result as nedy_hf_decomp, but the call allocates no device memory.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc once the
+ * simulation runs: a host program whose own pool allocator has reserved the free
+ * device memory, or a driver loop that must not stall the device, which the
+ * implicit synchronisation of cudaMalloc/cudaFree would do.  (nedy_hf_decomp may
+ * grow or merge the context's workspace, which allocates.)  Its intermediates
+ * live in one static device array of NEDY_NOALLOC_SCRATCH_BYTES, held by every
+ * GPU that loads the library until the process exits.  A call needs
+ * 16*naux bytes (rounded up to 256) + 16*nao*nao*naux bytes of it (nao=64,
+ * naux=256 fits); larger sizes are rejected with NEDY_ERR_ARG.
+ * The first call on a device looks up that array's device address (set-up);
+ * make that first call before any stream capture starts.  All calls on a device
+ * share the array: calls that overlap on the GPU (other host threads, other
+ * contexts on the same device) race.  Returns after the context's stream has
+ * finished the update, like nedy_hf_decomp. */
+#define NEDY_NOALLOC_SCRATCH_BYTES (24LL << 20)
+int nedy_hf_decomp_noalloc(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
 
 /* --- Dyson equation --- */
 /* dyson::Extrapolate(int, GREEN&)                          src/dyson.h:114 */

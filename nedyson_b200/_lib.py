@@ -61,6 +61,7 @@ SIGNATURES = {
     "nedy_gf2_full_solve": ([_P, _I, _P, _P], _I),
     "nedy_get_dm": ([_P, _P, _I, _P, _LL], _I),
     "nedy_hf_decomp": ([_P, _I, _P, _P], _I),
+    "nedy_hf_decomp_noalloc": ([_P, _I, _P, _P], _I),
     "nedy_hf_spin_decomp": ([_P, _I, _P, _P, _P], _I),
     "nedy_hf_full": ([_P, _I, _P, _P], _I),
     "nedy_extrapolate": ([_P, _I, _P], _I),
