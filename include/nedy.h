@@ -43,6 +43,13 @@ enum nedy_status {
 };
 
 enum nedy_component { NEDY_LES = 0, NEDY_RET = 1, NEDY_TV = 2, NEDY_MAT = 3 };
+/* Arithmetic of the self-energy contractions (nedy_ctx_set_precision).
+ * FP64: every product in FP64 on the DMMA tensor cores (the reference's arithmetic).
+ * SPLIT_BF16X3: the exchange contractions (the nao^4*naux part) as BF16 piece
+ *   products on tcgen05: each FP64 operand is split into three BF16 pieces, the six
+ *   piece products with combined weight >= 2^-16 are accumulated in FP32.  The Dyson
+ *   solves, the mean field, the density matrix and the residuals stay FP64. */
+enum nedy_precision { NEDY_PREC_FP64 = 0, NEDY_PREC_SPLIT_BF16X3 = 1 };
 
 typedef struct nedy_ctx nedy_ctx;
 typedef struct nedy_gf nedy_gf;
@@ -70,6 +77,9 @@ int nedy_ctx_stream(nedy_ctx *ctx, void **stream);
 /* Per-phase device timing of nedy_decomp_tstp / nedy_decomp_spin_tstp (CUDA events):
  * ms4 = accumulated milliseconds of predictor, mean field, self-energy, Dyson step. */
 int nedy_ctx_set_timing(nedy_ctx *ctx, int on);
+/* Self-energy arithmetic for this context (nedy_precision); FP64 by default.  The
+ * reference computes in FP64 only; the split modes are this engine's addition. */
+int nedy_ctx_set_precision(nedy_ctx *ctx, int mode);
 int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
 /* Number of engine kernel launches issued by this process so far. */
 unsigned long long nedy_launch_count(void);

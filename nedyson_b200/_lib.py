@@ -13,6 +13,7 @@ LIBPATH = os.path.join(HERE, "libnedy_b200.so")
 
 NEDY_OK = 0
 LES, RET, TV, MAT = 0, 1, 2, 3
+PREC_FP64, PREC_SPLIT_BF16X3 = 0, 1
 
 
 class NedyConfig(C.Structure):
@@ -62,6 +63,7 @@ SIGNATURES = {
     "nedy_get_dm": ([_P, _P, _I, _P, _LL], _I),
     "nedy_hf_decomp": ([_P, _I, _P, _P], _I),
     "nedy_hf_decomp_noalloc": ([_P, _I, _P, _P], _I),
+    "nedy_ctx_set_precision": ([_P, _I], _I),
     "nedy_hf_spin_decomp": ([_P, _I, _P, _P, _P], _I),
     "nedy_hf_full": ([_P, _I, _P, _P], _I),
     "nedy_extrapolate": ([_P, _I, _P], _I),

@@ -54,6 +54,10 @@ class Context:
     def synchronize(self):
         check(lib().nedy_ctx_synchronize(self.h))
 
+    def set_precision(self, mode):
+        """Self-energy arithmetic: _lib.PREC_FP64 (default) or _lib.PREC_SPLIT_BF16X3."""
+        check(lib().nedy_ctx_set_precision(self.h, int(mode)))
+
     def collocation(self):
         x = np.zeros(self.ntau + 1)
         w = np.zeros(self.ntau + 1)

@@ -85,7 +85,7 @@ void *Arena::get(size_t bytes) {
 
 Ctx::~Ctx() {
   auto f = [](void *p) { if (p) cudaFree(p); };
-  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
+  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -125,6 +125,7 @@ int guard(F &&f) {
     return NEDY_ERR_ARG;
   } catch (const CudaError &e) {
     g_err = e.what();
+    if (g_err.find("timed out") != std::string::npos) return NEDY_ERR_TIMEOUT;
     if (g_err.find("out of memory") != std::string::npos || g_err.find("allocation") != std::string::npos)
       return NEDY_ERR_OOM;
     return NEDY_ERR_CUDA;
@@ -229,6 +230,14 @@ int nedy_ctx_stream(nedy_ctx *ctx, void **stream) {
   return guard([&] {
     NEDY_REQUIRE(ctx && stream, "null argument");
     *stream = (void *)ctx->c.stream;
+  });
+}
+
+int nedy_ctx_set_precision(nedy_ctx *ctx, int mode) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null context");
+    NEDY_REQUIRE(mode == NEDY_PREC_FP64 || mode == NEDY_PREC_SPLIT_BF16X3, "unknown precision mode");
+    ctx->c.precision = mode;
   });
 }
 
@@ -439,6 +448,9 @@ int nedy_set_df_tensor(nedy_ctx *ctx, const double *Vija, int nao, int naux) {
     put(c.Viaj, viaj.data());
     put(c.Vaij, vaij.data());
     put(c.Vmbq, vmbq.data());
+    if (c.Vp) cudaFree(c.Vp);  // pieces of the previous tensor
+    c.Vp = nullptr;
+    c.Vp_np = 0;
     c.df_nao = nao;
     c.df_naux = naux;
     bool sym = true;

@@ -82,6 +82,11 @@ struct Ctx {
   double *Viaj = nullptr;  // [i][a][j]
   double *Vaij = nullptr;  // [a][i][j]
   double *Vmbq = nullptr;  // [m][b][q] = V^b_qm
+  // self-energy arithmetic: NEDY_PREC_FP64 or a split-precision mode; BF16 pieces of
+  // Vija ([piece][(i,j)][a], K padded to 64) for the split exchange, built on first use
+  int precision = 0;
+  void *Vp = nullptr;
+  int Vp_np = 0;
   // full U (N^4 real) and the exchange combination Uexch
   int u_nao = 0;
   double *U = nullptr, *Uexch = nullptr;

@@ -20,6 +20,8 @@
 // exchange intermediate S_{(l,n),(q,j)} lives only in a chunk-sized workspace.
 #include "engine.cuh"
 #include "sigma.cuh"
+#include "split_gemm.cuh"
+#include "../../include/nedy.h"
 
 namespace nedy {
 namespace {
@@ -143,6 +145,98 @@ struct DF {
     g.beta = make_double2(acc ? 1.0 : 0.0, 0);
     gemm(g, s);
   }
+  // Split-precision layouts of the exchange operands:
+  //   MT[s] = X_s * VY[s] stored [l][n][b] (rows (l,n), K = b contiguous)
+  void MxT(Blocks X, const double2 *vy, double2 *MT, double alpha, bool acc) {
+    GemmArgs g;
+    g.M = N; g.N = (int)NA; g.K = N; g.nb1 = nsl;
+    g.A = blk(X, N);
+    g.B = rowmajor(vy, NA); g.B.bs1 = N2A;
+    g.C.p = MT; g.C.rs_lo = NA; g.C.cdiv = N; g.C.cs_hi = 1; g.C.cs_lo = A; g.C.bs1 = N2A;
+    g.alpha = make_double2(alpha, 0);
+    g.beta = make_double2(acc ? 1.0 : 0.0, 0);
+    gemm(g, s);
+  }
+  //   VZT[s] = (V^a Z_s)_{nq} stored [a][q][n] (rows a, K = (q,n) contiguous)
+  void VZT(Blocks Z, double2 *out) {
+    GemmArgs g;
+    g.M = (int)NA; g.N = N; g.K = N; g.nb1 = nsl;
+    g.A = rowmajor(c.Viaj, N); g.a_cplx = false;
+    g.B = blk(Z, N);
+    g.C.p = out; g.C.rdiv = A; g.C.rs_hi = 1; g.C.rs_lo = es; g.C.cs_lo = N; g.C.bs1 = N2A;
+    gemm(g, s);
+  }
+  // BF16 pieces of Vija as the shared B operand of the split S contraction (rows (q,j), K = b).
+  Pieces vpieces(int np) {
+    Pieces v;
+    v.rows = (int)es; v.kpad = kpad64(A); v.nb = 1; v.ncomp = 1; v.np = np;
+    if (!c.Vp || c.Vp_np != np) {
+      if (c.Vp) cudaFree(c.Vp);
+      c.Vp = nullptr;
+      NEDY_CUDA(cudaMalloc(&c.Vp, v.elems() * 2));
+      c.Vp_np = np;
+      v.p = (__nv_bfloat16 *)c.Vp;
+      split_pieces(rowmajor(c.Vija, A), false, false, A, v, s);
+    }
+    v.p = (__nv_bfloat16 *)c.Vp;
+    return v;
+  }
+  // bytes of the MT / VZT piece planes for nu units
+  i64 mz_bytes(int nu, int np) const {
+    return std::max<i64>((i64)2 * np * nu * es * kpad64(A), (i64)2 * np * nu * A * kpad64((int)es)) * 2;
+  }
+  // Exchange of nu units with the two N^4 A contractions in split precision:
+  //   S'[u][(l,j)][(q,n)] = sum_b MT[u][(l,n)][b] V^b_qj          (BF16 pieces out)
+  //   Q[u][j][l][a]      = sum_{(q,n)} S'[u][(l,j)][(q,n)] VZT[u][a][(q,n)]   (FP64 out)
+  //   Sigma_u           -= sum_{l,a} V^a_il Q[u][j][l][a]            (FP64)
+  // wsS, wsM, wsZ: scratch for the S', MT and VZT pieces (split_bytes() each, for nu units)
+  void ExchSplit(int nu, const double2 *MT, const double2 *vzt, Blocks Sig, double2 *Q, void *wsS, void *wsM,
+                 void *wsZ, int np) {
+    const int kpA = kpad64(A), kpN = kpad64((int)es);
+    Pieces Mp, Zp, Sp;
+    Mp.rows = (int)es; Mp.kpad = kpA; Mp.nb = nu; Mp.ncomp = 2; Mp.np = np;
+    Zp.rows = A; Zp.kpad = kpN; Zp.nb = nu; Zp.ncomp = 2; Zp.np = np;
+    Sp.rows = (int)es; Sp.kpad = kpN; Sp.nb = nu; Sp.ncomp = 2; Sp.np = np;
+    Sp.p = (__nv_bfloat16 *)wsS;
+    Mp.p = (__nv_bfloat16 *)wsM;
+    Zp.p = (__nv_bfloat16 *)wsZ;
+    {
+      View v = rowmajor(MT, A); v.bs1 = N2A;
+      split_pieces(v, true, false, A, Mp, s);
+      View w = rowmajor(vzt, es); w.bs1 = N2A;
+      split_pieces(w, true, false, (int)es, Zp, s);
+    }
+    if (kpN != es) NEDY_CUDA(cudaMemsetAsync(Sp.p, 0, Sp.elems() * 2, s));
+    {
+      SplitGemmArgs g;
+      g.M = (int)es; g.N = (int)es; g.K = A; g.nb = nu;
+      g.A = Mp; g.B = vpieces(np);
+      g.out_pieces = true; g.Cp = Sp;
+      g.C.rdiv = N; g.C.rs_hi = (i64)N * kpN; g.C.rs_lo = 1;
+      g.C.cdiv = N; g.C.cs_hi = N; g.C.cs_lo = kpN;
+      g.C.bs1 = es * kpN;
+      split_gemm(g, s);
+    }
+    NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * nu * N2A, s));
+    {
+      SplitGemmArgs g;
+      g.M = (int)es; g.N = A; g.K = (int)es; g.nb = nu;
+      g.A = Sp; g.B = Zp;
+      g.C.p = Q; g.C.rdiv = N; g.C.rs_hi = A; g.C.rs_lo = NA; g.C.cs_lo = 1; g.C.bs1 = N2A;
+      g.accumulate = true;
+      split_gemm(g, s);
+    }
+    {
+      GemmArgs g;
+      g.M = N; g.N = N; g.K = (int)NA; g.nb1 = nu;
+      g.A = rowmajor(c.Vija, NA); g.a_cplx = false;
+      g.B.p = Q; g.B.rs_lo = 1; g.B.cs_lo = NA; g.B.bs1 = N2A;
+      g.C = blk(Sig, N);
+      g.alpha = make_double2(-1.0, 0);
+      g.beta = make_double2(1.0, 0);
+      gemm(g, s);
+    }
+  }
   // Exchange for units u0..u0+nu-1 of this chunk: Sigma_u -= sum_{l,a} V^a_il Q[l][j][a]
   //   S[u][(l,n)][(q,j)] = sum_b M[u][l][b][n] V^b_qj ;  Q[u][j][l][a] = sum_{(n,q)} S[u][l][(n,q)][j] VZ(Z)[u][n][a][q]
   void Exch(int nu, const double2 *M, const double2 *vzz, Blocks Sig, double2 *S, double2 *Q) {
@@ -237,6 +331,9 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
   }
   int chunk, sub;
   chunking(c, chunk, sub);
+  const bool split = c.precision == NEDY_PREC_SPLIT_BF16X3;
+  const int np = 3;
+  if (split) NEDY_REQUIRE(kpad64((int)es) <= 65535 * 64, "split self-energy: nao too large");
 
   // ---------------- lesser and mixed rows: one bubble unit + one exchange unit per slice.
   // With real symmetric B^Q the retarded row is Sigma^>(T,t') + Sigma^<(t',T)^+ (kind 2), where
@@ -285,10 +382,22 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
       double2 *M = c.ws.alloc<double2>(nsl * N2A);
       double2 *Q = c.ws.alloc<double2>(nsl * N2A);
       double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
+      double2 *VZt = split ? c.ws.alloc<double2>(nsl * N2A) : nullptr;
+      void *Mb = split ? c.ws.get(d.mz_bytes(sub, np)) : nullptr;
+      void *Zb = split ? c.ws.get(d.mz_bytes(sub, np)) : nullptr;
       for (int s = 0; s < nspin; s++) {
         d.VZ(Y[s], VY);
-        d.Mx(X[s], VY, M, 1.0, false);
         Blocks out = outb(s);
+        if (split) {
+          d.MxT(X[s], VY, M, 1.0, false);
+          d.VZT(X[s], VZt);
+          for (int u0 = 0; u0 < nsl; u0 += sub) {
+            int nu = std::min(sub, nsl - u0);
+            d.ExchSplit(nu, M + u0 * N2A, VZt + u0 * N2A, {out.p + u0 * es, es}, Q + u0 * N2A, S, Mb, Zb, np);
+          }
+          continue;
+        }
+        d.Mx(X[s], VY, M, 1.0, false);
         for (int u0 = 0; u0 < nsl; u0 += sub) {
           int nu = std::min(sub, nsl - u0);
           d.Exch(nu, M + u0 * N2A, VZ[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
@@ -298,6 +407,7 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
   }
   if (c.V_sym) {
     for (int s = 0; s < nspin; s++) adj_add(c, N, T + 1, Sig[s]->lesptr(0, T), Sig[s]->retptr(T, 0));
+    if (split && split_gemm_error(c.stream)) throw CudaError("split-precision GEMM: a bounded device wait timed out");
     return;
   }
 
@@ -350,26 +460,48 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
     double2 *M = c.ws.alloc<double2>(nsl * N2A);
     double2 *Q = c.ws.alloc<double2>(nsl * N2A);
     double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
+    double2 *VZt = split ? c.ws.alloc<double2>(nsl * N2A) : nullptr;
+    void *Mb = split ? c.ws.get(d.mz_bytes(sub, np)) : nullptr;
+    void *Zb = split ? c.ws.get(d.mz_bytes(sub, np)) : nullptr;
     for (int s = 0; s < nspin; s++) {
       Blocks out = {Sig[s]->retptr(T, t0), es};
       // unit 1: M = (-L^+) V (L - R^+), Z = R
       d.VZ(Y1[s], VY);
-      d.Mx(Lh[s], VY, M, -1.0, false);
+      if (split) {
+        d.MxT(Lh[s], VY, M, -1.0, false);
+        d.VZT(R[s], VZt);
+      } else {
+        d.Mx(Lh[s], VY, M, -1.0, false);
+      }
       for (int u0 = 0; u0 < nsl; u0 += sub) {
         int nu = std::min(sub, nsl - u0);
-        d.Exch(nu, M + u0 * N2A, vzR[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
+        if (split)
+          d.ExchSplit(nu, M + u0 * N2A, VZt + u0 * N2A, {out.p + u0 * es, es}, Q + u0 * N2A, S, Mb, Zb, np);
+        else
+          d.Exch(nu, M + u0 * N2A, vzR[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
       }
       // unit 2: M = R V L + (-L^+) V R^+, Z = R - L^+
       d.VZ(L[s], VY);
-      d.Mx(R[s], VY, M, 1.0, false);
-      d.VZ(Rh[s], VY);
-      d.Mx(Lh[s], VY, M, -1.0, true);
+      if (split) {
+        d.MxT(R[s], VY, M, 1.0, false);
+        d.VZ(Rh[s], VY);
+        d.MxT(Lh[s], VY, M, -1.0, true);
+        d.VZT(Zd[s], VZt);
+      } else {
+        d.Mx(R[s], VY, M, 1.0, false);
+        d.VZ(Rh[s], VY);
+        d.Mx(Lh[s], VY, M, -1.0, true);
+      }
       for (int u0 = 0; u0 < nsl; u0 += sub) {
         int nu = std::min(sub, nsl - u0);
-        d.Exch(nu, M + u0 * N2A, vzZd[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
+        if (split)
+          d.ExchSplit(nu, M + u0 * N2A, VZt + u0 * N2A, {out.p + u0 * es, es}, Q + u0 * N2A, S, Mb, Zb, np);
+        else
+          d.Exch(nu, M + u0 * N2A, vzZd[s] + u0 * N2A, {out.p + u0 * es, es}, S, Q + u0 * N2A);
       }
     }
   }
+  if (split && split_gemm_error(c.stream)) throw CudaError("split-precision GEMM: a bounded device wait timed out");
   (void)NA;
 }
 

@@ -1,0 +1,465 @@
+// Split-precision GEMM: BF16 piece products on tcgen05 with FP32 accumulation in
+// tensor memory, operands brought into shared memory by TMA (see split_gemm.cuh).
+//
+// One CTA computes a 128 x 256 tile of one output part (real or imaginary):
+//   warp 4      TMA producer (one thread): A tile 128 x 64 and B tile 256 x 64
+//               per stage, 4 stages, mbarrier transaction counts;
+//   warp 5      MMA issuer (one thread): 4 x tcgen05.mma (M128 N256 K16) per stage,
+//               tcgen05.commit frees the stage; owns the 256-column TMEM allocation;
+//   warps 0-3   epilogue: tcgen05.ld of their 32 TMEM lanes, FP64 or BF16-piece
+//               stores through the output View.
+// The K loop runs over (term, K block): a term is one (A plane, B plane, sign)
+// piece product.  Every mbarrier wait is bounded (2 s); a wait that gives up
+// sets the error word and the CTA drains and returns, so no launch can hang.
+#include "split_gemm.cuh"
+#include <cuda.h>
+#include <mutex>
+
+namespace nedy {
+namespace {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, THREADS = 192;
+constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 128;
+constexpr int MAX_TERMS = 12;
+constexpr unsigned long long WAIT_NS = 2000000000ULL;
+
+struct Term {
+  signed char pa, pb, neg, pad;
+};
+
+struct Params {
+  int M, N, kblocks, kb_per_split, ksplit, nb;
+  int a_nb, b_nb;  // batches stored in the A / B maps (1: shared)
+  int ntn, ncomp_out;
+  int nterms[2];
+  Term terms[2][MAX_TERMS];
+  // epilogue
+  int out_pieces, out_np, accumulate, atomic;
+  double alpha;
+  void *out;
+  i64 rs_hi, rs_lo, cs_hi, cs_lo, bs, plane;
+  int rdiv, cdiv;
+  int *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false after WAIT_NS or once another CTA reported an error.
+__device__ bool mbar_wait(uint32_t a, uint32_t parity, int *err, int code) {
+  if (mbar_try(a, parity)) return true;
+  const unsigned long long t0 = gtime();
+  for (unsigned it = 1;; it++) {
+    if (mbar_try(a, parity)) return true;
+    if ((it & 255) == 0) {
+      if (*(volatile int *)err != 0) return false;
+      if (gtime() - t0 > WAIT_NS) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t mbar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+          "r"(dst),
+      "l"(map), "r"(mbar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle: rows of 64 BF16 (128 B), 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);      // start address
+  d |= (uint64_t)1 << 16;                        // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;              // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                        // SWIZZLE_128B
+  return d;
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = 256.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const Params P) {
+  extern __shared__ uint8_t sraw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)sraw + 1023) & ~(uintptr_t)1023);
+  uint64_t *bar = (uint64_t *)(smem + STAGES * STAGE_BYTES);  // full[STAGES], empty[STAGES], done
+  uint32_t *tmem_slot = (uint32_t *)(bar + 2 * STAGES + 1);
+  __shared__ int s_skip;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  const int comp = blockIdx.y % P.ncomp_out, nt = blockIdx.y / P.ncomp_out;
+  const int b = blockIdx.z / P.ksplit, ks = blockIdx.z - (blockIdx.z / P.ksplit) * P.ksplit;
+  const int m0 = blockIdx.x * BM, n0 = nt * BN;
+  const int kb0 = ks * P.kb_per_split;
+  const int nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
+  int iters = nkb * P.nterms[comp];
+  const uint32_t full0 = smem_u32(bar), empty0 = smem_u32(bar + STAGES), done = smem_u32(bar + 2 * STAGES);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_skip = *(volatile int *)P.err != 0;  // an earlier CTA gave up: do nothing
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const bool skip = s_skip != 0;
+  if (skip) iters = 0;
+
+  if (warp == 4 && lane == 0) {
+    // ---- TMA producer
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    for (int it = 0; it < iters; it++) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (it >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) break;
+      const Term t = P.terms[comp][it / nkb];
+      const int kb = kb0 + it % nkb;
+      const uint32_t sa = smem_u32(smem + s * STAGE_BYTES), sb = sa + A_BYTES;
+      mbar_expect_tx(full0 + 8 * s, STAGE_BYTES);
+      tma_load_3d(sa, &tmA, full0 + 8 * s, kb * BK, m0, t.pa * P.a_nb + (P.a_nb > 1 ? b : 0));
+      tma_load_3d(sb, &tmB, full0 + 8 * s, kb * BK, n0, t.pb * P.b_nb + (P.b_nb > 1 ? b : 0));
+    }
+  } else if (warp == 5 && lane == 0) {
+    // ---- MMA issuer
+    for (int it = 0; it < iters; it++) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(full0 + 8 * s, ph, P.err, 2)) break;
+      tc_fence_after();
+      const Term t = P.terms[comp][it / nkb];
+      const uint32_t idesc = IDESC | (t.neg ? (1u << 13) : 0u);
+      const uint32_t sa = smem_u32(smem + s * STAGE_BYTES), sb = sa + A_BYTES;
+      const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
+#pragma unroll
+      for (int k = 0; k < BK / 16; k++)  // K = 16 per instruction: +32 bytes inside the swizzle atom
+        mma_bf16(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (it > 0 || k > 0) ? 1u : 0u);
+      mma_commit(empty0 + 8 * s);
+    }
+    mma_commit(done);
+  } else if (warp < 4) {
+    // ---- epilogue
+    // lane 0 waits and tells the warp, so the .sync.aligned TMEM loads stay convergent
+    int okl = 0;
+    if (lane == 0) okl = mbar_wait(done, 0, P.err, 3) ? 1 : 0;
+    __syncwarp();
+    const bool ok = __shfl_sync(0xffffffffu, okl, 0) != 0 && !skip;
+    tc_fence_after();
+    const int m = m0 + warp * 32 + lane;
+    const bool mok = m < P.M;
+    const i64 roff = (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    if (ok) {
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        if (n0 + c0 >= P.N) break;  // uniform across the warp
+        float v[16];
+        tmem_ld16(trow + (uint32_t)c0, v);
+        if (iters == 0) {
+#pragma unroll
+          for (int j = 0; j < 16; j++) v[j] = 0.f;
+        }
+        if (!mok) continue;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int n = n0 + c0 + j;
+          if (n >= P.N) break;
+          const i64 off = roff + (P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo : (i64)n * P.cs_lo);
+          if (P.out_pieces) {
+            float x = (float)P.alpha * v[j];
+            __nv_bfloat16 *o = (__nv_bfloat16 *)P.out + (i64)comp * P.out_np * P.plane + off;
+            for (int p = 0; p < P.out_np; p++) {
+              const __nv_bfloat16 h = __float2bfloat16_rn(x);
+              o[(i64)p * P.plane] = h;
+              x -= __bfloat162float(h);
+            }
+          } else {
+            double *o = (double *)P.out + 2 * off + comp;
+            const double x = P.alpha * (double)v[j];
+            if (P.atomic)
+              atomicAdd(o, x);
+            else if (P.accumulate)
+              *o += x;
+            else
+              *o = x;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+  }
+}
+
+// ---------------------------------------------------------------------------------
+__global__ void split_pieces_kernel(int rows, int K, int kpad, int nb, int cplx, int np, const double *in, View v,
+                                    double conj_sign, __nv_bfloat16 *out, i64 plane) {
+  const i64 tot = (i64)nb * rows * kpad;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < tot; idx += (i64)gridDim.x * blockDim.x) {
+    const int k = (int)(idx % kpad);
+    const i64 rb = idx / kpad;
+    const int r = (int)(rb % rows), b = (int)(rb / rows);
+    double x[2] = {0.0, 0.0};
+    if (k < K) {
+      const i64 off = (v.rdiv ? (i64)(r / v.rdiv) * v.rs_hi + (i64)(r % v.rdiv) * v.rs_lo : (i64)r * v.rs_lo) +
+                      (v.cdiv ? (i64)(k / v.cdiv) * v.cs_hi + (i64)(k % v.cdiv) * v.cs_lo : (i64)k * v.cs_lo) +
+                      (i64)b * v.bs1;
+      if (cplx) {
+        const double2 z = ((const double2 *)in)[off];
+        x[0] = z.x;
+        x[1] = conj_sign * z.y;
+      } else {
+        x[0] = in[off];
+      }
+    }
+    for (int c = 0; c < (cplx ? 2 : 1); c++) {
+      double r0 = x[c];
+      for (int p = 0; p < np; p++) {
+        const __nv_bfloat16 h = __double2bfloat16(r0);
+        out[(i64)(c * np + p) * plane + idx] = h;
+        r0 -= (double)__bfloat162float(h);
+      }
+    }
+  }
+}
+
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    NEDY_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    NEDY_REQUIRE(q == cudaDriverEntryPointSuccess && p, "cuTensorMapEncodeTiled is not available");
+    fn = (EncodeTiled)p;
+  }
+  return fn;
+}
+
+CUtensorMap make_map(const Pieces &x, int box_rows) {
+  NEDY_REQUIRE(x.p && x.kpad % 64 == 0 && x.rows > 0, "split gemm: bad piece planes");
+  NEDY_REQUIRE(((uintptr_t)x.p & 15) == 0, "split gemm: piece planes not 16-byte aligned");
+  CUtensorMap m;
+  const cuuint64_t dims[3] = {(cuuint64_t)x.kpad, (cuuint64_t)x.rows, (cuuint64_t)x.ncomp * x.np * x.nb};
+  const cuuint64_t strides[2] = {(cuuint64_t)x.kpad * 2, (cuuint64_t)x.kpad * 2 * x.rows};
+  const cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)x.p, dims, strides, box, es,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  NEDY_REQUIRE(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+// per-device error word
+int *err_word() {
+  static int *w[64] = {nullptr};
+  static std::mutex mu;
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  if (!w[dev]) {
+    NEDY_CUDA(cudaMalloc(&w[dev], sizeof(int)));
+    NEDY_CUDA(cudaMemset(w[dev], 0, sizeof(int)));
+  }
+  return w[dev];
+}
+
+void products(int np, int (&pa)[6], int (&pb)[6], int &n) {
+  static const int A3[6] = {0, 0, 1, 0, 1, 2}, B3[6] = {0, 1, 0, 2, 1, 0};
+  n = np == 3 ? 6 : np == 2 ? 3 : 1;
+  for (int i = 0; i < n; i++) {
+    pa[i] = A3[i];
+    pb[i] = B3[i];
+  }
+}
+
+}  // namespace
+
+void split_pieces(const View &v, bool cplx, bool conj, int K, Pieces &out, cudaStream_t s) {
+  NEDY_REQUIRE(out.p && out.ncomp == (cplx ? 2 : 1) && out.kpad >= K && out.np >= 1 && out.np <= 3,
+               "split_pieces: bad output planes");
+  const i64 tot = out.plane();
+  const unsigned blocks = (unsigned)std::min<i64>((tot + 255) / 256, 148LL * 16);
+  split_pieces_kernel<<<blocks, 256, 0, s>>>(out.rows, K, out.kpad, out.nb, cplx ? 1 : 0, out.np,
+                                              (const double *)v.p, v, conj ? -1.0 : 1.0, out.p, out.plane());
+  NEDY_CHECK_LAUNCH();
+}
+
+void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
+  const bool ac = g.A.ncomp == 2, bc = g.B.ncomp == 2;
+  NEDY_REQUIRE(ac || bc, "split_gemm: at least one operand must be complex");
+  NEDY_REQUIRE(g.A.rows >= g.M && g.B.rows >= g.N && g.A.kpad == g.B.kpad && g.A.kpad >= g.K,
+               "split_gemm: operand planes do not match the sizes");
+  NEDY_REQUIRE(g.A.np == g.B.np, "split_gemm: operands split into different piece counts");
+  NEDY_REQUIRE((g.A.nb == 1 || g.A.nb == g.nb) && (g.B.nb == 1 || g.B.nb == g.nb), "split_gemm: batch mismatch");
+  if (g.M == 0 || g.N == 0 || g.nb == 0) return;
+  Params P;
+  memset(&P, 0, sizeof(P));
+  P.M = g.M;
+  P.N = g.N;
+  P.kblocks = g.A.kpad / BK;
+  P.nb = g.nb;
+  P.a_nb = g.A.nb;
+  P.b_nb = g.B.nb;
+  P.ntn = (g.N + BN - 1) / BN;
+  P.ncomp_out = 2;
+  // terms per output part
+  int pa[6], pb[6], npr;
+  products(g.A.np, pa, pb, npr);
+  const int np = g.A.np;
+  const int sA = g.conjA ? 1 : 0, sB = g.conjB ? 1 : 0;  // sign bits of the imaginary parts
+  for (int oc = 0; oc < 2; oc++) {
+    int n = 0;
+    auto add = [&](int ca, int cb, int neg) {
+      for (int i = 0; i < npr; i++) P.terms[oc][n++] = Term{(signed char)(ca * np + pa[i]), (signed char)(cb * np + pb[i]), (signed char)neg, 0};
+    };
+    if (ac && bc) {
+      if (oc == 0) {
+        add(0, 0, 0);
+        add(1, 1, 1 ^ sA ^ sB);
+      } else {
+        add(0, 1, sB);
+        add(1, 0, sA);
+      }
+    } else if (ac) {
+      add(oc, 0, oc ? sA : 0);
+    } else {
+      add(0, oc, oc ? sB : 0);
+    }
+    P.nterms[oc] = n;
+  }
+  // K split: bounded FP32 accumulation length, and enough CTAs for the GPU
+  int ksplit = g.ksplit;
+  const i64 tiles = (i64)((g.M + BM - 1) / BM) * P.ntn * 2 * g.nb;
+  if (ksplit <= 0) {
+    ksplit = 1;
+    if (g.accumulate) {
+      while (tiles * ksplit < 2 * 148 && P.kblocks / (ksplit * 2) >= 4) ksplit *= 2;
+      if (g.max_kblocks > 0)
+        while ((P.kblocks + ksplit - 1) / ksplit > g.max_kblocks) ksplit++;
+    }
+  }
+  NEDY_REQUIRE(ksplit == 1 || (g.accumulate && !g.out_pieces), "split_gemm: K split needs an accumulating FP64 output");
+  P.ksplit = ksplit;
+  P.kb_per_split = (P.kblocks + ksplit - 1) / ksplit;
+  NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && (i64)P.ntn * 2 <= 65535, "split_gemm: grid too large");
+  P.out_pieces = g.out_pieces ? 1 : 0;
+  P.accumulate = g.accumulate ? 1 : 0;
+  P.atomic = ksplit > 1 ? 1 : 0;
+  P.alpha = g.alpha;
+  if (g.out_pieces) {
+    NEDY_REQUIRE(g.Cp.p && g.Cp.ncomp == 2 && !g.accumulate, "split_gemm: bad piece output");
+    P.out = g.Cp.p;
+    P.out_np = g.Cp.np;
+    P.plane = g.Cp.plane();
+  } else {
+    NEDY_REQUIRE(g.C.p, "split_gemm: no output");
+    P.out = (void *)g.C.p;
+  }
+  P.rs_hi = g.C.rs_hi;
+  P.rs_lo = g.C.rs_lo;
+  P.rdiv = g.C.rdiv;
+  P.cs_hi = g.C.cs_hi;
+  P.cs_lo = g.C.cs_lo;
+  P.cdiv = g.C.cdiv;
+  P.bs = g.C.bs1;
+  P.err = err_word();
+  const CUtensorMap ma = make_map(g.A, BM), mb = make_map(g.B, BN);
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  if (!attr_set[dev]) {
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr_set[dev] = true;
+  }
+  dim3 grid((g.M + BM - 1) / BM, P.ntn * 2, g.nb * ksplit);
+  split_gemm_kernel<<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, P);
+  NEDY_CHECK_LAUNCH();
+}
+
+int split_gemm_error(cudaStream_t s) {
+  int *w = err_word();
+  int h = 0;
+  NEDY_CUDA(cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, s));
+  NEDY_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+}  // namespace nedy

@@ -1,0 +1,56 @@
+// Split-precision GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// An FP64 operand x is held as BF16 pieces x = x0 + x1 + x2 (+ O(2^-24 |x|)),
+// each piece the BF16 rounding of what the previous ones left over.  A product
+// a*b is then the sum of the piece products a_i b_j with i + j < npieces (6
+// products for 3 pieces, 3 for 2), which the tensor cores form exactly and
+// accumulate in FP32 in tensor memory.  Complex operands are separate real and
+// imaginary piece planes; one output tile holds either the real or the
+// imaginary part, so a complex x complex product is 2 x npieces(npieces+1)/2
+// real BF16 GEMMs per output part.
+//
+// Storage of an operand ("piece planes"): BF16, [comp][piece][batch][row][kpad],
+// K contiguous and padded with zeros to kpad, a multiple of 64 (one 128-byte
+// swizzle atom).  A is M x K (rows = M), B is N x K (rows = N): C = A * B^T.
+#pragma once
+#include "common.cuh"
+#include "gemm_f64.cuh"
+#include <cuda_bf16.h>
+
+namespace nedy {
+
+struct Pieces {
+  __nv_bfloat16 *p = nullptr;
+  int rows = 0, kpad = 0, nb = 1;  // nb = 1 with a batched GEMM: shared by every batch
+  int ncomp = 1, np = 3;           // ncomp 2: complex (re plane group, then im)
+  i64 plane() const { return (i64)nb * rows * kpad; }
+  i64 elems() const { return plane() * ncomp * np; }
+};
+
+inline int kpad64(int k) { return (k + 63) / 64 * 64; }
+
+// FP64 (complex or real) matrix rows x K, read through a View (units: complex or
+// real elements), batch b at b * v.bs1  ->  piece planes (allocated by the caller,
+// rows/kpad/nb/ncomp/np set).  conj negates the imaginary part.
+void split_pieces(const View &v, bool cplx, bool conj, int K, Pieces &out, cudaStream_t s);
+
+struct SplitGemmArgs {
+  int M = 0, N = 0, K = 0, nb = 1;  // C[b] (M x N) = alpha * A[b] (M x K) * B[b]^T (+ C[b])
+  Pieces A, B;                       // complex when ncomp == 2; at least one is complex
+  bool conjA = false, conjB = false;
+  double alpha = 1.0;
+  // output: FP64 complex through a View (units: complex elements), or BF16 pieces
+  bool out_pieces = false;
+  View C;                 // FP64 output (C.bs1 = batch stride); element offsets for pieces
+  Pieces Cp;              // piece output: planes [comp][piece] of Cp.plane() elements, offsets from C
+  bool accumulate = false;  // FP64 output only: C += alpha * A B^T
+  int ksplit = 0;           // 0: choose; > 1 needs accumulate (FP64 atomics)
+  int max_kblocks = 0;      // upper bound on 64-wide K blocks accumulated in FP32 per tile (0: none)
+};
+
+void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
+
+// Device error word of the split kernels (non-zero after a bounded wait gave up).
+int split_gemm_error(cudaStream_t s);
+
+}  // namespace nedy
