@@ -169,6 +169,12 @@ int nedy_energy_conv(nedy_ctx *ctx, int tstp, const nedy_gf *Sigma, const nedy_g
  * err: residual of the last dyson_step (sum of the three components). */
 int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
                      double mu, int corr_steps, double *err);
+/* The same step with a residual exit: corrector iterations stop after the first whose
+ * dyson_step residual (sum of the three components) is below tol, at most max_corr.
+ * The reference always runs CorrSteps iterations; this exit is the engine's addition.
+ * iters: iterations run; err_hist (optional, max_corr entries): residual per iteration. */
+int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
+                         double mu, int max_corr, double tol, int *iters, double *err_hist);
 /* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122). */
 int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
                           nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,

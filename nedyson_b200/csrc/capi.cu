@@ -634,6 +634,49 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
   });
 }
 
+int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const nedy_buf *h_t,
+                         double mu, int max_corr, double tol, int *iters, double *err_hist) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G && S && hmf && h_t, "null argument");
+    NEDY_REQUIRE(max_corr >= 1 && tol >= 0.0, "max_corr must be >= 1 and tol >= 0");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    const int N = G->g.nao;
+    const i64 es = (i64)N * N;
+    NEDY_REQUIRE(h_t->bytes >= es * 16, "h_t buffer too small");
+    double2 *hT = hmf_row(hmf, ctx, tstp, N);
+    hmf_row(hmf, ctx, G->g.nt, N);
+    PhaseTimer pt(c);
+    pt.mark(0);
+    extrapolate(c, tstp, G->g);
+    int it = 0;
+    for (; it < max_corr;) {
+      c.ws.reset();
+      pt.mark(1);
+      double2 *rho = c.ws.alloc<double2>(es);
+      get_dm(c, G->g, tstp, rho);
+      NEDY_CUDA(cudaMemcpyAsync(hT, h_t->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      double2 *h[1] = {hT};
+      hf_decomp(c, 1, h, rho);
+      DevGF *Ss[1] = {&S->g};
+      const DevGF *Gs[1] = {&G->g};
+      pt.mark(2);
+      sigma_df(c, tstp, 1, Ss, Gs);
+      pt.mark(3);
+      double e[3] = {0, 0, 0};
+      dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
+      const double r = e[0] + e[1] + e[2];
+      if (err_hist) err_hist[it] = r;
+      it++;
+      if (r < tol) break;
+    }
+    pt.mark(-1);
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    pt.collect();
+    if (iters) *iters = it;
+  });
+}
+
 int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *Gu, nedy_gf *Gd, nedy_gf *Su, nedy_gf *Sd,
                           nedy_buf *hu, nedy_buf *hd, const nedy_buf *htu, const nedy_buf *htd, double mu_up,
                           double mu_dn, int corr_steps, double *err) {

@@ -181,12 +181,47 @@ struct DF {
     v.p = (__nv_bfloat16 *)c.Vp;
     return v;
   }
+  // Bubble contractions in split precision (same results as P() and W()):
+  //   P[s] (+)= sign * sum_{(n,q)} VZ[s][n][a][q] VYt[s][n][b][q]   (A x A, K = N^2)
+  void Psplit(const double2 *vz, const double2 *vyt, double2 *Pm, double sign, bool acc, void *wsA, void *wsB,
+              int np) {
+    Pieces a, b;
+    a.rows = A; a.kpad = kpad64((int)es); a.nb = nsl; a.ncomp = 2; a.np = np; a.p = (__nv_bfloat16 *)wsA;
+    b = a;
+    b.p = (__nv_bfloat16 *)wsB;
+    View va; va.p = vz; va.rs_lo = N; va.cdiv = N; va.cs_hi = NA; va.cs_lo = 1; va.bs1 = N2A;
+    View vb; vb.p = vyt; vb.rs_lo = N; vb.cdiv = N; vb.cs_hi = NA; vb.cs_lo = 1; vb.bs1 = N2A;
+    split_pieces(va, true, false, (int)es, a, s);
+    split_pieces(vb, true, false, (int)es, b, s);
+    if (!acc) NEDY_CUDA(cudaMemsetAsync(Pm, 0, sizeof(double2) * nsl * A * A, s));
+    SplitGemmArgs g;
+    g.M = A; g.N = A; g.K = (int)es; g.nb = nsl;
+    g.A = a; g.B = b;
+    g.C = rowmajor(Pm, A); g.C.bs1 = (i64)A * A;
+    g.alpha = sign;
+    g.accumulate = true;
+    split_gemm(g, s);
+  }
+  //   W[s] = P[s] (A x A) * Vaij (A x N^2): B operand = pieces of Vija (rows (k,j), K = a)
+  void Wsplit(const double2 *Pm, double2 *Wm, void *wsP, int np) {
+    Pieces a;
+    a.rows = A; a.kpad = kpad64(A); a.nb = nsl; a.ncomp = 2; a.np = np; a.p = (__nv_bfloat16 *)wsP;
+    View va = rowmajor(Pm, A); va.bs1 = (i64)A * A;
+    split_pieces(va, true, false, A, a, s);
+    SplitGemmArgs g;
+    g.M = A; g.N = (int)es; g.K = A; g.nb = nsl;
+    g.A = a; g.B = vpieces(np);
+    g.C = rowmajor(Wm, es); g.C.bs1 = N2A;
+    split_gemm(g, s);
+  }
+  i64 pz_bytes(int np) const { return (i64)2 * np * nsl * A * kpad64((int)es) * 2; }
+  i64 pp_bytes(int np) const { return (i64)2 * np * nsl * A * kpad64(A) * 2; }
   // bytes of the MT / VZT piece planes for nu units
   i64 mz_bytes(int nu, int np) const {
     return std::max<i64>((i64)2 * np * nu * es * kpad64(A), (i64)2 * np * nu * A * kpad64((int)es)) * 2;
   }
   // Exchange of nu units with the two N^4 A contractions in split precision:
-  //   S'[u][(l,j)][(q,n)] = sum_b MT[u][(l,n)][b] V^b_qj          (BF16 pieces out)
+  //   S'[u][(l,j)][(q,n)] = sum_b V^b_qj MT[u][(l,n)][b]          (BF16 pieces out)
   //   Q[u][j][l][a]      = sum_{(q,n)} S'[u][(l,j)][(q,n)] VZT[u][a][(q,n)]   (FP64 out)
   //   Sigma_u           -= sum_{l,a} V^a_il Q[u][j][l][a]            (FP64)
   // wsS, wsM, wsZ: scratch for the S', MT and VZT pieces (split_bytes() each, for nu units)
@@ -207,13 +242,13 @@ struct DF {
       split_pieces(w, true, false, (int)es, Zp, s);
     }
     if (kpN != es) NEDY_CUDA(cudaMemsetAsync(Sp.p, 0, Sp.elems() * 2, s));
-    {
+    {  // computed as S^T (rows (q,j), columns (l,n)) so that each thread stores runs of n
       SplitGemmArgs g;
       g.M = (int)es; g.N = (int)es; g.K = A; g.nb = nu;
-      g.A = Mp; g.B = vpieces(np);
+      g.A = vpieces(np); g.B = Mp;
       g.out_pieces = true; g.Cp = Sp;
-      g.C.rdiv = N; g.C.rs_hi = (i64)N * kpN; g.C.rs_lo = 1;
-      g.C.cdiv = N; g.C.cs_hi = N; g.C.cs_lo = kpN;
+      g.C.rdiv = N; g.C.rs_hi = N; g.C.rs_lo = kpN;
+      g.C.cdiv = N; g.C.cs_hi = (i64)N * kpN; g.C.cs_lo = 1;
       g.C.bs1 = es * kpN;
       split_gemm(g, s);
     }
@@ -299,13 +334,14 @@ void prep(Ctx &c, int mode, int nsl, const double2 *L0, i64 Ls, const double2 *R
 } // namespace
 
 // Chunk sizes: slices per chunk and exchange units per S buffer, from the workspace budget.
-static void chunking(const Ctx &c, int &chunk, int &sub) {
+static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
   i64 N = c.df_nao, A = c.df_naux;
   i64 n2a = N * N * A * 16;  // bytes of one [n][a][q] intermediate
   i64 n4 = N * N * N * N * 16;
   i64 budget = c.ws_budget;
   // per slice (retarded, the largest): 5 VZ/VYt + 3 VY + 2 M + Q + 2 P/W + prep
   i64 per = 13 * n2a + 2 * A * A * 16;
+  if (split) per += 3 * n2a;  // BF16 pieces of the bubble operands and the VZT layout
   sub = (int)std::max<i64>(1, std::min<i64>(16, (budget / 3) / n4));
   chunk = (int)std::max<i64>(1, std::min<i64>(64, (budget - sub * n4) / std::max<i64>(per, 1)));
   if (chunk < sub) sub = chunk;
@@ -329,9 +365,9 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
     NEDY_CUDA(cudaMemsetAsync(Sig[s]->lesptr(0, T), 0, sizeof(double2) * (T + 1) * es, c.stream));
     NEDY_CUDA(cudaMemsetAsync(Sig[s]->tvptr(T, 0), 0, sizeof(double2) * (ntau + 1) * es, c.stream));
   }
-  int chunk, sub;
-  chunking(c, chunk, sub);
   const bool split = c.precision == NEDY_PREC_SPLIT_BF16X3;
+  int chunk, sub;
+  chunking(c, chunk, sub, split);
   const int np = 3;
   if (split) NEDY_REQUIRE(kpad64((int)es) <= 65535 * 64, "split self-energy: nao too large");
 
@@ -374,8 +410,14 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
       };
       double2 *P = c.ws.alloc<double2>((i64)nsl * A * A);
       double2 *Wb = c.ws.alloc<double2>(nsl * N2A);
-      for (int s = 0; s < nspin; s++) d.P(VZ[s], VYt[s], P, 1.0, s > 0);
-      d.W(P, Wb);
+      if (split) {
+        void *pa = c.ws.get(d.pz_bytes(np)), *pb = c.ws.get(d.pz_bytes(np)), *pp = c.ws.get(d.pp_bytes(np));
+        for (int s = 0; s < nspin; s++) d.Psplit(VZ[s], VYt[s], P, 1.0, s > 0, pa, pb, np);
+        d.Wsplit(P, Wb, pp, np);
+      } else {
+        for (int s = 0; s < nspin; s++) d.P(VZ[s], VYt[s], P, 1.0, s > 0);
+        d.W(P, Wb);
+      }
       for (int s = 0; s < nspin; s++) d.SigB(VZ[s], Wb, outb(s), fb);
       // exchange (per spin): M = X V Y, Z = X
       double2 *VY = c.ws.alloc<double2>(nsl * N2A);
@@ -441,15 +483,26 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
     }
     double2 *PA = c.ws.alloc<double2>((i64)nsl * A * A);
     double2 *PB = c.ws.alloc<double2>((i64)nsl * A * A);
-    for (int s = 0; s < nspin; s++) {
-      d.P(vzZd[s], vytL[s], PA, 1.0, s > 0);
-      d.P(vzLh[s], vytRh[s], PB, 1.0, s > 0);
-      d.P(vzR[s], vytL[s], PB, -1.0, true);
-    }
     double2 *WA = c.ws.alloc<double2>(nsl * N2A);
     double2 *WB = c.ws.alloc<double2>(nsl * N2A);
-    d.W(PA, WA);
-    d.W(PB, WB);
+    if (split) {
+      void *pa = c.ws.get(d.pz_bytes(np)), *pb = c.ws.get(d.pz_bytes(np)), *pp = c.ws.get(d.pp_bytes(np));
+      for (int s = 0; s < nspin; s++) {
+        d.Psplit(vzZd[s], vytL[s], PA, 1.0, s > 0, pa, pb, np);
+        d.Psplit(vzLh[s], vytRh[s], PB, 1.0, s > 0, pa, pb, np);
+        d.Psplit(vzR[s], vytL[s], PB, -1.0, true, pa, pb, np);
+      }
+      d.Wsplit(PA, WA, pp, np);
+      d.Wsplit(PB, WB, pp, np);
+    } else {
+      for (int s = 0; s < nspin; s++) {
+        d.P(vzZd[s], vytL[s], PA, 1.0, s > 0);
+        d.P(vzLh[s], vytRh[s], PB, 1.0, s > 0);
+        d.P(vzR[s], vytL[s], PB, -1.0, true);
+      }
+      d.W(PA, WA);
+      d.W(PB, WB);
+    }
     for (int s = 0; s < nspin; s++) {
       Blocks out = {Sig[s]->retptr(T, t0), es};
       d.SigB(vzR[s], WA, out, fb);

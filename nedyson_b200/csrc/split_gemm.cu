@@ -18,9 +18,11 @@
 namespace nedy {
 namespace {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4, THREADS = 192;
+constexpr int BM = 128, BN = 256, BK = 64, THREADS = 192;
 constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 128;
+// STAGES 4: one CTA per SM (long K loops); STAGES 2: two CTAs per SM, so one CTA's
+// epilogue overlaps the other's main loop (short K loops with heavy epilogues)
+constexpr int smem_bytes(int stages) { return stages * STAGE_BYTES + 1024 + 128; }
 constexpr int MAX_TERMS = 12;
 constexpr unsigned long long WAIT_NS = 2000000000ULL;
 
@@ -131,7 +133,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+template <int STAGES>
+__global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const Params P) {
   extern __shared__ uint8_t sraw[];
@@ -225,20 +228,65 @@ __global__ void __launch_bounds__(THREADS, 1)
           for (int j = 0; j < 16; j++) v[j] = 0.f;
         }
         if (!mok) continue;
+        // column offsets of this 16-column chunk: one division per chunk when the chunk
+        // stays inside one cdiv segment, then base + j * cs_lo
+        const int nf = n0 + c0;
+        bool fast = nf + 16 <= P.N;
+        i64 cbase = 0;
+        if (fast) {
+          if (P.cdiv) {
+            const int qd = nf / P.cdiv, rm = nf - qd * P.cdiv;
+            fast = rm + 16 <= P.cdiv;
+            cbase = (i64)qd * P.cs_hi + (i64)rm * P.cs_lo;
+          } else {
+            cbase = (i64)nf * P.cs_lo;
+          }
+        }
+        if (P.out_pieces) {
+          __nv_bfloat16 *o = (__nv_bfloat16 *)P.out + (i64)comp * P.out_np * P.plane;
+          const float al = (float)P.alpha;
+          if (fast && P.cs_lo == 1 && ((roff + cbase) & 7) == 0) {
+            // 16 contiguous BF16 per piece plane: two 16-byte stores each
+            float x[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          const int n = n0 + c0 + j;
-          if (n >= P.N) break;
-          const i64 off = roff + (P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo : (i64)n * P.cs_lo);
-          if (P.out_pieces) {
-            float x = (float)P.alpha * v[j];
-            __nv_bfloat16 *o = (__nv_bfloat16 *)P.out + (i64)comp * P.out_np * P.plane + off;
+            for (int j = 0; j < 16; j++) x[j] = al * v[j];
             for (int p = 0; p < P.out_np; p++) {
-              const __nv_bfloat16 h = __float2bfloat16_rn(x);
-              o[(i64)p * P.plane] = h;
-              x -= __bfloat162float(h);
+              uint32_t w[8];
+#pragma unroll
+              for (int j = 0; j < 8; j++) {
+                const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * j]), h1 = __float2bfloat16_rn(x[2 * j + 1]);
+                x[2 * j] -= __bfloat162float(h0);
+                x[2 * j + 1] -= __bfloat162float(h1);
+                w[j] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+              }
+              uint4 *dst = (uint4 *)(o + (i64)p * P.plane + roff + cbase);
+              dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+              dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
             }
           } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+              const int n = nf + j;
+              if (n >= P.N) break;
+              const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo
+                                           : (P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo
+                                                     : (i64)n * P.cs_lo));
+              float x = al * v[j];
+              for (int p = 0; p < P.out_np; p++) {
+                const __nv_bfloat16 h = __float2bfloat16_rn(x);
+                o[(i64)p * P.plane + off] = h;
+                x -= __bfloat162float(h);
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const int n = nf + j;
+            if (n >= P.N) break;
+            const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo
+                                         : (P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo
+                                                   : (i64)n * P.cs_lo));
             double *o = (double *)P.out + 2 * off + comp;
             const double x = P.alpha * (double)v[j];
             if (P.atomic)
@@ -445,12 +493,18 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   static bool attr_set[64] = {false};
   int dev = 0;
   NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
   if (!attr_set[dev]) {
-    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(2)));
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(4)));
     attr_set[dev] = true;
   }
   dim3 grid((g.M + BM - 1) / BM, P.ntn * 2, g.nb * ksplit);
-  split_gemm_kernel<<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, P);
+  const int kiters = P.kb_per_split * std::max(P.nterms[0], P.nterms[1]);
+  if (g.out_pieces || kiters <= 48)
+    split_gemm_kernel<2><<<grid, THREADS, smem_bytes(2), s>>>(ma, mb, P);
+  else
+    split_gemm_kernel<4><<<grid, THREADS, smem_bytes(4), s>>>(ma, mb, P);
   NEDY_CHECK_LAUNCH();
 }
 
