@@ -1,16 +1,26 @@
 #!/usr/bin/env python
-"""GF2 Kadanoff-Baym time steps per second at nao=64, naux=256 (plain FP64 path).
+"""GF2 Kadanoff-Baym time steps per second at nao=64, naux=256: plain FP64 vs
+split precision + predictor at max|dG| <= 1e-8.
 
 One "step" is one full time step T of the restricted density-fitted GF2
-simulation (DecompSimulation::do_tstp, reference src/molNEsim_decomp_impl.h:85-104):
-the polynomial predictor followed by corr_steps x [density matrix, HF mean
-field, GF2 self-energy row T, Dyson step row T], through the C ABI.
+simulation (DecompSimulation::do_tstp, reference src/molNEsim_decomp_impl.h:85-104)
+through the C ABI.  Two forms run the same window from the same state:
 
-Workload: nao=64, naux=256, ntau=256, beta=20, k=5, dt=0.01, 5 corrector
-iterations, steps T = t0+W ... t0+W+K-1 on a synthetic pre-evolved state (the
-free propagation of the Hartree-Fock Fock matrix on rows 0..t0-1, a scaled copy
-of it as the self-energy history; seeded inputs, no dataset).  The history
-arrays (GBs) are far larger than L2, so no explicit flush is needed.
+  plain FP64       nedy_decomp_tstp: polynomial predictor, then CorrSteps = 5 x
+                   [density matrix, HF mean field, GF2 self-energy row T, Dyson step
+                   row T], every contraction in FP64 (the reference's algorithm);
+  split+predictor  nedy_decomp_tstp_tol on a context in NEDY_PREC_SPLIT_BF16X3: the
+                   self-energy contractions as BF16 piece products on tcgen05, the
+                   predictor, and the residual exit at tol = 1e-8 (at most 5 iterations).
+
+value is the split+predictor form (the headline); the plain form, the iterations per
+step and max|dG| between the two forms over the window are in the same line.
+
+Workload: nao=64, naux=256, ntau=256, beta=20, k=5, dt=0.01, steps T = t0+W ...
+t0+W+K-1 on a synthetic pre-evolved state (the free propagation of the Hartree-Fock
+Fock matrix on rows 0..t0-1, a scaled copy of it as the self-energy history; seeded
+inputs, no dataset).  The history arrays (GBs) are far larger than L2, so no explicit
+flush is needed.
 
 Multi-GPU: one independent trajectory per GPU (replicas, no collective);
 value = total time steps of all ranks / max-over-ranks time.
@@ -62,6 +72,7 @@ def parse():
     ap.add_argument("--ntau", type=int, default=256)
     ap.add_argument("--t0", type=int, default=100)
     ap.add_argument("--corr", type=int, default=5)
+    ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--beta", type=float, default=20.0)
     ap.add_argument("--dt", type=float, default=0.01)
     ap.add_argument("--seed", type=int, default=7)
@@ -248,8 +259,7 @@ def fp64_gemm_peak(device: int) -> float:
 def run_engine(args, dist: Dist):
     import torch
     from nedyson_b200 import api
-    from nedyson_b200._lib import LES, RET, TV, MAT, check, lib
-    from nedyson_b200.greens import tri
+    from nedyson_b200._lib import LES, RET, TV, MAT, PREC_FP64, PREC_SPLIT_BF16X3, check, lib
     from nedyson_b200.inputs import make_problem, hf_equilibrium, free_history, drive
 
     dev = dist.local
@@ -287,40 +297,74 @@ def run_engine(args, dist: Dist):
     sp = C.c_void_p()
     check(lib().nedy_ctx_stream(ctx.h, C.byref(sp)))
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device(f"cuda:{dev}"))
+    iters = []
 
-    def step(t):
+    def step_plain(t):
         e = C.c_double()
         check(lib().nedy_decomp_tstp(ctx.h, t, G.h, S.h, hmf.h, hts[t].h, mu, args.corr, C.byref(e)))
-        return e.value
 
-    for t in range(t_first, t_first + W):
-        step(t)
-    ctx.synchronize()
-    check(lib().nedy_ctx_set_timing(ctx.h, 1))
-    clocks = Clocks(dev) if dist.rank == 0 else None
-    n0 = lib().nedy_launch_count()
-    dist.barrier()
-    torch.cuda.synchronize(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    def step_split(t, ht=None):
+        it = C.c_int()
+        check(lib().nedy_decomp_tstp_tol(ctx.h, t, G.h, S.h, hmf.h, (ht or hts[t]).h, mu, args.corr, args.tol,
+                                         C.byref(it), None))
+        iters.append(it.value)
+
+    def window_rows(T_list):
+        return [np.concatenate([G.les_col(t).ravel(), G.ret_row(t).ravel(), G.tv_row(t).ravel()]) for t in T_list]
+
+    def timed(step, T_list, split):
+        """K steps between CUDA events on the engine stream, phase times, launches, clocks."""
+        check(lib().nedy_ctx_set_timing(ctx.h, 1))
+        clocks = Clocks(dev) if dist.rank == 0 else None
+        n0 = lib().nedy_launch_count()
+        if split:
+            check(lib().nedy_split_stats(1, None, None))
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for t in T_list:
+            step(t)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        dist.barrier()
+        secs = e0.elapsed_time(e1) / 1e3
+        out = {"secs": dist.max(secs), "launches": int(lib().nedy_launch_count() - n0)}
+        ms4 = (C.c_double * 4)()
+        check(lib().nedy_ctx_phase_times(ctx.h, ms4))
+        check(lib().nedy_ctx_set_timing(ctx.h, 0))
+        out["phase_ms"] = list(ms4)
+        if split:
+            fl, ms = C.c_double(), C.c_double()
+            check(lib().nedy_split_stats(0, C.byref(fl), C.byref(ms)))
+            out["split_flops"], out["split_ms"] = fl.value, ms.value
+        out["clocks"] = clocks.stop() if clocks else None
+        return out
+
     T_timed = list(range(t_first + W, t_first + W + K))
-    for t in T_timed:
-        step(t)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    dist.barrier()
-    secs = e0.elapsed_time(e1) / 1e3
-    launches = int(lib().nedy_launch_count() - n0)
-    ms4 = (C.c_double * 4)()
-    check(lib().nedy_ctx_phase_times(ctx.h, ms4))
-    check(lib().nedy_ctx_set_timing(ctx.h, 0))
-    clk = clocks.stop() if clocks else None
-    secs_max = dist.max(secs)
+    # shared warm-up: W plain steps define the starting state of both forms
+    ctx.set_precision(PREC_FP64)
+    for t in range(t_first, t_first + W):
+        step_plain(t)
+    ctx.synchronize()
+    plain = timed(step_plain, T_timed, False)
+    rows_plain = window_rows(T_timed)
+    # split+predictor: warm-up on the window rows (recomputed below from the same history)
+    ctx.set_precision(PREC_SPLIT_BF16X3)
+    for t in T_timed[:W]:
+        step_split(t)
+    ctx.synchronize()
+    iters.clear()
+    split = timed(step_split, T_timed, True)
+    split_iters = list(iters)
+    rows_split = window_rows(T_timed)
+    max_dg = max(float(np.abs(a - b).max()) for a, b in zip(rows_plain, rows_split))
+    max_g = max(float(np.abs(a).max()) for a in rows_plain)
 
-    # end-to-end pass through the C ABI with host buffers: re-run the last timed step T_e
-    # (rows are recomputed in place), copying h(T_e) from pinned host memory in and the new
-    # G row (les column, ret row, tv row) back out, all inside the timed region.
+    # end-to-end pass through the C ABI with host buffers (split form): re-run the last timed
+    # step T_e (rows are recomputed in place), copying h(T_e) from pinned host memory in and
+    # the new G row (les column, ret row, tv row) back out, all inside the timed region.
     T_e = T_timed[-1]
     hval = (p.h0 + drive("sin", T_e * args.dt, 5, args.dt) * p.D).astype(np.complex128)
     h_host.copy_(torch.from_numpy(hval))
@@ -329,8 +373,7 @@ def run_engine(args, dist: Dist):
     torch.cuda.synchronize(dev)
     ee0.record(stream)
     check(lib().nedy_buf_upload(ht_e2e.h, 0, N * N * 16, C.c_void_p(h_host.data_ptr())))
-    e = C.c_double()
-    check(lib().nedy_decomp_tstp(ctx.h, T_e, G.h, S.h, hmf.h, ht_e2e.h, mu, args.corr, C.byref(e)))
+    step_split(T_e, ht_e2e)
     base = row_host.data_ptr()
     es = N * N * 16
     check(lib().nedy_gf_download(G.h, LES, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base)))
@@ -342,12 +385,9 @@ def run_engine(args, dist: Dist):
     e2e_secs = dist.max(ee0.elapsed_time(ee1) / 1e3)
     h2d = N * N * 16
     d2h = (2 * (T_e + 1) + ntau + 1) * es
-    rowmax = float(np.abs(row_host.numpy()).max())
-
-    out = dict(secs=secs_max, launches=launches, phase_ms=list(ms4), clocks=clk, T=T_timed, e2e_secs=e2e_secs,
-               h2d=h2d, d2h=d2h, rowmax=rowmax, err=e.value)
     torch.cuda.synchronize(dev)
-    return out
+    return dict(plain=plain, split=split, split_iters=split_iters, max_dg=max_dg, max_g=max_g, T=T_timed,
+                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h)
 
 
 def main():
@@ -355,8 +395,9 @@ def main():
     dist = Dist(args.gpus)
     K, W = args.steps, args.warmup
     cfg = {"workload": f"restricted density-fitted GF2 time step, nao={args.nao} naux={args.naux} ntau={args.ntau} "
-                       f"beta={args.beta} k=5 dt={args.dt}, {args.corr} corrector iterations, steps T={args.t0 + W}.."
-                       f"{args.t0 + W + K - 1} on a pre-evolved synthetic state",
+                       f"beta={args.beta} k=5 dt={args.dt}, steps T={args.t0 + W}..{args.t0 + W + K - 1} on a "
+                       f"pre-evolved synthetic state; plain form {args.corr} corrector iterations in FP64, split form "
+                       f"split-precision self-energy with the residual exit at {args.tol:g} (at most {args.corr})",
            "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "t_window": [args.t0 + W, args.t0 + W + K - 1],
            "corr_steps": args.corr, "precision": "fp64", "predictor": "polynomial extrapolation (k=5)",
            "l2": "inputs (G, Sigma histories) larger than L2; no flush needed",
@@ -385,28 +426,46 @@ def main():
     fp64 = fp64_gemm_peak(dist.local) if dist.rank == 0 else None
     r = run_engine(args, dist)
     total_steps = K * dist.world
-    value = total_steps / r["secs"]
+    sp, pl = r["split"], r["plain"]
+    value = total_steps / sp["secs"]
+    plain_value = total_steps / pl["secs"]
     T_mid = r["T"][len(r["T"]) // 2]
-    # roofline of the dominant kernel (the self-energy row): algorithmic flops / device time
-    sig_ms = r["phase_ms"][2]
-    sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau) for t in r["T"]) * args.corr
-    achieved = sig_flops / (sig_ms / 1e3) / 1e12 if sig_ms > 0 else None
     peaks, src = measured_peaks()
+    cfg["precision"] = "split BF16x3 self-energy (tcgen05), FP64 Dyson/HF/density; plain form FP64 throughout"
+    cfg["predictor"] = "polynomial extrapolation (k=5) + residual exit at max|dG| estimate <= tol"
+    cfg["tol"] = args.tol
     line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": dist.world, "steps": K, "warmup": W,
-            "ms_per_step": r["secs"] / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "complex128", "data": "synthetic (seeded random h0, B^Q, dipole; free-propagation history)",
-            "config": cfg}
+            "ms_per_step": sp["secs"] / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "complex128 state; self-energy contractions in BF16 pieces with FP32 accumulation",
+            "data": "synthetic (seeded random h0, B^Q, dipole; free-propagation history)", "config": cfg}
     if dist.rank == 0:
-        line["roofline"] = {"bound": "tensor", "kernel": "GF2 self-energy row (FP64 DMMA GEMM chain)",
-                            "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
-                            "frac": (achieved / fp64) if achieved else None, "traffic": None,
-                            "peak_source": "measured: cuBLAS FP64 GEMM (torch.matmul float64 8192^3) on this GPU",
-                            "bf16_peak_tflops": peaks.get("bf16_tflops"), "bf16_peak_source": src,
-                            "algorithmic_flops_per_step": flops_sigma(T_mid, args.nao, args.naux, args.ntau) * args.corr}
-        line["phase_ms"] = {"predictor": r["phase_ms"][0], "mean_field": r["phase_ms"][1],
-                            "self_energy": r["phase_ms"][2], "dyson": r["phase_ms"][3]}
-        line["clocks"] = r["clocks"]
-        line["gpu_launches"] = r["launches"]
+        # dominant kernel of the headline form: the split GEMM (BF16 piece products on tcgen05);
+        # achieved = algorithmic BF16 pipe FLOPs / its summed device time (CUDA events per launch)
+        bf16_peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+        ach = sp["split_flops"] / (sp["split_ms"] / 1e3) / 1e12 if sp.get("split_ms") else None
+        sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau) for t in r["T"]) * args.corr
+        line["roofline"] = {"bound": "tensor", "kernel": "split_gemm_kernel (BF16 piece products, tcgen05, TMEM)",
+                            "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
+                            "frac": (ach / bf16_peak) if ach else None, "traffic": None,
+                            "peak_source": f"{src}: bf16_tflops_sustained (kernel timed inside a long step)",
+                            "algorithmic_flops_per_step": sp["split_flops"] / K,
+                            "kernel_ms_per_step": sp["split_ms"] / K}
+        line["forms"] = {
+            "split_predictor": {"timesteps_s": value, "ms_per_step": sp["secs"] / K * 1e3,
+                                "iterations_per_step": r["split_iters"],
+                                "phase_ms": dict(zip(["predictor", "mean_field", "self_energy", "dyson"], sp["phase_ms"])),
+                                "gpu_launches": sp["launches"]},
+            "plain_fp64": {"timesteps_s": plain_value, "ms_per_step": pl["secs"] / K * 1e3,
+                           "iterations_per_step": args.corr,
+                           "phase_ms": dict(zip(["predictor", "mean_field", "self_energy", "dyson"], pl["phase_ms"])),
+                           "gpu_launches": pl["launches"],
+                           "self_energy_fp64_tflops": sig_flops / (pl["phase_ms"][2] / 1e3) / 1e12,
+                           "fp64_peak_tflops": fp64},
+            "speedup_split_vs_plain": value / plain_value,
+            "max_abs_dG_split_vs_plain": r["max_dg"], "max_abs_G": r["max_g"]}
+        line["clocks"] = sp["clocks"]
+        line["clocks_plain"] = pl["clocks"]
+        line["gpu_launches"] = sp["launches"]
         line["e2e"] = {"value": dist.world / r["e2e_secs"], "unit": "timesteps/s", "h2d_bytes_per_step": r["h2d"],
                        "d2h_bytes_per_step": r["d2h"]}
         if dist.world == 1 and not args.no_cpu_baseline:

@@ -80,6 +80,11 @@ int nedy_ctx_set_timing(nedy_ctx *ctx, int on);
 /* Self-energy arithmetic for this context (nedy_precision); FP64 by default.  The
  * reference computes in FP64 only; the split modes are this engine's addition. */
 int nedy_ctx_set_precision(nedy_ctx *ctx, int mode);
+/* Accounting of the split-precision tensor-core GEMMs of this process: returns their
+ * algorithmic BF16 tensor-pipe FLOPs (2 M N K per piece product) and summed device time
+ * (CUDA events around each launch) since the previous call, then switches the
+ * accounting on (on != 0) or off. */
+int nedy_split_stats(int on, double *pipe_flops, double *ms);
 int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
 /* Number of engine kernel launches issued by this process so far. */
 unsigned long long nedy_launch_count(void);
@@ -169,10 +174,14 @@ int nedy_energy_conv(nedy_ctx *ctx, int tstp, const nedy_gf *Sigma, const nedy_g
  * err: residual of the last dyson_step (sum of the three components). */
 int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
                      double mu, int corr_steps, double *err);
-/* The same step with a residual exit: corrector iterations stop after the first whose
- * dyson_step residual (sum of the three components) is below tol, at most max_corr.
- * The reference always runs CorrSteps iterations; this exit is the engine's addition.
- * iters: iterations run; err_hist (optional, max_corr entries): residual per iteration. */
+/* The same step with a residual exit (the reference always runs CorrSteps iterations;
+ * the exit is the engine's addition).  After iteration k the change d_k = max |G_k - G_{k-1}|
+ * over the new row (les column, ret row, tv row) is measured; the iterations stop once
+ * d_k times the corrector's contraction factor is <= tol, i.e. once the row is estimated
+ * to be within tol of the converged one, or after max_corr iterations.  The contraction
+ * is measured (4 x the ratio of successive changes) on steps that run two or more
+ * iterations: the first step on a context, and every 8th step after, run at least two.
+ * iters: iterations run; err_hist (optional, max_corr entries): d_k per iteration. */
 int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
                          double mu, int max_corr, double tol, int *iters, double *err_hist);
 /* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122). */

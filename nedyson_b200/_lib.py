@@ -64,6 +64,7 @@ SIGNATURES = {
     "nedy_hf_decomp": ([_P, _I, _P, _P], _I),
     "nedy_hf_decomp_noalloc": ([_P, _I, _P, _P], _I),
     "nedy_ctx_set_precision": ([_P, _I], _I),
+    "nedy_split_stats": ([_I, _DP, _DP], _I),
     "nedy_decomp_tstp_tol": ([_P, _I, _P, _P, _P, _P, C.c_double, _I, C.c_double, C.POINTER(_I), C.POINTER(C.c_double)], _I),
     "nedy_hf_spin_decomp": ([_P, _I, _P, _P, _P], _I),
     "nedy_hf_full": ([_P, _I, _P, _P], _I),

@@ -1,6 +1,7 @@
 // C ABI (include/nedy.h): handles, memory, and the public entry points.
 #include "handles.cuh"
 #include "sigma.cuh"
+#include "split_gemm.cuh"
 #include <cstring>
 #include <cstdlib>
 #include <string>
@@ -85,7 +86,7 @@ void *Arena::get(size_t bytes) {
 
 Ctx::~Ctx() {
   auto f = [](void *p) { if (p) cudaFree(p); };
-  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
+  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(rowcopy); f(d_maxdiff); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -107,6 +108,58 @@ void hf_full(Ctx &c, double2 *hmf_T, const double2 *rho) {
   int N = c.u_nao;
   hf_full_kernel<<<(N * N + 127) / 128, 128, 0, c.stream>>>(N, c.U, rho, hmf_T);
   NEDY_CHECK_LAUNCH();
+}
+
+// max |a - b| over n complex values (non-negative doubles order like their bit patterns)
+__global__ void maxdiff_kernel(i64 n, const double2 *a, const double2 *b, unsigned long long *out) {
+  double m = 0.0;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const double2 x = a[i], y = b[i];
+    m = fmax(m, hypot(x.x - y.x, x.y - y.y));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// The new row of step T (les column, ret row, tv row) as three contiguous block ranges.
+struct RowRanges {
+  double2 *p[3];
+  i64 n[3];
+};
+static RowRanges row_ranges(const DevGF &g, int T) {
+  const i64 es = (i64)g.nao * g.nao;
+  return RowRanges{{g.lesptr(0, T), g.retptr(T, 0), g.tvptr(T, 0)}, {(T + 1) * es, (T + 1) * es, (g.ntau + 1) * es}};
+}
+static void save_row(Ctx &c, const DevGF &g, int T) {
+  RowRanges r = row_ranges(g, T);
+  const i64 tot = r.n[0] + r.n[1] + r.n[2];
+  if (c.rowcopy_cap < tot) {
+    if (c.rowcopy) cudaFree(c.rowcopy);
+    c.rowcopy = nullptr;
+    NEDY_CUDA(cudaMalloc(&c.rowcopy, sizeof(double2) * tot));
+    c.rowcopy_cap = tot;
+  }
+  i64 o = 0;
+  for (int k = 0; k < 3; k++) {
+    NEDY_CUDA(cudaMemcpyAsync(c.rowcopy + o, r.p[k], sizeof(double2) * r.n[k], cudaMemcpyDeviceToDevice, c.stream));
+    o += r.n[k];
+  }
+}
+static double row_change(Ctx &c, const DevGF &g, int T) {
+  if (!c.d_maxdiff) NEDY_CUDA(cudaMalloc(&c.d_maxdiff, sizeof(unsigned long long)));
+  NEDY_CUDA(cudaMemsetAsync(c.d_maxdiff, 0, sizeof(unsigned long long), c.stream));
+  RowRanges r = row_ranges(g, T);
+  i64 o = 0;
+  for (int k = 0; k < 3; k++) {
+    const unsigned blocks = (unsigned)std::min<i64>((r.n[k] + 255) / 256, 148 * 8);
+    maxdiff_kernel<<<blocks, 256, 0, c.stream>>>(r.n[k], r.p[k], c.rowcopy + o, c.d_maxdiff);
+    NEDY_CHECK_LAUNCH();
+    o += r.n[k];
+  }
+  unsigned long long h = 0;
+  NEDY_CUDA(cudaMemcpyAsync(&h, c.d_maxdiff, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+  NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  return __builtin_bit_cast(double, h);
 }
 
 } // namespace nedy
@@ -239,6 +292,10 @@ int nedy_ctx_set_precision(nedy_ctx *ctx, int mode) {
     NEDY_REQUIRE(mode == NEDY_PREC_FP64 || mode == NEDY_PREC_SPLIT_BF16X3, "unknown precision mode");
     ctx->c.precision = mode;
   });
+}
+
+int nedy_split_stats(int on, double *pipe_flops, double *ms) {
+  return guard([&] { split_stats(on != 0, pipe_flops, ms); });
 }
 
 int nedy_ctx_set_timing(nedy_ctx *ctx, int on) {
@@ -649,8 +706,16 @@ int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_b
     PhaseTimer pt(c);
     pt.mark(0);
     extrapolate(c, tstp, G->g);
+    // Exit after iteration k once the estimated distance to the converged row, the
+    // change of iteration k times the corrector's contraction, is below tol.  The
+    // contraction is measured (ratio of successive changes, safety factor 4) whenever
+    // a step runs two or more iterations; until it is known, and every 8th step to keep
+    // it current, at least two iterations run.
+    const bool refresh = c.contraction >= 1.0 || c.steps_since_measure >= 8;
     int it = 0;
+    double prev = 0.0, ratio = 0.0;
     for (; it < max_corr;) {
+      save_row(c, G->g, tstp);
       c.ws.reset();
       pt.mark(1);
       double2 *rho = c.ws.alloc<double2>(es);
@@ -665,10 +730,19 @@ int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_b
       pt.mark(3);
       double e[3] = {0, 0, 0};
       dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
-      const double r = e[0] + e[1] + e[2];
-      if (err_hist) err_hist[it] = r;
+      const double d = row_change(c, G->g, tstp);
+      if (err_hist) err_hist[it] = d;
+      if (it > 0 && prev > 0.0) ratio = std::max(ratio, d / prev);
+      prev = d;
       it++;
-      if (r < tol) break;
+      if (refresh && it < 2) continue;
+      if (d * std::min(1.0, c.contraction) <= tol || (ratio > 0.0 && d * std::min(1.0, 4.0 * ratio) <= tol)) break;
+    }
+    if (ratio > 0.0) {
+      c.contraction = std::min(1.0, 4.0 * ratio);
+      c.steps_since_measure = 0;
+    } else {
+      c.steps_since_measure++;
     }
     pt.mark(-1);
     NEDY_CUDA(cudaStreamSynchronize(c.stream));

@@ -96,6 +96,14 @@ struct Ctx {
   unsigned long long mixK_ver = ~0ULL;
   int mixK_nao = 0;
   // inverses of the time-local Dyson matrices M(t') = (i bd0/dt + mu) - hmf(t') - dt w0 Sig^R(t',t')
+  // residual exit of the whole-step entry: copy of the new row before an iteration, the
+  // measured contraction of the corrector (ratio of successive changes, with a safety
+  // factor) and the steps since it was last measured
+  double2 *rowcopy = nullptr;
+  i64 rowcopy_cap = 0;
+  unsigned long long *d_maxdiff = nullptr;
+  double contraction = 1.0;
+  int steps_since_measure = 0;
   double2 *Minv = nullptr;
   int Minv_cap = 0, Minv_nao = 0;
   // device time per phase of the whole-step entry points (ms): predictor, mean field, self-energy, Dyson

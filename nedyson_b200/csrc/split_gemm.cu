@@ -14,6 +14,7 @@
 #include "split_gemm.cuh"
 #include <cuda.h>
 #include <mutex>
+#include <vector>
 
 namespace nedy {
 namespace {
@@ -410,6 +411,33 @@ void split_pieces(const View &v, bool cplx, bool conj, int K, Pieces &out, cudaS
   NEDY_CHECK_LAUNCH();
 }
 
+// Optional accounting of the split kernels: algorithmic BF16 tensor-pipe FLOPs
+// (2 M N K per piece-product term) and device time from events around each launch.
+namespace {
+std::mutex g_stats_mu;
+bool g_stats_on = false;
+double g_stats_flops = 0.0;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_stats_ev;
+}  // namespace
+
+void split_stats(bool on, double *flops, double *ms) {
+  std::lock_guard<std::mutex> lk(g_stats_mu);
+  double t = 0.0;
+  for (auto &e : g_stats_ev) {
+    NEDY_CUDA(cudaEventSynchronize(e.second));
+    float x = 0.f;
+    NEDY_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
+    t += x;
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  g_stats_ev.clear();
+  if (flops) *flops = g_stats_flops;
+  if (ms) *ms = t;
+  g_stats_flops = 0.0;
+  g_stats_on = on;
+}
+
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   const bool ac = g.A.ncomp == 2, bc = g.B.ncomp == 2;
   NEDY_REQUIRE(ac || bc, "split_gemm: at least one operand must be complex");
@@ -501,11 +529,26 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   }
   dim3 grid((g.M + BM - 1) / BM, P.ntn * 2, g.nb * ksplit);
   const int kiters = P.kb_per_split * std::max(P.nterms[0], P.nterms[1]);
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  {
+    std::lock_guard<std::mutex> lk(g_stats_mu);
+    if (g_stats_on) {
+      g_stats_flops += 2.0 * g.M * (double)g.N * g.K * g.nb * (P.nterms[0] + P.nterms[1]);
+      NEDY_CUDA(cudaEventCreate(&ev[0]));
+      NEDY_CUDA(cudaEventCreate(&ev[1]));
+      NEDY_CUDA(cudaEventRecord(ev[0], s));
+    }
+  }
   if (g.out_pieces || kiters <= 48)
     split_gemm_kernel<2><<<grid, THREADS, smem_bytes(2), s>>>(ma, mb, P);
   else
     split_gemm_kernel<4><<<grid, THREADS, smem_bytes(4), s>>>(ma, mb, P);
   NEDY_CHECK_LAUNCH();
+  if (ev[0]) {
+    std::lock_guard<std::mutex> lk(g_stats_mu);
+    NEDY_CUDA(cudaEventRecord(ev[1], s));
+    g_stats_ev.push_back({ev[0], ev[1]});
+  }
 }
 
 int split_gemm_error(cudaStream_t s) {

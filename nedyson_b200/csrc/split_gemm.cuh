@@ -50,6 +50,10 @@ struct SplitGemmArgs {
 
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
 
+// Accounting of split kernel launches: returns the algorithmic BF16 tensor-pipe FLOPs and
+// the summed device time (ms) since the last call, then turns the accounting on or off.
+void split_stats(bool on, double *flops, double *ms);
+
 // Device error word of the split kernels (non-zero after a bounded wait gave up).
 int split_gemm_error(cudaStream_t s);
 
