@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--t0", type=int, default=100)
     ap.add_argument("--corr", type=int, default=5)
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--state", default="trajectory", choices=["trajectory", "synthetic"])
+    ap.add_argument("--predictor", default="learned", choices=["learned", "poly"])
     ap.add_argument("--beta", type=float, default=20.0)
     ap.add_argument("--dt", type=float, default=0.01)
     ap.add_argument("--seed", type=int, default=7)
@@ -273,22 +275,60 @@ def run_engine(args, dist: Dist):
     x, _ = ctx.collocation()
     G = api.green_func(ctx, nt, ntau, N, -1)
     S = api.green_func(ctx, nt, ntau, N, -1)
-    les, ret, tv, mat = free_history(nt, t_first, ntau, x, mu, F, args.beta, args.dt)
-    G.upload(LES, 0, les)
-    G.upload(RET, 0, ret)
-    G.upload(TV, 0, tv)
-    G.upload(MAT, 0, mat)
-    S.upload(LES, 0, 0.02 * les)
-    S.upload(RET, 0, 0.02 * ret)
-    S.upload(TV, 0, 0.02 * tv)
-    del les, ret, tv
     solver = api.molGF2SolverDecomp(ctx, p.Vija)
     hm = np.zeros((nt + 1, N, N), np.complex128)
-    hm[:t_first] = F
-    hmf = api.hmf_buffer(ctx, N, hm)
-    # one-body Hamiltonian of every step, resident on the device (drive: 0.1 sin(2t) along D)
-    hts = [api.DeviceBuffer.from_array(ctx, (p.h0 + drive("sin", t * args.dt, 5, args.dt) * p.D).astype(np.complex128))
-           for t in range(nt + 1)]
+    kk = 5
+    traj = args.state == "trajectory"
+    # one-body Hamiltonian of every step, resident on the device.  Trajectory state: the
+    # Gaussian pulse E0 = 0.05, t0 = 2, sigma = 0.5 along D; synthetic state: 0.1 sin(2t).
+    dkind, dkw = ("gauss", {"E0": 0.05, "t0": 2.0, "sigma": 0.5}) if traj else ("sin", {})
+    hts = [api.DeviceBuffer.from_array(ctx, (p.h0 + drive(dkind, t * args.dt, kk, args.dt, **dkw) * p.D)
+                                       .astype(np.complex128)) for t in range(nt + 1)]
+    prep = {}
+    if traj:
+        # GF2 trajectory from the Hartree-Fock equilibrium: free propagation on rows 0..k as
+        # the bootstrap guess, dyson_start to self-consistency, then time steps up to t0-1
+        # (split form with the residual exit at 1e-10).
+        les, ret, tv, mat = free_history(nt, kk + 1, ntau, x, mu, F, args.beta, args.dt)
+        G.upload(LES, 0, les)
+        G.upload(RET, 0, ret)
+        G.upload(TV, 0, tv)
+        G.upload(MAT, 0, mat)
+        del les, ret, tv
+        hm[:kk + 1] = F
+        hmf = api.hmf_buffer(ctx, N, hm)
+        dy = api.dyson(ctx)
+        tp = time.time()
+        for it in range(40):
+            for t in range(kk + 1):
+                solver.solve(t, S, G)
+            berr = dy.dyson_start(G, S, hmf, mu)
+            if berr < 1e-12:
+                break
+        ctx.set_precision(PREC_SPLIT_BF16X3)
+        itc = C.c_int()
+        for t in range(kk + 1, t_first):
+            check(lib().nedy_decomp_tstp_tol(ctx.h, t, G.h, S.h, hmf.h, hts[t].h, mu, args.corr, 1e-10,
+                                             C.byref(itc), None))
+        ctx.synchronize()
+        prep = {"boot_iterations": it + 1, "boot_err": berr, "steps": t_first - kk - 1,
+                "seconds": time.time() - tp}
+    else:
+        les, ret, tv, mat = free_history(nt, t_first, ntau, x, mu, F, args.beta, args.dt)
+        G.upload(LES, 0, les)
+        G.upload(RET, 0, ret)
+        G.upload(TV, 0, tv)
+        G.upload(MAT, 0, mat)
+        S.upload(LES, 0, 0.02 * les)
+        S.upload(RET, 0, 0.02 * ret)
+        S.upload(TV, 0, 0.02 * tv)
+        del les, ret, tv
+        hm[:t_first] = F
+        hmf = api.hmf_buffer(ctx, N, hm)
+    # learned predictor: trained on small trajectories the engine generates (outside the timing)
+    pred, pred_info = None, None
+    if args.predictor == "learned":
+        pred, pred_info = train_predictor(ctx, args)
     # pinned host buffers for the end-to-end pass: h(t) in, new G row out
     row_blocks = 2 * (nt + 1) + (ntau + 1)
     h_host = torch.empty((N, N), dtype=torch.complex128).pin_memory()
@@ -352,6 +392,8 @@ def run_engine(args, dist: Dist):
     rows_plain = window_rows(T_timed)
     # split+predictor: warm-up on the window rows (recomputed below from the same history)
     ctx.set_precision(PREC_SPLIT_BF16X3)
+    if pred is not None:
+        ctx.set_predictor(pred)
     for t in T_timed[:W]:
         step_split(t)
     ctx.synchronize()
@@ -386,8 +428,41 @@ def run_engine(args, dist: Dist):
     h2d = N * N * 16
     d2h = (2 * (T_e + 1) + ntau + 1) * es
     torch.cuda.synchronize(dev)
+    pstats = ctx.predictor_stats() if pred is not None else None
     return dict(plain=plain, split=split, split_iters=split_iters, max_dg=max_dg, max_g=max_g, T=T_timed,
-                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h)
+                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h, prep=prep, pred_info=pred_info, pred_stats=pstats)
+
+
+def train_predictor(ctx, args):
+    """Train the learned predictor on short GF2 trajectories of small molecules (nao=8,
+    naux=24, Gaussian pulses of different strength and width), generated by the engine
+    itself with the corrector converged; returns the predictor on ctx and a summary."""
+    from nedyson_b200 import api
+    from nedyson_b200.inputs import make_problem
+    from nedyson_b200.simulation import DecompSimulation
+    t0 = time.time()
+    w, n, loss = None, 0, None
+    for seed, kw in [(11, {"E0": 0.1, "t0": 0.4, "sigma": 0.15}), (12, {"E0": 0.05, "t0": 0.3, "sigma": 0.1}),
+                     (14, {"E0": 0.08, "t0": 0.35, "sigma": 0.08})]:
+        sm = DecompSimulation(make_problem(8, 24, seed), 60, 32, 10.0, args.dt, drive_kind="gauss", drive_kw=kw,
+                              device=ctx.device)
+        sm.free_gf()
+        sm.do_boot()
+        P = api.Predictor(sm.ctx, 1 << 21, seed=5)
+        if w is not None:
+            P.set_params(w)
+        for t in range(6, sm.nt + 1):
+            sm.do_tstp_tol(t, 1e-13, 8)
+            if t >= 9:
+                P.collect(sm.G, t, 1)
+        n += P.samples()
+        loss = P.train(1500, 1024, 1e-3)
+        w = P.params()
+        P.close()
+        sm.ctx.close()
+    pred = api.Predictor(ctx, 1 << 10, seed=5)
+    pred.set_params(w)
+    return pred, {"trajectories": 3, "samples": n, "final_loss": loss, "seconds": time.time() - t0}
 
 
 def main():
@@ -432,12 +507,15 @@ def main():
     T_mid = r["T"][len(r["T"]) // 2]
     peaks, src = measured_peaks()
     cfg["precision"] = "split BF16x3 self-energy (tcgen05), FP64 Dyson/HF/density; plain form FP64 throughout"
-    cfg["predictor"] = "polynomial extrapolation (k=5) + residual exit at max|dG| estimate <= tol"
+    cfg["predictor"] = ("learned MLP correction of the k=5 extrapolation (polynomial fallback)" if args.predictor == "learned"
+                        else "polynomial extrapolation (k=5)") + " + residual exit at max|dG| estimate <= tol"
+    cfg["state"] = ("GF2 trajectory from the HF equilibrium (Gaussian pulse E0=0.05 t0=2 sigma=0.5)"
+                    if args.state == "trajectory" else "synthetic free-propagation history, 0.1 sin(2t) drive")
     cfg["tol"] = args.tol
     line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": dist.world, "steps": K, "warmup": W,
             "ms_per_step": sp["secs"] / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "complex128 state; self-energy contractions in BF16 pieces with FP32 accumulation",
-            "data": "synthetic (seeded random h0, B^Q, dipole; free-propagation history)", "config": cfg}
+            "data": ("synthetic (seeded random h0, B^Q, dipole); state: " + cfg["state"]), "config": cfg}
     if dist.rank == 0:
         # dominant kernel of the headline form: the split GEMM (BF16 piece products on tcgen05);
         # achieved = algorithmic BF16 pipe FLOPs / its summed device time (CUDA events per launch)
@@ -461,6 +539,8 @@ def main():
                            "gpu_launches": pl["launches"],
                            "self_energy_fp64_tflops": sig_flops / (pl["phase_ms"][2] / 1e3) / 1e12,
                            "fp64_peak_tflops": fp64},
+            "state_preparation": r["prep"], "predictor_training": r["pred_info"],
+            "predictor_stats": r["pred_stats"],
             "speedup_split_vs_plain": value / plain_value,
             "max_abs_dG_split_vs_plain": r["max_dg"], "max_abs_G": r["max_g"]}
         line["clocks"] = sp["clocks"]

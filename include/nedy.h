@@ -184,6 +184,40 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_b
  * iters: iterations run; err_hist (optional, max_corr entries): d_k per iteration. */
 int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
                          double mu, int max_corr, double tol, int *iters, double *err_hist);
+/* --- Learned next-step predictor (no counterpart in the reference, whose predictor is the
+ * polynomial extrapolation dyson::Extrapolate, src/dyson.cpp:47-117).  A 2-layer MLP of
+ * width 256 (BF16 operands, FP32 accumulation, FP32 master weights, Adam) corrects the
+ * k = 5 extrapolation of every element of the new row that has 9 history points and
+ * oscillates smoothly, from the three previous sixth differences of its time series.
+ * It is trained on the GPU on rows the engine converged (collect) and used by
+ * nedy_decomp_tstp_tol: after the first corrector iteration the step compares the
+ * learned and the polynomial prediction with the corrected row; once 8 steps are judged,
+ * fewer than 3 wins among the last 8 switch the context back to the polynomial predictor. */
+typedef struct nedy_predictor nedy_predictor;
+int nedy_predictor_create(nedy_ctx *ctx, long long capacity, unsigned long long seed, nedy_predictor **out);
+int nedy_predictor_destroy(nedy_predictor *p);
+/* training samples from the converged row tstp of G (every stride-th eligible element) */
+int nedy_predictor_collect(nedy_predictor *p, const nedy_gf *G, int tstp, int stride);
+int nedy_predictor_samples(nedy_predictor *p, long long *n);
+int nedy_predictor_clear(nedy_predictor *p);
+/* iters Adam steps on random minibatches of the collected samples; loss: last minibatch */
+int nedy_predictor_train(nedy_predictor *p, int iters, int batch, double lr, double *loss);
+/* number of parameters; copy them out (get != 0) or in (FP32: W1 256x12, b1, W2 256x256, b2, W3 2x256, b3) */
+long long nedy_predictor_nparams(void);
+int nedy_predictor_params(nedy_predictor *p, float *host, int get);
+/* forward pass on n host feature rows (n x 12) -> y (n x 2); loss 0.5 sum|y-t|^2 / n and
+ * its gradient (nparams floats) on host rows, for checks against a CPU restatement */
+int nedy_predictor_forward(nedy_predictor *p, const float *x, int n, float *y);
+int nedy_predictor_loss_grad(nedy_predictor *p, const float *x, const float *t, int n, double *loss, float *grad);
+/* the prediction of row tstp alone: dyson::Extrapolate, plus the learned correction of
+ * the context's predictor when learned != 0 */
+int nedy_predict(nedy_ctx *ctx, int tstp, nedy_gf *G, int learned);
+/* use p in nedy_decomp_tstp_tol of ctx (NULL: polynomial extrapolation only) */
+int nedy_ctx_set_predictor(nedy_ctx *ctx, nedy_predictor *p);
+/* active: learned predictor in use; judged / better: steps judged and won by it;
+ * last2: the last judged max changes from the learned and from the polynomial prediction */
+int nedy_ctx_predictor_stats(const nedy_ctx *ctx, int *active, long long *judged, long long *better, double *last2);
+
 /* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122). */
 int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
                           nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,

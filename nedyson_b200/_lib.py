@@ -65,6 +65,19 @@ SIGNATURES = {
     "nedy_hf_decomp_noalloc": ([_P, _I, _P, _P], _I),
     "nedy_ctx_set_precision": ([_P, _I], _I),
     "nedy_split_stats": ([_I, _DP, _DP], _I),
+    "nedy_predictor_create": ([_P, _LL, C.c_ulonglong, _PP], _I),
+    "nedy_predictor_destroy": ([_P], _I),
+    "nedy_predictor_collect": ([_P, _P, _I, _I], _I),
+    "nedy_predictor_samples": ([_P, C.POINTER(_LL)], _I),
+    "nedy_predictor_clear": ([_P], _I),
+    "nedy_predictor_train": ([_P, _I, _I, _D, _DP], _I),
+    "nedy_predictor_nparams": ([], _LL),
+    "nedy_predictor_params": ([_P, _P, _I], _I),
+    "nedy_predictor_forward": ([_P, _P, _I, _P], _I),
+    "nedy_predictor_loss_grad": ([_P, _P, _P, _I, _DP, _P], _I),
+    "nedy_predict": ([_P, _I, _P, _I], _I),
+    "nedy_ctx_set_predictor": ([_P, _P], _I),
+    "nedy_ctx_predictor_stats": ([_P, C.POINTER(_I), C.POINTER(_LL), C.POINTER(_LL), _DP], _I),
     "nedy_decomp_tstp_tol": ([_P, _I, _P, _P, _P, _P, C.c_double, _I, C.c_double, C.POINTER(_I), C.POINTER(C.c_double)], _I),
     "nedy_hf_spin_decomp": ([_P, _I, _P, _P, _P], _I),
     "nedy_hf_full": ([_P, _I, _P, _P], _I),

@@ -34,6 +34,7 @@ class Context:
     def __init__(self, nt, ntau, nao, k=5, beta=1.0, dt=0.01, device=0, workspace_bytes=0):
         self.nt, self.ntau, self.nao, self.k = int(nt), int(ntau), int(nao), int(k)
         self.beta, self.dt = float(beta), float(dt)
+        self.device = int(device)
         cfg = _lib.NedyConfig(self.nt, self.ntau, self.nao, self.k, self.beta, self.dt, int(device),
                               int(workspace_bytes))
         h = C.c_void_p()
@@ -57,6 +58,16 @@ class Context:
     def set_precision(self, mode):
         """Self-energy arithmetic: _lib.PREC_FP64 (default) or _lib.PREC_SPLIT_BF16X3."""
         check(lib().nedy_ctx_set_precision(self.h, int(mode)))
+
+    def set_predictor(self, pred: "Predictor | None"):
+        """Learned predictor for nedy_decomp_tstp_tol (None: polynomial extrapolation)."""
+        check(lib().nedy_ctx_set_predictor(self.h, pred.h if pred is not None else None))
+
+    def predictor_stats(self):
+        a, j, b = C.c_int(), C.c_longlong(), C.c_longlong()
+        last = (C.c_double * 2)()
+        check(lib().nedy_ctx_predictor_stats(self.h, C.byref(a), C.byref(j), C.byref(b), last))
+        return {"active": bool(a.value), "judged": j.value, "learned_better": b.value, "last": list(last)}
 
     def collocation(self):
         x = np.zeros(self.ntau + 1)
@@ -244,3 +255,70 @@ class dyson:
 
     def get_dm(self, G, tstp, rho: DeviceBuffer, offset=0):
         check(lib().nedy_get_dm(self.ctx.h, G.h, tstp, rho.h, offset))
+
+
+class Predictor:
+    """Learned next-step predictor (no reference counterpart; corrects dyson::Extrapolate).
+
+    2-layer MLP of width 256 on the three previous sixth differences of every element's
+    time series; trained on the GPU on rows the engine converged."""
+
+    IN = 12
+
+    def __init__(self, ctx: Context, capacity: int = 1 << 22, seed: int = 1):
+        self.ctx = ctx
+        h = C.c_void_p()
+        check(lib().nedy_predictor_create(ctx.h, int(capacity), int(seed), C.byref(h)))
+        self.h = h
+        self.nparams = int(lib().nedy_predictor_nparams())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nedy_predictor_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def collect(self, G: green_func, tstp: int, stride: int = 1):
+        check(lib().nedy_predictor_collect(self.h, G.h, int(tstp), int(stride)))
+
+    def samples(self) -> int:
+        n = C.c_longlong()
+        check(lib().nedy_predictor_samples(self.h, C.byref(n)))
+        return n.value
+
+    def clear(self):
+        check(lib().nedy_predictor_clear(self.h))
+
+    def train(self, iters: int, batch: int = 512, lr: float = 1e-3) -> float:
+        loss = C.c_double()
+        check(lib().nedy_predictor_train(self.h, int(iters), int(batch), float(lr), C.byref(loss)))
+        return loss.value
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.nparams, np.float32)
+        check(lib().nedy_predictor_params(self.h, _ptr(out), 1))
+        return out
+
+    def set_params(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == self.nparams
+        check(lib().nedy_predictor_params(self.h, _ptr(w), 0))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty((x.shape[0], 2), np.float32)
+        check(lib().nedy_predictor_forward(self.h, _ptr(x), x.shape[0], _ptr(y)))
+        return y
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.empty(self.nparams, np.float32)
+        loss = C.c_double()
+        check(lib().nedy_predictor_loss_grad(self.h, _ptr(x), _ptr(t), x.shape[0], C.byref(loss), _ptr(g)))
+        return loss.value, g

@@ -2,6 +2,7 @@
 #include "handles.cuh"
 #include "sigma.cuh"
 #include "split_gemm.cuh"
+#include "predictor.cuh"
 #include <cstring>
 #include <cstdlib>
 #include <string>
@@ -86,7 +87,7 @@ void *Arena::get(size_t bytes) {
 
 Ctx::~Ctx() {
   auto f = [](void *p) { if (p) cudaFree(p); };
-  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(rowcopy); f(d_maxdiff); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
+  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(rowcopy); f(d_maxdiff); f(pred_corr); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -706,6 +707,17 @@ int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_b
     PhaseTimer pt(c);
     pt.mark(0);
     extrapolate(c, tstp, G->g);
+    const i64 npred = c.pred ? Predictor::row_elements(G->g, tstp) : 0;
+    const bool learned = c.pred && c.pred_active && npred > 0;
+    if (learned) {
+      if (c.pred_corr_cap < npred) {
+        if (c.pred_corr) cudaFree(c.pred_corr);
+        c.pred_corr = nullptr;
+        NEDY_CUDA(cudaMalloc(&c.pred_corr, sizeof(double2) * npred));
+        c.pred_corr_cap = npred;
+      }
+      c.pred->apply(G->g, tstp, c.pred_corr);
+    }
     // Exit after iteration k once the estimated distance to the converged row, the
     // change of iteration k times the corrector's contraction, is below tol.  The
     // contraction is measured (ratio of successive changes, safety factor 4) whenever
@@ -732,6 +744,20 @@ int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_b
       dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
       const double d = row_change(c, G->g, tstp);
       if (err_hist) err_hist[it] = d;
+      if (learned && it == 0) {
+        // the first iteration judges the learned prediction against the polynomial one;
+        // once 8 steps are judged, fewer than 3 wins among the last 8 switch back to the
+        // polynomial predictor
+        double dl = 0, dp = 0;
+        c.pred->judge(G->g, tstp, c.rowcopy, c.pred_corr, dl, dp);
+        c.pred_last[0] = dl;
+        c.pred_last[1] = dp;
+        c.pred_judged++;
+        const bool won = dl <= dp;
+        if (won) c.pred_better++;
+        c.pred_window = (c.pred_window << 1) | (won ? 1u : 0u);
+        if (c.pred_judged >= 8 && __builtin_popcount(c.pred_window & 0xFFu) < 3) c.pred_active = false;
+      }
       if (it > 0 && prev > 0.0) ratio = std::max(ratio, d / prev);
       prev = d;
       it++;
@@ -748,6 +774,174 @@ int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_b
     NEDY_CUDA(cudaStreamSynchronize(c.stream));
     pt.collect();
     if (iters) *iters = it;
+  });
+}
+
+int nedy_predictor_create(nedy_ctx *ctx, long long capacity, unsigned long long seed, nedy_predictor **out) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && out && capacity > 0, "bad argument");
+    set_dev(ctx);
+    NEDY_REQUIRE(ctx->c.k == 5, "the learned predictor corrects the k = 5 extrapolation");
+    ensure_tables(ctx->c);
+    auto *h = new nedy_predictor;
+    h->ctx = ctx;
+    try {
+      h->p = new Predictor(ctx->c, capacity, seed);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int nedy_predictor_destroy(nedy_predictor *p) {
+  return guard([&] {
+    if (!p) return;
+    cudaSetDevice(p->p->ctx.device);
+    if (p->ctx->c.pred == p->p) {
+      p->ctx->c.pred = nullptr;
+      p->ctx->c.pred_active = false;
+    }
+    delete p->p;
+    delete p;
+  });
+}
+
+int nedy_predictor_collect(nedy_predictor *p, const nedy_gf *G, int tstp, int stride) {
+  return guard([&] {
+    NEDY_REQUIRE(p && G && tstp >= 0 && tstp <= G->g.nt, "bad argument");
+    set_dev(p->ctx);
+    p->p->collect(G->g, tstp, stride);
+  });
+}
+
+int nedy_predictor_samples(nedy_predictor *p, long long *n) {
+  return guard([&] {
+    NEDY_REQUIRE(p && n, "null argument");
+    set_dev(p->ctx);
+    *n = p->p->samples();
+  });
+}
+
+int nedy_predictor_clear(nedy_predictor *p) {
+  return guard([&] {
+    NEDY_REQUIRE(p, "null argument");
+    set_dev(p->ctx);
+    p->p->clear_samples();
+  });
+}
+
+int nedy_predictor_train(nedy_predictor *p, int iters, int batch, double lr, double *loss) {
+  return guard([&] {
+    NEDY_REQUIRE(p, "null argument");
+    set_dev(p->ctx);
+    const double l = p->p->train(iters, batch, lr);
+    if (loss) *loss = l;
+  });
+}
+
+long long nedy_predictor_nparams(void) { return PRED_NPARAM; }
+
+int nedy_predictor_params(nedy_predictor *p, float *host, int get) {
+  return guard([&] {
+    NEDY_REQUIRE(p && host, "null argument");
+    set_dev(p->ctx);
+    if (get)
+      p->p->get_params(host);
+    else
+      p->p->set_params(host);
+  });
+}
+
+int nedy_predictor_forward(nedy_predictor *p, const float *x, int n, float *y) {
+  return guard([&] {
+    NEDY_REQUIRE(p && x && y && n > 0, "bad argument");
+    set_dev(p->ctx);
+    Ctx &c = p->ctx->c;
+    float *d = nullptr;
+    NEDY_CUDA(cudaMalloc(&d, sizeof(float) * (size_t)n * (PRED_IN + 2 * PRED_W + 2)));
+    float *h1 = d + (i64)n * PRED_IN, *h2 = h1 + (i64)n * PRED_W, *yd = h2 + (i64)n * PRED_W;
+    cudaError_t e = cudaMemcpyAsync(d, x, sizeof(float) * n * PRED_IN, cudaMemcpyHostToDevice, c.stream);
+    if (e == cudaSuccess) {
+      try {
+        p->p->forward(n, d, h1, h2, yd);
+      } catch (...) {
+        cudaFree(d);
+        throw;
+      }
+      e = cudaMemcpyAsync(y, yd, sizeof(float) * n * 2, cudaMemcpyDeviceToHost, c.stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    cudaFree(d);
+    NEDY_CUDA(e);
+  });
+}
+
+int nedy_predictor_loss_grad(nedy_predictor *p, const float *x, const float *t, int n, double *loss, float *grad) {
+  return guard([&] {
+    NEDY_REQUIRE(p && x && t && n > 0, "bad argument");
+    set_dev(p->ctx);
+    Ctx &c = p->ctx->c;
+    float *d = nullptr;
+    NEDY_CUDA(cudaMalloc(&d, sizeof(float) * (size_t)n * (PRED_IN + 2)));
+    cudaError_t e = cudaMemcpyAsync(d, x, sizeof(float) * n * PRED_IN, cudaMemcpyHostToDevice, c.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d + (i64)n * PRED_IN, t, sizeof(float) * n * 2, cudaMemcpyHostToDevice, c.stream);
+    double l = 0;
+    if (e == cudaSuccess) {
+      try {
+        l = p->p->loss_grad(n, d, d + (i64)n * PRED_IN, true);
+      } catch (...) {
+        cudaFree(d);
+        throw;
+      }
+      if (grad) e = cudaMemcpyAsync(grad, p->p->grad(), sizeof(float) * PRED_NPARAM, cudaMemcpyDeviceToHost, c.stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    cudaFree(d);
+    NEDY_CUDA(e);
+    if (loss) *loss = l;
+  });
+}
+
+int nedy_predict(nedy_ctx *ctx, int tstp, nedy_gf *G, int learned) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G, "null argument");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    extrapolate(c, tstp, G->g);
+    if (learned) {
+      NEDY_REQUIRE(c.pred, "nedy_predict: no learned predictor set on this context");
+      c.pred->apply(G->g, tstp, nullptr);
+    }
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int nedy_ctx_set_predictor(nedy_ctx *ctx, nedy_predictor *p) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null context");
+    NEDY_REQUIRE(!p || p->ctx == ctx, "predictor belongs to another context");
+    Ctx &c = ctx->c;
+    c.pred = p ? p->p : nullptr;
+    c.pred_active = p != nullptr;
+    c.pred_window = 0;
+    c.pred_judged = c.pred_better = 0;
+  });
+}
+
+int nedy_ctx_predictor_stats(const nedy_ctx *ctx, int *active, long long *judged, long long *better, double *last2) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null context");
+    const Ctx &c = ctx->c;
+    if (active) *active = c.pred && c.pred_active ? 1 : 0;
+    if (judged) *judged = c.pred_judged;
+    if (better) *better = c.pred_better;
+    if (last2) {
+      last2[0] = c.pred_last[0];
+      last2[1] = c.pred_last[1];
+    }
   });
 }
 

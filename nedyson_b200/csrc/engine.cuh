@@ -61,6 +61,8 @@ struct Colloc {
 Colloc make_colloc(int ntau);
 void build_mixing_eval(Colloc &c);
 
+class Predictor;
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -104,6 +106,15 @@ struct Ctx {
   unsigned long long *d_maxdiff = nullptr;
   double contraction = 1.0;
   int steps_since_measure = 0;
+  // learned predictor used by the residual-exit step (not owned); its corrections of the
+  // current row, and how it fared against the polynomial prediction after iteration 1
+  Predictor *pred = nullptr;
+  bool pred_active = false;
+  double2 *pred_corr = nullptr;
+  i64 pred_corr_cap = 0;
+  long long pred_judged = 0, pred_better = 0;
+  unsigned pred_window = 0;  // outcomes of the last judged steps, one bit each (1: learned won)
+  double pred_last[2] = {0, 0};
   double2 *Minv = nullptr;
   int Minv_cap = 0, Minv_nao = 0;
   // device time per phase of the whole-step entry points (ms): predictor, mean field, self-energy, Dyson

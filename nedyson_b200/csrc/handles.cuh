@@ -22,6 +22,11 @@ struct nedy_buf {
   long long bytes;
 };
 
+struct nedy_predictor {
+  nedy_ctx *ctx;
+  nedy::Predictor *p;
+};
+
 namespace nedy {
 // Runs f, maps its exceptions to a nedy_status and records the message for
 // nedy_last_error (the same mapping every entry point uses).

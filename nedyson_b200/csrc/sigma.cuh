@@ -19,6 +19,8 @@ void get_dm(Ctx &c, const DevGF &G, int T, double2 *rho);
 
 // dyson::Extrapolate (dyson.cpp:47-117)
 void extrapolate(Ctx &c, int n, DevGF &G);
+// calculus tables (Gregory, BDF, extrapolation weights) on the device
+void ensure_tables(Ctx &c);
 // dyson::dyson_step (dyson_step.h:329-382); hmf: (nt+1) x nao x nao on the device.
 // Returns the sum of the three component errors (ret, tv, les) when err != nullptr.
 void dyson_step(Ctx &c, int n, DevGF &G, const DevGF &Sig, const double2 *hmf, double mu, double *err);

@@ -71,6 +71,18 @@ class DecompSimulation:
                                      self.corr_steps, C.byref(e)))
         return e.value
 
+    def do_tstp_tol(self, t: int, tol: float, max_corr: int | None = None):
+        """One step with the residual exit (nedy_decomp_tstp_tol): (iterations, changes per iteration)."""
+        import ctypes as C
+        from ._lib import check, lib
+        self.ht.upload(self.h_of_t(t))
+        m = max_corr or self.corr_steps
+        it = C.c_int()
+        hist = (C.c_double * m)()
+        check(lib().nedy_decomp_tstp_tol(self.ctx.h, t, self.G.h, self.Sigma.h, self.hmf.h, self.ht.h, self.mu, m,
+                                         float(tol), C.byref(it), hist))
+        return it.value, list(hist)[: it.value]
+
     def run(self, nt: int | None = None, boot_iter: int = 50, boot_tol: float = 1e-12):
         self.free_gf()
         self.do_boot(boot_iter, boot_tol)

@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "nedy.h")
 
 def declared():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char \*|unsigned long long)\s*(nedy_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*|unsigned long long|long long)\s*(nedy_\w+)\s*\(", src, re.M)))
 
 
 @pytest.fixture(scope="module")
