@@ -471,7 +471,7 @@ def main():
     K, W = args.steps, args.warmup
     cfg = {"workload": f"restricted density-fitted GF2 time step, nao={args.nao} naux={args.naux} ntau={args.ntau} "
                        f"beta={args.beta} k=5 dt={args.dt}, steps T={args.t0 + W}..{args.t0 + W + K - 1} on a "
-                       f"pre-evolved synthetic state; plain form {args.corr} corrector iterations in FP64, split form "
+                       f"pre-evolved {args.state} state; plain form {args.corr} corrector iterations in FP64, split form "
                        f"split-precision self-energy with the residual exit at {args.tol:g} (at most {args.corr})",
            "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "t_window": [args.t0 + W, args.t0 + W + K - 1],
            "corr_steps": args.corr, "precision": "fp64", "predictor": "polynomial extrapolation (k=5)",
