@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--state", default="trajectory", choices=["trajectory", "synthetic"])
     ap.add_argument("--predictor", default="learned", choices=["learned", "poly"])
+    ap.add_argument("--split-only", action="store_true",
+                    help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
     ap.add_argument("--beta", type=float, default=20.0)
     ap.add_argument("--dt", type=float, default=0.01)
     ap.add_argument("--seed", type=int, default=7)
@@ -384,12 +386,14 @@ def run_engine(args, dist: Dist):
 
     T_timed = list(range(t_first + W, t_first + W + K))
     # shared warm-up: W plain steps define the starting state of both forms
-    ctx.set_precision(PREC_FP64)
+    ctx.set_precision(PREC_SPLIT_BF16X3 if args.split_only else PREC_FP64)
     for t in range(t_first, t_first + W):
-        step_plain(t)
+        (step_split if args.split_only else step_plain)(t)
     ctx.synchronize()
-    plain = timed(step_plain, T_timed, False)
-    rows_plain = window_rows(T_timed)
+    plain, rows_plain = None, None
+    if not args.split_only:
+        plain = timed(step_plain, T_timed, False)
+        rows_plain = window_rows(T_timed)
     # split+predictor: warm-up on the window rows (recomputed below from the same history)
     ctx.set_precision(PREC_SPLIT_BF16X3)
     if pred is not None:
@@ -401,8 +405,8 @@ def run_engine(args, dist: Dist):
     split = timed(step_split, T_timed, True)
     split_iters = list(iters)
     rows_split = window_rows(T_timed)
-    max_dg = max(float(np.abs(a - b).max()) for a, b in zip(rows_plain, rows_split))
-    max_g = max(float(np.abs(a).max()) for a in rows_plain)
+    max_dg = max(float(np.abs(a - b).max()) for a, b in zip(rows_plain, rows_split)) if rows_plain else None
+    max_g = max(float(np.abs(a).max()) for a in rows_split)
 
     # end-to-end pass through the C ABI with host buffers (split form): re-run the last timed
     # step T_e (rows are recomputed in place), copying h(T_e) from pinned host memory in and
@@ -503,7 +507,7 @@ def main():
     total_steps = K * dist.world
     sp, pl = r["split"], r["plain"]
     value = total_steps / sp["secs"]
-    plain_value = total_steps / pl["secs"]
+    plain_value = total_steps / pl["secs"] if pl else None
     T_mid = r["T"][len(r["T"]) // 2]
     peaks, src = measured_peaks()
     cfg["precision"] = "split BF16x3 self-energy (tcgen05), FP64 Dyson/HF/density; plain form FP64 throughout"
@@ -538,13 +542,13 @@ def main():
                            "phase_ms": dict(zip(["predictor", "mean_field", "self_energy", "dyson"], pl["phase_ms"])),
                            "gpu_launches": pl["launches"],
                            "self_energy_fp64_tflops": sig_flops / (pl["phase_ms"][2] / 1e3) / 1e12,
-                           "fp64_peak_tflops": fp64},
+                           "fp64_peak_tflops": fp64} if pl else None,
             "state_preparation": r["prep"], "predictor_training": r["pred_info"],
             "predictor_stats": r["pred_stats"],
-            "speedup_split_vs_plain": value / plain_value,
+            "speedup_split_vs_plain": value / plain_value if pl else None,
             "max_abs_dG_split_vs_plain": r["max_dg"], "max_abs_G": r["max_g"]}
         line["clocks"] = sp["clocks"]
-        line["clocks_plain"] = pl["clocks"]
+        line["clocks_plain"] = pl["clocks"] if pl else None
         line["gpu_launches"] = sp["launches"]
         line["e2e"] = {"value": dist.world / r["e2e_secs"], "unit": "timesteps/s", "h2d_bytes_per_step": r["h2d"],
                        "d2h_bytes_per_step": r["d2h"]}

@@ -146,9 +146,11 @@ __global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  const int comp = blockIdx.y % P.ncomp_out, nt = blockIdx.y / P.ncomp_out;
+  // x: output part fastest (the real- and imaginary-part CTAs of a tile read the same A and
+  // B planes and run together, so the second reads them from L2), then N tiles; y: M tiles
+  const int comp = blockIdx.x % P.ncomp_out, nt = blockIdx.x / P.ncomp_out;
   const int b = blockIdx.z / P.ksplit, ks = blockIdx.z - (blockIdx.z / P.ksplit) * P.ksplit;
-  const int m0 = blockIdx.x * BM, n0 = nt * BN;
+  const int m0 = blockIdx.y * BM, n0 = nt * BN;
   const int kb0 = ks * P.kb_per_split;
   const int nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
   int iters = nkb * P.nterms[comp];
@@ -495,7 +497,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   NEDY_REQUIRE(ksplit == 1 || (g.accumulate && !g.out_pieces), "split_gemm: K split needs an accumulating FP64 output");
   P.ksplit = ksplit;
   P.kb_per_split = (P.kblocks + ksplit - 1) / ksplit;
-  NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && (i64)P.ntn * 2 <= 65535, "split_gemm: grid too large");
+  NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && (i64)(g.M + BM - 1) / BM <= 65535, "split_gemm: grid too large");
   P.out_pieces = g.out_pieces ? 1 : 0;
   P.accumulate = g.accumulate ? 1 : 0;
   P.atomic = ksplit > 1 ? 1 : 0;
@@ -527,7 +529,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(4)));
     attr_set[dev] = true;
   }
-  dim3 grid((g.M + BM - 1) / BM, P.ntn * 2, g.nb * ksplit);
+  dim3 grid(P.ntn * 2, (g.M + BM - 1) / BM, g.nb * ksplit);
   const int kiters = P.kb_per_split * std::max(P.nterms[0], P.nterms[1]);
   cudaEvent_t ev[2] = {nullptr, nullptr};
   {
