@@ -962,7 +962,9 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
     NEDY_CUDA(cudaMemcpyAsync(X + es, Qs, sizeof(double2) * kn * N, cudaMemcpyDeviceToDevice, c.stream));
   }
   // sequential m = k+1 .. n-1, then the diagonal
-  const int LC = 8;  // blocks per split-K chunk of the pull sums
+  // blocks per split-K chunk of the pull sums: one block per CTA, so the sequential
+  // step m runs m CTAs (each 64x64x64 at nao=64) instead of m/8 long ones
+  const int LC = 1;
   for (int m = k + 1; m <= n; m++) {
     // Q_m += sum_{l<m} dt w(m,l) Sig^R(m,l) X_l   (split-K over l in chunks of LC blocks, atomics)
     for (int part = 0; part < 2; part++) {
