@@ -87,7 +87,7 @@ void *Arena::get(size_t bytes) {
 
 Ctx::~Ctx() {
   auto f = [](void *p) { if (p) cudaFree(p); };
-  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(rowcopy); f(d_maxdiff); f(pred_corr); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
+  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(Vanj_p); f(Vjkb_p); f(Vila_p); f(rowcopy); f(d_maxdiff); f(pred_corr); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -506,8 +506,10 @@ int nedy_set_df_tensor(nedy_ctx *ctx, const double *Vija, int nao, int naux) {
     put(c.Viaj, viaj.data());
     put(c.Vaij, vaij.data());
     put(c.Vmbq, vmbq.data());
-    if (c.Vp) cudaFree(c.Vp);  // pieces of the previous tensor
-    c.Vp = nullptr;
+    for (void **q : {&c.Vp, &c.Vanj_p, &c.Vjkb_p, &c.Vila_p}) {  // pieces of the previous tensor
+      if (*q) cudaFree(*q);
+      *q = nullptr;
+    }
     c.Vp_np = 0;
     c.df_nao = nao;
     c.df_naux = naux;

@@ -89,6 +89,9 @@ struct Ctx {
   int precision = 0;
   void *Vp = nullptr;
   int Vp_np = 0;
+  // further BF16-piece layouts of the interaction for the all-split les-form chain:
+  // [(a,n)][j] = V^a_nj, [(j,k)][b] = V^b_kj, [i][(l,a)] = V^a_il
+  void *Vanj_p = nullptr, *Vjkb_p = nullptr, *Vila_p = nullptr;
   // full U (N^4 real) and the exchange combination Uexch
   int u_nao = 0;
   double *U = nullptr, *Uexch = nullptr;

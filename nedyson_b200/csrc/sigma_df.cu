@@ -216,6 +216,127 @@ struct DF {
   }
   i64 pz_bytes(int np) const { return (i64)2 * np * nsl * A * kpad64((int)es) * 2; }
   i64 pp_bytes(int np) const { return (i64)2 * np * nsl * A * kpad64(A) * 2; }
+  // ---- all-split chain of the les-form units (X, Y, Z = X): every operand a BF16-piece
+  // array written directly by the producing contraction in the layout its consumer reads.
+  Pieces static_pieces(void *&slot, const View &v, int rows, int K, int np) {
+    Pieces x;
+    x.rows = rows; x.kpad = kpad64(K); x.nb = 1; x.ncomp = 1; x.np = np;
+    if (!slot) {
+      NEDY_CUDA(cudaMalloc(&slot, x.elems() * 2));
+      x.p = (__nv_bfloat16 *)slot;
+      split_pieces(v, false, false, K, x, s);
+    }
+    x.p = (__nv_bfloat16 *)slot;
+    return x;
+  }
+  Pieces vanj(int np) {  // rows (a,n), K = j: V^a_nj = Vija[n][j][a]
+    View v; v.p = c.Vija; v.rdiv = N; v.rs_hi = 1; v.rs_lo = NA; v.cs_lo = A;
+    return static_pieces(c.Vanj_p, v, (int)NA, N, np);
+  }
+  Pieces vjkb(int np) {  // rows (j,k), K = b: V^b_kj = Vija[k][j][b] (= Vija rows (j,k) when symmetric)
+    if (c.V_sym) return vpieces(np);
+    View v; v.p = c.Vija; v.rdiv = N; v.rs_hi = A; v.rs_lo = NA; v.cs_lo = 1;
+    return static_pieces(c.Vjkb_p, v, (int)es, A, np);
+  }
+  Pieces vila(int np) {  // rows i, K = (l,a): Vija[i][l][a]
+    return static_pieces(c.Vila_p, rowmajor(c.Vija, NA), N, (int)NA, np);
+  }
+  Pieces arr(void *p, int rows, int K, int nb, int np) {
+    Pieces x;
+    x.p = (__nv_bfloat16 *)p; x.rows = rows; x.kpad = kpad64(K); x.nb = nb; x.ncomp = 2; x.np = np;
+    return x;
+  }
+  static i64 arr_bytes(int rows, int K, int nb, int np) { return (i64)2 * np * nb * rows * kpad64(K) * 2; }
+  // C (pieces, zero-padded K) = A * B^T
+  void to_pieces(const Pieces &a, const Pieces &b, int M, int Nn, int K, Pieces &out, const View &ov, int nb,
+                 int out_K) {
+    if (out.kpad != out_K) NEDY_CUDA(cudaMemsetAsync(out.p, 0, out.elems() * 2, s));
+    SplitGemmArgs g;
+    g.M = M; g.N = Nn; g.K = K; g.nb = nb;
+    g.A = a; g.B = b;
+    g.out_pieces = true; g.Cp = out; g.C = ov;
+    split_gemm(g, s);
+  }
+  // C (FP64, accumulated) += alpha * A * B^T
+  void to_fp64(const Pieces &a, const Pieces &b, int M, int Nn, int K, const View &cv, int nb, double alpha) {
+    SplitGemmArgs g;
+    g.M = M; g.N = Nn; g.K = K; g.nb = nb;
+    g.A = a; g.B = b;
+    g.C = cv; g.alpha = alpha; g.accumulate = true;
+    split_gemm(g, s);
+  }
+  Pieces blk_pieces(Blocks b, bool transpose, void *buf, int np) {
+    Pieces x = arr(buf, N, N, nsl, np);
+    split_pieces(transpose ? blkT(b, N) : blk(b, N), true, false, N, x, s);
+    return x;
+  }
+  // VZa = [a][(q,n)] pieces of (V^a Z)_nq for P (A operand) and Q (B operand)
+  Pieces VZa(const Pieces &zt, void *buf, int np) {
+    Pieces o = arr(buf, A, (int)es, nsl, np);
+    View v; v.rdiv = N; v.rs_hi = o.kpad; v.rs_lo = 1; v.cs_lo = N; v.bs1 = (i64)A * o.kpad;
+    to_pieces(vanj(np), zt, (int)NA, N, N, o, v, nsl, (int)es);
+    return o;
+  }
+  // VYb = [b][(q,n)] pieces of (V^b Y)_qn for P (B operand)
+  Pieces VYb(const Pieces &yt, void *buf, int np) {
+    Pieces o = arr(buf, A, (int)es, nsl, np);
+    View v; v.rdiv = N; v.rs_hi = o.kpad; v.rs_lo = N; v.cs_lo = 1; v.bs1 = (i64)A * o.kpad;
+    to_pieces(vanj(np), yt, (int)NA, N, N, o, v, nsl, (int)es);
+    return o;
+  }
+  // VZn = [n][(a,k)] pieces of (V^a X)_nk for the bubble contraction (A operand)
+  Pieces VZn(const Pieces &xt, void *buf, int np) {
+    Pieces o = arr(buf, N, (int)NA, nsl, np);
+    View v; v.rdiv = N; v.rs_hi = N; v.rs_lo = o.kpad; v.cs_lo = 1; v.bs1 = (i64)N * o.kpad;
+    to_pieces(vanj(np), xt, (int)NA, N, N, o, v, nsl, (int)NA);
+    return o;
+  }
+  // VYp = [(n,b)][k] pieces of (V^b Y)_kn for the M contraction (B operand)
+  Pieces VYp(const Pieces &yt, void *buf, int np) {
+    Pieces o = arr(buf, (int)NA, N, nsl, np);
+    View v; v.rdiv = N; v.rs_hi = o.kpad; v.rs_lo = 1; v.cs_lo = (i64)A * o.kpad; v.bs1 = NA * o.kpad;
+    to_pieces(vanj(np), yt, (int)NA, N, N, o, v, nsl, N);
+    return o;
+  }
+  // Wp = [j][(a,k)] pieces of W[a][k][j] = sum_b P[a][b] V^b_kj (B operand of the bubble)
+  Pieces Wp(const Pieces &pp, void *buf, int np) {
+    Pieces o = arr(buf, N, (int)NA, nsl, np);
+    View v; v.rdiv = N; v.rs_hi = o.kpad; v.rs_lo = 1; v.cs_lo = N; v.bs1 = (i64)N * o.kpad;
+    to_pieces(vjkb(np), pp, (int)es, A, A, o, v, nsl, (int)NA);
+    return o;
+  }
+  // exchange of units u0..u0+nu-1: Mp = X VY, S', Q, Sigma -= V Q
+  void ExchAllSplit(int u0, int nu, const Pieces &xp, const Pieces &vyp, const Pieces &vza, Blocks Sig, double2 *Q,
+                    void *wsS, void *wsM, void *wsQ, int np) {
+    const int kpN = kpad64((int)es);
+    Pieces xs = xp, vs = vyp, zs = vza;
+    xs.b0 = vs.b0 = zs.b0 = u0;
+    Pieces Mp;
+    Mp.p = (__nv_bfloat16 *)wsM; Mp.rows = (int)es; Mp.kpad = kpad64(A); Mp.nb = nu; Mp.ncomp = 2; Mp.np = np;
+    {
+      View v; v.rs_lo = (i64)N * Mp.kpad; v.cdiv = A; v.cs_hi = Mp.kpad; v.cs_lo = 1; v.bs1 = es * Mp.kpad;
+      to_pieces(xs, vs, N, (int)NA, N, Mp, v, nu, A);
+    }
+    Pieces Sp;
+    Sp.p = (__nv_bfloat16 *)wsS; Sp.rows = (int)es; Sp.kpad = kpN; Sp.nb = nu; Sp.ncomp = 2; Sp.np = np;
+    {
+      View v; v.rdiv = N; v.rs_hi = N; v.rs_lo = kpN; v.cdiv = N; v.cs_hi = (i64)N * kpN; v.cs_lo = 1; v.bs1 = es * kpN;
+      to_pieces(vpieces(np), Mp, (int)es, (int)es, A, Sp, v, nu, (int)es);
+    }
+    NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * nu * N2A, s));
+    {
+      View v; v.p = Q; v.rdiv = N; v.rs_hi = A; v.rs_lo = NA; v.cs_lo = 1; v.bs1 = N2A;
+      to_fp64(Sp, zs, (int)es, A, (int)es, v, nu, 1.0);
+    }
+    Pieces Qp;
+    Qp.p = (__nv_bfloat16 *)wsQ; Qp.rows = N; Qp.kpad = kpad64((int)NA); Qp.nb = nu; Qp.ncomp = 2; Qp.np = np;
+    {
+      View v = rowmajor(Q, NA); v.bs1 = N2A;
+      split_pieces(v, true, false, (int)NA, Qp, s);
+    }
+    to_fp64(vila(np), Qp, N, N, (int)NA, blk(Sig, N), nu, -1.0);
+  }
+
   // bytes of the MT / VZT piece planes for nu units
   i64 mz_bytes(int nu, int np) const {
     return std::max<i64>((i64)2 * np * nu * es * kpad64(A), (i64)2 * np * nu * A * kpad64((int)es)) * 2;
@@ -341,7 +462,7 @@ static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
   i64 budget = c.ws_budget;
   // per slice (retarded, the largest): 5 VZ/VYt + 3 VY + 2 M + Q + 2 P/W + prep
   i64 per = 13 * n2a + 2 * A * A * 16;
-  if (split) per += 3 * n2a;  // BF16 pieces of the bubble operands and the VZT layout
+  if (split) per += 6 * n2a;  // BF16 pieces of the operands (12 bytes per complex element each)
   sub = (int)std::max<i64>(1, std::min<i64>(16, (budget / 3) / n4));
   chunk = (int)std::max<i64>(1, std::min<i64>(64, (budget - sub * n4) / std::max<i64>(per, 1)));
   if (chunk < sub) sub = chunk;
@@ -383,6 +504,7 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
       DF d(c, nsl);
       double2 *Hb[2], *VZ[2], *VYt[2];
       Blocks X[2], Y[2];
+      const bool allsplit = split;  // les-form units: every contraction in split precision
       for (int s = 0; s < nspin; s++) {
         Hb[s] = c.ws.alloc<double2>(nsl * es);
         if (kind == 1) {
@@ -399,6 +521,7 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
             Y[s] = {G[s]->lesptr(t0, T), es};
           }
         }
+        if (allsplit) continue;
         VZ[s] = c.ws.alloc<double2>(nsl * N2A);
         VYt[s] = c.ws.alloc<double2>(nsl * N2A);
         d.VZ(X[s], VZ[s]);
@@ -408,6 +531,53 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
         return kind == 0 ? Blocks{Sig[s]->lesptr(t0, T), es}
                          : (kind == 1 ? Blocks{Sig[s]->tvptr(T, t0), es} : Blocks{Sig[s]->retptr(T, t0), es});
       };
+      if (allsplit) {
+        // each piece array sized for its own rows x padded K
+        const i64 bb = DF::arr_bytes(N, N, nsl, np), big = DF::arr_bytes(A, (int)es, nsl, np);
+        const i64 nk = DF::arr_bytes(N, (int)NA, nsl, np), vyk = DF::arr_bytes((int)NA, N, nsl, np);
+        Pieces xp[2], xtp[2], ytp[2], vza[2];
+        for (int s = 0; s < nspin; s++) {
+          xp[s] = d.blk_pieces(X[s], false, c.ws.get(bb), np);
+          xtp[s] = d.blk_pieces(X[s], true, c.ws.get(bb), np);
+          ytp[s] = d.blk_pieces(Y[s], true, c.ws.get(bb), np);
+          vza[s] = d.VZa(xtp[s], c.ws.get(big), np);
+        }
+        // bubble: P = sum_s VZa VYb^T (FP64), W pieces, Sigma_s += f VZn W
+        double2 *P = c.ws.alloc<double2>((i64)nsl * A * A);
+        NEDY_CUDA(cudaMemsetAsync(P, 0, sizeof(double2) * nsl * A * A, c.stream));
+        void *vyb = c.ws.get(big);
+        for (int s = 0; s < nspin; s++) {
+          Pieces yb = d.VYb(ytp[s], vyb, np);
+          View pv = rowmajor(P, A); pv.bs1 = (i64)A * A;
+          d.to_fp64(vza[s], yb, A, A, (int)es, pv, nsl, 1.0);
+        }
+        Pieces pp = d.arr(c.ws.get(DF::arr_bytes(A, A, nsl, np)), A, A, nsl, np);
+        {
+          View pv = rowmajor(P, A); pv.bs1 = (i64)A * A;
+          split_pieces(pv, true, false, A, pp, c.stream);
+        }
+        Pieces wp = d.Wp(pp, c.ws.get(nk), np);
+        void *vzn = c.ws.get(nk);
+        for (int s = 0; s < nspin; s++) {
+          Pieces zn = d.VZn(xtp[s], vzn, np);
+          d.to_fp64(zn, wp, N, N, (int)NA, blk(outb(s), N), nsl, fb);
+        }
+        // exchange per spin
+        double2 *Q = c.ws.alloc<double2>(nsl * N2A);
+        double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
+        void *vyp = c.ws.get(vyk);
+        void *Mb = c.ws.get(DF::arr_bytes((int)es, A, sub, np));
+        void *Qb = c.ws.get(DF::arr_bytes(N, (int)NA, sub, np));
+        for (int s = 0; s < nspin; s++) {
+          Pieces yp = d.VYp(ytp[s], vyp, np);
+          Blocks out = outb(s);
+          for (int u0 = 0; u0 < nsl; u0 += sub) {
+            const int nu = std::min(sub, nsl - u0);
+            d.ExchAllSplit(u0, nu, xp[s], yp, vza[s], {out.p + u0 * es, es}, Q + u0 * N2A, S, Mb, Qb, np);
+          }
+        }
+        continue;
+      }
       double2 *P = c.ws.alloc<double2>((i64)nsl * A * A);
       double2 *Wb = c.ws.alloc<double2>(nsl * N2A);
       if (split) {

@@ -1,16 +1,19 @@
 // Split-precision GEMM: BF16 piece products on tcgen05 with FP32 accumulation in
 // tensor memory, operands brought into shared memory by TMA (see split_gemm.cuh).
 //
-// One CTA computes a 128 x 256 tile of one output part (real or imaginary):
-//   warp 4      TMA producer (one thread): A tile 128 x 64 and B tile 256 x 64
-//               per stage, 4 stages, mbarrier transaction counts;
-//   warp 5      MMA issuer (one thread): 4 x tcgen05.mma (M128 N256 K16) per stage,
-//               tcgen05.commit frees the stage; owns the 256-column TMEM allocation;
-//   warps 0-3   epilogue: tcgen05.ld of their 32 TMEM lanes, FP64 or BF16-piece
-//               stores through the output View.
-// The K loop runs over (term, K block): a term is one (A plane, B plane, sign)
-// piece product.  Every mbarrier wait is bounded (2 s); a wait that gives up
-// sets the error word and the CTA drains and returns, so no launch can hang.
+// One CTA computes a 128 x BN tile of both output parts: the real part accumulates in
+// TMEM columns [0, BN), the imaginary part in [BN, 2 BN).
+//   warp 4      TMA producer (one thread): per stage the A tiles (128 x 64; real and
+//               imaginary plane of a complex operand) and B tiles (BN x 64) of one
+//               piece product and K block, mbarrier transaction counts;
+//   warp 5      MMA issuer (one thread): per stage 2 (complex x real) or 4 (complex x
+//               complex) tile products, each 4 x tcgen05.mma (M128 N BN K16) into the
+//               accumulator of its part, the instruction's negate bit giving the minus
+//               of Re = Ar Br - Ai Bi; tcgen05.commit frees the stage; owns the TMEM;
+//   warps 0-3   epilogue: tcgen05.ld of their 32 TMEM lanes of both parts, FP64 complex
+//               or BF16-piece stores through the output View.
+// Every mbarrier wait is bounded (2 s); a wait that gives up sets the error word and
+// the CTA drains and returns, so no launch can hang.
 #include "split_gemm.cuh"
 #include <cuda.h>
 #include <mutex>
@@ -19,24 +22,24 @@
 namespace nedy {
 namespace {
 
-constexpr int BM = 128, BN = 256, BK = 64, THREADS = 192;
-constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
-// STAGES 4: one CTA per SM (long K loops); STAGES 2: two CTAs per SM, so one CTA's
-// epilogue overlaps the other's main loop (short K loops with heavy epilogues)
-constexpr int smem_bytes(int stages) { return stages * STAGE_BYTES + 1024 + 128; }
-constexpr int MAX_TERMS = 12;
+constexpr int BM = 128, BK = 64, THREADS = 192;
+constexpr int A_BYTES = BM * BK * 2;
+constexpr int SMEM_LIMIT = 196608;  // operand stages per CTA (the rest: alignment, barriers)
 constexpr unsigned long long WAIT_NS = 2000000000ULL;
 
-struct Term {
-  signed char pa, pb, neg, pad;
+// one tile product of a stage: A slot, B slot, accumulator (0 real, 1 imaginary), negate A
+struct Mma {
+  signed char sa, sb, acc, neg;
 };
 
 struct Params {
   int M, N, kblocks, kb_per_split, ksplit, nb;
   int a_nb, b_nb;  // batches stored in the A / B maps (1: shared)
-  int ntn, ncomp_out;
-  int nterms[2];
-  Term terms[2][MAX_TERMS];
+  int a_b0, b_b0;  // first stored batch used
+  int nA, nB, nmma, nprod, np, stage_bytes;
+  int a_comp[2], b_comp[2];  // plane group (0 real, 1 imaginary) of each A / B slot
+  Mma mma[4];
+  int pa[6], pb[6];  // piece products
   // epilogue
   int out_pieces, out_np, accumulate, atomic;
   double alpha;
@@ -45,6 +48,8 @@ struct Params {
   int rdiv, cdiv;
   int *err;
 };
+
+constexpr int smem_bytes(int stage_bytes, int stages) { return stages * stage_bytes + 1024 + 256; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -106,8 +111,10 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = 256.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = bn.
+constexpr uint32_t idesc_for(int bn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   asm volatile(
@@ -134,26 +141,82 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-template <int STAGES>
-__global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
+// column offsets of a 16-column chunk: one division when the chunk stays inside one cdiv
+// segment (fast), then base + j * cs_lo
+__device__ __forceinline__ bool chunk_base(const Params &P, int nf, i64 &cbase) {
+  bool fast = nf + 16 <= P.N;
+  cbase = 0;
+  if (fast) {
+    if (P.cdiv) {
+      const int qd = nf / P.cdiv, rm = nf - qd * P.cdiv;
+      fast = rm + 16 <= P.cdiv;
+      cbase = (i64)qd * P.cs_hi + (i64)rm * P.cs_lo;
+    } else {
+      cbase = (i64)nf * P.cs_lo;
+    }
+  }
+  return fast;
+}
+__device__ __forceinline__ i64 col_off(const Params &P, int n) {
+  return P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo : (i64)n * P.cs_lo;
+}
+
+// BF16 pieces of 16 values into the np planes of one part
+__device__ __forceinline__ void store_pieces16(const Params &P, __nv_bfloat16 *o, i64 roff, i64 cbase, bool fast,
+                                               int nf, const float (&v)[16]) {
+  const float al = (float)P.alpha;
+  if (fast && P.cs_lo == 1 && ((roff + cbase) & 7) == 0) {
+    float x[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) x[j] = al * v[j];
+    for (int p = 0; p < P.out_np; p++) {
+      uint32_t w[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * j]), h1 = __float2bfloat16_rn(x[2 * j + 1]);
+        x[2 * j] -= __bfloat162float(h0);
+        x[2 * j + 1] -= __bfloat162float(h1);
+        w[j] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      }
+      uint4 *dst = (uint4 *)(o + (i64)p * P.plane + roff + cbase);
+      dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+      dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    }
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < 16; j++) {
+    const int n = nf + j;
+    if (n >= P.N) break;
+    const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo : col_off(P, n));
+    float x = al * v[j];
+    for (int p = 0; p < P.out_np; p++) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(x);
+      o[(i64)p * P.plane + off] = h;
+      x -= __bfloat162float(h);
+    }
+  }
+}
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                      const Params P) {
+                      const __grid_constant__ Params P) {
+  constexpr int B_BYTES = BN * BK * 2;
+  constexpr uint32_t TCOLS = 2 * BN;
+  constexpr uint32_t IDESC = idesc_for(BN);
   extern __shared__ uint8_t sraw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)sraw + 1023) & ~(uintptr_t)1023);
-  uint64_t *bar = (uint64_t *)(smem + STAGES * STAGE_BYTES);  // full[STAGES], empty[STAGES], done
+  uint64_t *bar = (uint64_t *)(smem + STAGES * P.stage_bytes);  // full[STAGES], empty[STAGES], done
   uint32_t *tmem_slot = (uint32_t *)(bar + 2 * STAGES + 1);
   __shared__ int s_skip;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  // x: output part fastest (the real- and imaginary-part CTAs of a tile read the same A and
-  // B planes and run together, so the second reads them from L2), then N tiles; y: M tiles
-  const int comp = blockIdx.x % P.ncomp_out, nt = blockIdx.x / P.ncomp_out;
   const int b = blockIdx.z / P.ksplit, ks = blockIdx.z - (blockIdx.z / P.ksplit) * P.ksplit;
-  const int m0 = blockIdx.y * BM, n0 = nt * BN;
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
   const int kb0 = ks * P.kb_per_split;
   const int nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
-  int iters = nkb * P.nterms[comp];
+  int iters = nkb * P.nprod;
   const uint32_t full0 = smem_u32(bar), empty0 = smem_u32(bar + STAGES), done = smem_u32(bar + 2 * STAGES);
 
   if (threadIdx.x == 0) {
@@ -167,7 +230,7 @@ __global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
   }
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(BN));
+                 "r"(TCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -185,27 +248,40 @@ __global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
       if (it >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) break;
-      const Term t = P.terms[comp][it / nkb];
-      const int kb = kb0 + it % nkb;
-      const uint32_t sa = smem_u32(smem + s * STAGE_BYTES), sb = sa + A_BYTES;
-      mbar_expect_tx(full0 + 8 * s, STAGE_BYTES);
-      tma_load_3d(sa, &tmA, full0 + 8 * s, kb * BK, m0, t.pa * P.a_nb + (P.a_nb > 1 ? b : 0));
-      tma_load_3d(sb, &tmB, full0 + 8 * s, kb * BK, n0, t.pb * P.b_nb + (P.b_nb > 1 ? b : 0));
+      const int pr = it / nkb, kb = kb0 + it % nkb;
+      const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+      mbar_expect_tx(full0 + 8 * s, P.stage_bytes);
+      for (int i = 0; i < P.nA; i++)
+        tma_load_3d(base + i * A_BYTES, &tmA, full0 + 8 * s, kb * BK, m0,
+                    (P.a_comp[i] * P.np + P.pa[pr]) * P.a_nb + (P.a_nb > 1 ? P.a_b0 + b : 0));
+      for (int j = 0; j < P.nB; j++)
+        tma_load_3d(base + P.nA * A_BYTES + j * B_BYTES, &tmB, full0 + 8 * s, kb * BK, n0,
+                    (P.b_comp[j] * P.np + P.pb[pr]) * P.b_nb + (P.b_nb > 1 ? P.b_b0 + b : 0));
     }
   } else if (warp == 5 && lane == 0) {
     // ---- MMA issuer
+    bool started0 = false, started1 = false;  // accumulator written once (then accumulate)
     for (int it = 0; it < iters; it++) {
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
       if (!mbar_wait(full0 + 8 * s, ph, P.err, 2)) break;
       tc_fence_after();
-      const Term t = P.terms[comp][it / nkb];
-      const uint32_t idesc = IDESC | (t.neg ? (1u << 13) : 0u);
-      const uint32_t sa = smem_u32(smem + s * STAGE_BYTES), sb = sa + A_BYTES;
-      const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
+      const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+      for (int q = 0; q < P.nmma; q++) {
+        const Mma mq = P.mma[q];
+        const uint64_t da = sw128_desc(base + mq.sa * A_BYTES);
+        const uint64_t db = sw128_desc(base + P.nA * A_BYTES + mq.sb * B_BYTES);
+        const uint32_t idesc = IDESC | (mq.neg ? (1u << 13) : 0u);
+        const uint32_t tacc = tmem + (uint32_t)(mq.acc * BN);
 #pragma unroll
-      for (int k = 0; k < BK / 16; k++)  // K = 16 per instruction: +32 bytes inside the swizzle atom
-        mma_bf16(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc, (it > 0 || k > 0) ? 1u : 0u);
+        for (int k = 0; k < BK / 16; k++)  // K = 16 per instruction: +32 bytes inside the swizzle atom
+          mma_bf16(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                   ((mq.acc ? started1 : started0) || k > 0) ? 1u : 0u);
+        if (mq.acc)
+          started1 = true;
+        else
+          started0 = true;
+      }
       mma_commit(empty0 + 8 * s);
     }
     mma_commit(done);
@@ -219,85 +295,46 @@ __global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
     tc_fence_after();
     const int m = m0 + warp * 32 + lane;
     const bool mok = m < P.M;
-    const i64 roff = (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
+    const i64 roff =
+        (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     if (ok) {
       for (int c0 = 0; c0 < BN; c0 += 16) {
         if (n0 + c0 >= P.N) break;  // uniform across the warp
-        float v[16];
-        tmem_ld16(trow + (uint32_t)c0, v);
+        float vr[16], vi[16];
+        tmem_ld16(trow + (uint32_t)c0, vr);
+        tmem_ld16(trow + (uint32_t)(BN + c0), vi);
         if (iters == 0) {
 #pragma unroll
-          for (int j = 0; j < 16; j++) v[j] = 0.f;
+          for (int j = 0; j < 16; j++) vr[j] = vi[j] = 0.f;
         }
         if (!mok) continue;
-        // column offsets of this 16-column chunk: one division per chunk when the chunk
-        // stays inside one cdiv segment, then base + j * cs_lo
         const int nf = n0 + c0;
-        bool fast = nf + 16 <= P.N;
-        i64 cbase = 0;
-        if (fast) {
-          if (P.cdiv) {
-            const int qd = nf / P.cdiv, rm = nf - qd * P.cdiv;
-            fast = rm + 16 <= P.cdiv;
-            cbase = (i64)qd * P.cs_hi + (i64)rm * P.cs_lo;
-          } else {
-            cbase = (i64)nf * P.cs_lo;
-          }
-        }
+        i64 cbase;
+        const bool fast = chunk_base(P, nf, cbase);
         if (P.out_pieces) {
-          __nv_bfloat16 *o = (__nv_bfloat16 *)P.out + (i64)comp * P.out_np * P.plane;
-          const float al = (float)P.alpha;
-          if (fast && P.cs_lo == 1 && ((roff + cbase) & 7) == 0) {
-            // 16 contiguous BF16 per piece plane: two 16-byte stores each
-            float x[16];
-#pragma unroll
-            for (int j = 0; j < 16; j++) x[j] = al * v[j];
-            for (int p = 0; p < P.out_np; p++) {
-              uint32_t w[8];
-#pragma unroll
-              for (int j = 0; j < 8; j++) {
-                const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * j]), h1 = __float2bfloat16_rn(x[2 * j + 1]);
-                x[2 * j] -= __bfloat162float(h0);
-                x[2 * j + 1] -= __bfloat162float(h1);
-                w[j] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-              }
-              uint4 *dst = (uint4 *)(o + (i64)p * P.plane + roff + cbase);
-              dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-              dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < 16; j++) {
-              const int n = nf + j;
-              if (n >= P.N) break;
-              const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo
-                                           : (P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo
-                                                     : (i64)n * P.cs_lo));
-              float x = al * v[j];
-              for (int p = 0; p < P.out_np; p++) {
-                const __nv_bfloat16 h = __float2bfloat16_rn(x);
-                o[(i64)p * P.plane + off] = h;
-                x -= __bfloat162float(h);
-              }
-            }
-          }
+          __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
+          store_pieces16(P, o, roff, cbase, fast, nf, vr);
+          store_pieces16(P, o + (i64)P.out_np * P.plane, roff, cbase, fast, nf, vi);
         } else {
 #pragma unroll
           for (int j = 0; j < 16; j++) {
             const int n = nf + j;
             if (n >= P.N) break;
-            const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo
-                                         : (P.cdiv ? (i64)(n / P.cdiv) * P.cs_hi + (i64)(n % P.cdiv) * P.cs_lo
-                                                   : (i64)n * P.cs_lo));
-            double *o = (double *)P.out + 2 * off + comp;
-            const double x = P.alpha * (double)v[j];
-            if (P.atomic)
-              atomicAdd(o, x);
-            else if (P.accumulate)
-              *o += x;
-            else
-              *o = x;
+            const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo : col_off(P, n));
+            double2 *o = (double2 *)P.out + off;
+            const double xr = P.alpha * (double)vr[j], xi = P.alpha * (double)vi[j];
+            if (P.atomic) {
+              atomicAdd(&o->x, xr);
+              atomicAdd(&o->y, xi);
+            } else if (P.accumulate) {
+              double2 t = *o;
+              t.x += xr;
+              t.y += xi;
+              *o = t;
+            } else {
+              *o = make_double2(xr, xi);
+            }
           }
         }
       }
@@ -308,7 +345,7 @@ __global__ void __launch_bounds__(THREADS, STAGES == 2 ? 2 : 1)
   if (warp == 5) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
   }
 }
 
@@ -440,13 +477,32 @@ void split_stats(bool on, double *flops, double *ms) {
   g_stats_on = on;
 }
 
+template <int BN, int STAGES>
+void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 grid, cudaStream_t s) {
+  static bool attr[64] = {false};
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  const int bytes = smem_bytes(P.stage_bytes, STAGES);
+  NEDY_REQUIRE(STAGES * P.stage_bytes <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  if (!attr[dev]) {
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   smem_bytes(SMEM_LIMIT / STAGES, STAGES)));
+    attr[dev] = true;
+  }
+  split_gemm_kernel<BN, STAGES><<<grid, THREADS, bytes, s>>>(ma, mb, P);
+  NEDY_CHECK_LAUNCH();
+}
+
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   const bool ac = g.A.ncomp == 2, bc = g.B.ncomp == 2;
   NEDY_REQUIRE(ac || bc, "split_gemm: at least one operand must be complex");
   NEDY_REQUIRE(g.A.rows >= g.M && g.B.rows >= g.N && g.A.kpad == g.B.kpad && g.A.kpad >= g.K,
                "split_gemm: operand planes do not match the sizes");
   NEDY_REQUIRE(g.A.np == g.B.np, "split_gemm: operands split into different piece counts");
-  NEDY_REQUIRE((g.A.nb == 1 || g.A.nb == g.nb) && (g.B.nb == 1 || g.B.nb == g.nb), "split_gemm: batch mismatch");
+  NEDY_REQUIRE((g.A.nb == 1 || (g.A.b0 >= 0 && g.A.b0 + g.nb <= g.A.nb)) &&
+                   (g.B.nb == 1 || (g.B.b0 >= 0 && g.B.b0 + g.nb <= g.B.nb)),
+               "split_gemm: batch range outside the operand planes");
   if (g.M == 0 || g.N == 0 || g.nb == 0) return;
   Params P;
   memset(&P, 0, sizeof(P));
@@ -456,36 +512,42 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   P.nb = g.nb;
   P.a_nb = g.A.nb;
   P.b_nb = g.B.nb;
-  P.ntn = (g.N + BN - 1) / BN;
-  P.ncomp_out = 2;
-  // terms per output part
-  int pa[6], pb[6], npr;
-  products(g.A.np, pa, pb, npr);
-  const int np = g.A.np;
-  const int sA = g.conjA ? 1 : 0, sB = g.conjB ? 1 : 0;  // sign bits of the imaginary parts
-  for (int oc = 0; oc < 2; oc++) {
-    int n = 0;
-    auto add = [&](int ca, int cb, int neg) {
-      for (int i = 0; i < npr; i++) P.terms[oc][n++] = Term{(signed char)(ca * np + pa[i]), (signed char)(cb * np + pb[i]), (signed char)neg, 0};
-    };
-    if (ac && bc) {
-      if (oc == 0) {
-        add(0, 0, 0);
-        add(1, 1, 1 ^ sA ^ sB);
-      } else {
-        add(0, 1, sB);
-        add(1, 0, sA);
-      }
-    } else if (ac) {
-      add(oc, 0, oc ? sA : 0);
-    } else {
-      add(0, oc, oc ? sB : 0);
-    }
-    P.nterms[oc] = n;
+  P.a_b0 = g.A.b0;
+  P.b_b0 = g.B.b0;
+  P.np = g.A.np;
+  products(g.A.np, P.pa, P.pb, P.nprod);
+  const signed char cA = g.conjA ? 1 : 0, cB = g.conjB ? 1 : 0;  // negate the imaginary part
+  // tile products of a stage (slots: A re/im, B re/im)
+  if (ac && bc) {  // Re = Ar Br - Ai Bi, Im = Ar Bi + Ai Br (with the conjugation signs)
+    P.nA = 2; P.nB = 2;
+    P.a_comp[0] = 0; P.a_comp[1] = 1; P.b_comp[0] = 0; P.b_comp[1] = 1;
+    P.nmma = 4;
+    P.mma[0] = Mma{0, 0, 0, 0};
+    P.mma[1] = Mma{1, 1, 0, (signed char)(1 ^ cA ^ cB)};
+    P.mma[2] = Mma{0, 1, 1, cB};
+    P.mma[3] = Mma{1, 0, 1, cA};
+  } else if (ac) {  // Re = Ar B, Im = Ai B
+    P.nA = 2; P.nB = 1;
+    P.a_comp[0] = 0; P.a_comp[1] = 1; P.b_comp[0] = 0;
+    P.nmma = 2;
+    P.mma[0] = Mma{0, 0, 0, 0};
+    P.mma[1] = Mma{1, 0, 1, cA};
+  } else {  // Re = A Br, Im = A Bi
+    P.nA = 1; P.nB = 2;
+    P.a_comp[0] = 0; P.b_comp[0] = 0; P.b_comp[1] = 1;
+    P.nmma = 2;
+    P.mma[0] = Mma{0, 0, 0, 0};
+    P.mma[1] = Mma{0, 1, 1, cB};  // negating A negates the product
   }
+  // instance: outputs at most 64 wide use 64-wide tiles; piece outputs 128-wide tiles (two
+  // CTAs per SM overlap one CTA's store-heavy epilogue with the other's main loop); FP64
+  // outputs 256-wide tiles, as many stages as fit
+  const int BNsel = g.N <= 64 ? 64 : g.out_pieces ? 128 : 256;
+  P.stage_bytes = P.nA * A_BYTES + P.nB * BNsel * BK * 2;
+  const int ntn = (g.N + BNsel - 1) / BNsel, ntm = (g.M + BM - 1) / BM;
   // K split: bounded FP32 accumulation length, and enough CTAs for the GPU
   int ksplit = g.ksplit;
-  const i64 tiles = (i64)((g.M + BM - 1) / BM) * P.ntn * 2 * g.nb;
+  const i64 tiles = (i64)ntm * ntn * g.nb;
   if (ksplit <= 0) {
     ksplit = 1;
     if (g.accumulate) {
@@ -497,7 +559,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   NEDY_REQUIRE(ksplit == 1 || (g.accumulate && !g.out_pieces), "split_gemm: K split needs an accumulating FP64 output");
   P.ksplit = ksplit;
   P.kb_per_split = (P.kblocks + ksplit - 1) / ksplit;
-  NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && (i64)(g.M + BM - 1) / BM <= 65535, "split_gemm: grid too large");
+  NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && ntm <= 65535, "split_gemm: grid too large");
   P.out_pieces = g.out_pieces ? 1 : 0;
   P.accumulate = g.accumulate ? 1 : 0;
   P.atomic = ksplit > 1 ? 1 : 0;
@@ -519,33 +581,27 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   P.cdiv = g.C.cdiv;
   P.bs = g.C.bs1;
   P.err = err_word();
-  const CUtensorMap ma = make_map(g.A, BM), mb = make_map(g.B, BN);
-  static bool attr_set[64] = {false};
-  int dev = 0;
-  NEDY_CUDA(cudaGetDevice(&dev));
-  NEDY_REQUIRE(dev < 64, "device index out of range");
-  if (!attr_set[dev]) {
-    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(2)));
-    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(4)));
-    attr_set[dev] = true;
-  }
-  dim3 grid(P.ntn * 2, (g.M + BM - 1) / BM, g.nb * ksplit);
-  const int kiters = P.kb_per_split * std::max(P.nterms[0], P.nterms[1]);
+  const CUtensorMap ma = make_map(g.A, BM), mb = make_map(g.B, BNsel);
+  dim3 grid(ntn, ntm, g.nb * ksplit);
   cudaEvent_t ev[2] = {nullptr, nullptr};
   {
     std::lock_guard<std::mutex> lk(g_stats_mu);
     if (g_stats_on) {
-      g_stats_flops += 2.0 * g.M * (double)g.N * g.K * g.nb * (P.nterms[0] + P.nterms[1]);
+      g_stats_flops += 2.0 * g.M * (double)g.N * g.K * g.nb * P.nprod * P.nmma;
       NEDY_CUDA(cudaEventCreate(&ev[0]));
       NEDY_CUDA(cudaEventCreate(&ev[1]));
       NEDY_CUDA(cudaEventRecord(ev[0], s));
     }
   }
-  if (g.out_pieces || kiters <= 48)
-    split_gemm_kernel<2><<<grid, THREADS, smem_bytes(2), s>>>(ma, mb, P);
+  const int stages = std::min(4, SMEM_LIMIT / P.stage_bytes);
+  if (BNsel == 64)
+    launch<64, 4>(P, ma, mb, grid, s);
+  else if (BNsel == 128)
+    launch<128, 2>(P, ma, mb, grid, s);
+  else if (stages >= 3)
+    launch<256, 3>(P, ma, mb, grid, s);
   else
-    split_gemm_kernel<4><<<grid, THREADS, smem_bytes(4), s>>>(ma, mb, P);
-  NEDY_CHECK_LAUNCH();
+    launch<256, 2>(P, ma, mb, grid, s);
   if (ev[0]) {
     std::lock_guard<std::mutex> lk(g_stats_mu);
     NEDY_CUDA(cudaEventRecord(ev[1], s));

@@ -23,6 +23,7 @@ struct Pieces {
   __nv_bfloat16 *p = nullptr;
   int rows = 0, kpad = 0, nb = 1;  // nb = 1 with a batched GEMM: shared by every batch
   int ncomp = 1, np = 3;           // ncomp 2: complex (re plane group, then im)
+  int b0 = 0;                      // first stored batch a batched GEMM uses (nb > 1)
   i64 plane() const { return (i64)nb * rows * kpad; }
   i64 elems() const { return plane() * ncomp * np; }
 };
