@@ -198,6 +198,33 @@ __device__ __forceinline__ void store_pieces16(const Params &P, __nv_bfloat16 *o
   }
 }
 
+// BF16 pieces of a 32-row x 16-column chunk whose 32 rows are contiguous in the output
+// (one warp, lane = row): staged through a warp-private 1 KB shared buffer so that every
+// lane stores two 16-byte runs of 8 consecutive rows instead of 16 scattered elements.
+__device__ __forceinline__ void store_pieces16_rows(const Params &P, __nv_bfloat16 *o, i64 roff0, i64 cbase, int nf,
+                                                    const float (&v)[16], __nv_bfloat16 *sbuf, int lane) {
+  const float al = (float)P.alpha;
+  float x[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) x[j] = al * v[j];
+  for (int p = 0; p < P.out_np; p++) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(x[j]);
+      x[j] -= __bfloat162float(h);
+      sbuf[j * 32 + lane] = h;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const int w = lane + 32 * i, c = w >> 2, r8 = (w & 3) * 8;
+      if (nf + c < P.N)
+        *(uint4 *)(o + (i64)p * P.plane + roff0 + r8 + cbase + (i64)c * P.cs_lo) = *(const uint4 *)(sbuf + c * 32 + r8);
+    }
+    __syncwarp();
+  }
+}
+
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -298,6 +325,13 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
     const i64 roff =
         (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // piece outputs whose 32 rows of this warp are contiguous use the staged store
+    const int r0 = m0 + warp * 32;
+    bool rows_contig = P.out_pieces && P.rs_lo == 1 && r0 + 32 <= P.M;
+    if (rows_contig && P.rdiv) rows_contig = (r0 % P.rdiv) + 32 <= P.rdiv;
+    const i64 roff0 = __shfl_sync(0xffffffffu, roff, 0);
+    rows_contig = rows_contig && (roff0 & 7) == 0;
+    __nv_bfloat16 *sbuf = (__nv_bfloat16 *)(smem + warp * 1024);  // stages are idle in the epilogue
     if (ok) {
       for (int c0 = 0; c0 < BN; c0 += 16) {
         if (n0 + c0 >= P.N) break;  // uniform across the warp
@@ -314,8 +348,13 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
         const bool fast = chunk_base(P, nf, cbase);
         if (P.out_pieces) {
           __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
-          store_pieces16(P, o, roff, cbase, fast, nf, vr);
-          store_pieces16(P, o + (i64)P.out_np * P.plane, roff, cbase, fast, nf, vi);
+          if (rows_contig && fast && (cbase & 7) == 0 && (P.cs_lo & 7) == 0) {
+            store_pieces16_rows(P, o, roff0, cbase, nf, vr, sbuf, lane);
+            store_pieces16_rows(P, o + (i64)P.out_np * P.plane, roff0, cbase, nf, vi, sbuf, lane);
+          } else {
+            store_pieces16(P, o, roff, cbase, fast, nf, vr);
+            store_pieces16(P, o + (i64)P.out_np * P.plane, roff, cbase, fast, nf, vi);
+          }
         } else {
 #pragma unroll
           for (int j = 0; j < 16; j++) {
