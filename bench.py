@@ -433,8 +433,11 @@ def run_engine(args, dist: Dist):
     d2h = (2 * (T_e + 1) + ntau + 1) * es
     torch.cuda.synchronize(dev)
     pstats = ctx.predictor_stats() if pred is not None else None
+    rep = C.create_string_buffer(16384)
+    check(lib().nedy_split_tune_report(rep, 16384))
+    tune = [x for x in rep.value.decode().split(";") if x]
     return dict(plain=plain, split=split, split_iters=split_iters, max_dg=max_dg, max_g=max_g, T=T_timed,
-                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h, prep=prep, pred_info=pred_info, pred_stats=pstats)
+                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h, prep=prep, pred_info=pred_info, pred_stats=pstats, tune=tune)
 
 
 def train_predictor(ctx, args):
@@ -544,7 +547,7 @@ def main():
                            "self_energy_fp64_tflops": sig_flops / (pl["phase_ms"][2] / 1e3) / 1e12,
                            "fp64_peak_tflops": fp64} if pl else None,
             "state_preparation": r["prep"], "predictor_training": r["pred_info"],
-            "predictor_stats": r["pred_stats"],
+            "predictor_stats": r["pred_stats"], "split_tile_autotune": r["tune"],
             "speedup_split_vs_plain": value / plain_value if pl else None,
             "max_abs_dG_split_vs_plain": r["max_dg"], "max_abs_G": r["max_g"]}
         line["clocks"] = sp["clocks"]

@@ -85,6 +85,12 @@ int nedy_ctx_set_precision(nedy_ctx *ctx, int mode);
  * (CUDA events around each launch) since the previous call, then switches the
  * accounting on (on != 0) or off. */
 int nedy_split_stats(int on, double *pipe_flops, double *ms);
+/* Autotuner of the split GEMM tile shapes (on by default): each problem class (operand
+ * kinds, output kind, M, N, padded K) times its candidate shapes (64/128/256-wide tiles,
+ * 2-4 pipeline stages) on its first launches and keeps the fastest; every candidate
+ * computes the same result.  The report lists classes, candidate times and choices. */
+int nedy_split_autotune(int on);
+int nedy_split_tune_report(char *buf, int len);
 int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
 /* Number of engine kernel launches issued by this process so far. */
 unsigned long long nedy_launch_count(void);

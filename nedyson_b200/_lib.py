@@ -65,6 +65,8 @@ SIGNATURES = {
     "nedy_hf_decomp_noalloc": ([_P, _I, _P, _P], _I),
     "nedy_ctx_set_precision": ([_P, _I], _I),
     "nedy_split_stats": ([_I, _DP, _DP], _I),
+    "nedy_split_autotune": ([_I], _I),
+    "nedy_split_tune_report": ([C.c_char_p, _I], _I),
     "nedy_predictor_create": ([_P, _LL, C.c_ulonglong, _PP], _I),
     "nedy_predictor_destroy": ([_P], _I),
     "nedy_predictor_collect": ([_P, _P, _I, _I], _I),

@@ -295,6 +295,20 @@ int nedy_ctx_set_precision(nedy_ctx *ctx, int mode) {
   });
 }
 
+int nedy_split_autotune(int on) {
+  return guard([&] { split_autotune(on != 0); });
+}
+
+int nedy_split_tune_report(char *buf, int len) {
+  return guard([&] {
+    NEDY_REQUIRE(buf && len > 0, "bad argument");
+    const std::string r = split_tune_report();
+    const size_t n = std::min<size_t>(r.size(), (size_t)len - 1);
+    memcpy(buf, r.data(), n);
+    buf[n] = 0;
+  });
+}
+
 int nedy_split_stats(int on, double *pipe_flops, double *ms) {
   return guard([&] { split_stats(on != 0, pipe_flops, ms); });
 }

@@ -16,7 +16,11 @@
 // the CTA drains and returns, so no launch can hang.
 #include "split_gemm.cuh"
 #include <cuda.h>
+#include <algorithm>
+#include <map>
 #include <mutex>
+#include <string>
+#include <tuple>
 #include <vector>
 
 namespace nedy {
@@ -533,6 +537,110 @@ void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 
   NEDY_CHECK_LAUNCH();
 }
 
+// ---- autotuner: the tile shape (BN, stages) of each problem class is chosen by timing
+// the candidates on the live launches.  Every candidate computes the same result; the
+// first launches of a class cycle through the candidates with CUDA events around them,
+// and once each has TUNE_TRIALS timings the fastest (device time per batch) is kept.
+namespace {
+struct Cand {
+  int bn, stages;
+};
+struct TuneKey {
+  int dev, nA, nB, out_pieces, acc, M, N, kpad;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(dev, nA, nB, out_pieces, acc, M, N, kpad) <
+           std::tie(o.dev, o.nA, o.nB, o.out_pieces, o.acc, o.M, o.N, o.kpad);
+  }
+};
+struct Pending {
+  int c, nb;
+  cudaEvent_t e0, e1;
+};
+struct TuneEntry {
+  std::vector<Cand> cands;
+  std::vector<double> best;  // ms per batch, min over trials
+  std::vector<int> trials, inflight;
+  std::vector<Pending> pend;
+  int chosen = -1;
+};
+constexpr int TUNE_TRIALS = 2;
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tune;
+bool g_tune_on = true;
+
+std::vector<Cand> candidates(int nA, int nB, int N) {
+  std::vector<Cand> c;
+  for (int bn : {64, 128, 256}) {
+    if (bn > 64 && N <= 64) continue;    // one 64-wide tile covers the output
+    if (bn == 256 && N <= 128) continue;
+    const int sb = nA * A_BYTES + nB * bn * BK * 2;
+    const int st = std::min(4, SMEM_LIMIT / sb);
+    if (st < 2) continue;
+    if (bn == 64) {
+      if (st >= 4) c.push_back({64, 4});
+    } else if (bn == 128) {
+      c.push_back({128, 2});
+      if (st >= 3) c.push_back({128, std::min(st, 4)});
+    } else {
+      c.push_back({256, std::min(st, 3)});
+    }
+  }
+  return c;
+}
+
+void poll(TuneEntry &e) {
+  for (size_t i = 0; i < e.pend.size();) {
+    Pending &q = e.pend[i];
+    if (cudaEventQuery(q.e1) != cudaSuccess) {
+      cudaGetLastError();  // cudaErrorNotReady is not an error here
+      i++;
+      continue;
+    }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, q.e0, q.e1) == cudaSuccess) {
+      e.best[q.c] = std::min(e.best[q.c], (double)ms / std::max(1, q.nb));
+      e.trials[q.c]++;
+    } else {
+      cudaGetLastError();
+    }
+    e.inflight[q.c]--;
+    cudaEventDestroy(q.e0);
+    cudaEventDestroy(q.e1);
+    e.pend.erase(e.pend.begin() + i);
+  }
+  if (e.chosen < 0) {
+    bool all = true;
+    for (int t : e.trials) all = all && t >= TUNE_TRIALS;
+    if (all) e.chosen = (int)(std::min_element(e.best.begin(), e.best.end()) - e.best.begin());
+  }
+}
+}  // namespace
+
+void split_autotune(bool on) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_on = on;
+}
+
+std::string split_tune_report() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  std::string r;
+  for (auto &kv : g_tune) {
+    TuneEntry &e = kv.second;
+    poll(e);
+    const TuneKey &k = kv.first;
+    r += "M=" + std::to_string(k.M) + " N=" + std::to_string(k.N) + " K=" + std::to_string(k.kpad) +
+         (k.nA == 2 ? (k.nB == 2 ? " cxc" : " cxr") : " rxc") + (k.out_pieces ? " pieces" : " fp64") + ":";
+    for (size_t i = 0; i < e.cands.size(); i++) {
+      char buf[96];
+      snprintf(buf, sizeof(buf), " %d/%d=%.1fus%s", e.cands[i].bn, e.cands[i].stages,
+               e.trials[i] ? e.best[i] * 1e3 : -1.0, (int)i == e.chosen ? "*" : "");
+      r += buf;
+    }
+    r += ";";
+  }
+  return r;
+}
+
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   const bool ac = g.A.ncomp == 2, bc = g.B.ncomp == 2;
   NEDY_REQUIRE(ac || bc, "split_gemm: at least one operand must be complex");
@@ -581,7 +689,42 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   // instance: outputs at most 64 wide use 64-wide tiles; piece outputs 128-wide tiles (two
   // CTAs per SM overlap one CTA's store-heavy epilogue with the other's main loop); FP64
   // outputs 256-wide tiles, as many stages as fit
-  const int BNsel = g.N <= 64 ? 64 : g.out_pieces ? 128 : 256;
+  int BNsel = g.N <= 64 ? 64 : g.out_pieces ? 128 : 256;
+  int STsel = 0;  // 0: as many stages as fit
+  int tune_c = -1;
+  TuneEntry *te = nullptr;
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune_on) {
+      const TuneKey key{dev, P.nA, P.nB, g.out_pieces ? 1 : 0, g.accumulate ? 1 : 0, g.M, g.N, g.A.kpad};
+      auto it = g_tune.find(key);
+      if (it == g_tune.end()) {
+        TuneEntry e;
+        e.cands = candidates(P.nA, P.nB, g.N);
+        e.best.assign(e.cands.size(), 1e30);
+        e.trials.assign(e.cands.size(), 0);
+        e.inflight.assign(e.cands.size(), 0);
+        if (e.cands.size() <= 1) e.chosen = e.cands.empty() ? -2 : 0;
+        it = g_tune.emplace(key, std::move(e)).first;
+      }
+      TuneEntry &e = it->second;
+      poll(e);
+      int c = e.chosen;
+      if (c == -1) {  // still tuning: the candidate with the fewest timings so far
+        c = 0;
+        for (size_t i = 1; i < e.cands.size(); i++)
+          if (e.trials[i] + e.inflight[i] < e.trials[c] + e.inflight[c]) c = (int)i;
+        tune_c = c;
+        te = &e;
+      }
+      if (c >= 0) {
+        BNsel = e.cands[c].bn;
+        STsel = e.cands[c].stages;
+      }
+    }
+  }
   P.stage_bytes = P.nA * A_BYTES + P.nB * BNsel * BK * 2;
   const int ntn = (g.N + BNsel - 1) / BNsel, ntm = (g.M + BM - 1) / BM;
   // K split: bounded FP32 accumulation length, and enough CTAs for the GPU
@@ -632,15 +775,31 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       NEDY_CUDA(cudaEventRecord(ev[0], s));
     }
   }
-  const int stages = std::min(4, SMEM_LIMIT / P.stage_bytes);
+  const int stages = STsel ? STsel : BNsel == 128 ? 2 : std::min(4, SMEM_LIMIT / P.stage_bytes);
+  cudaEvent_t tev[2] = {nullptr, nullptr};
+  if (te) {
+    NEDY_CUDA(cudaEventCreate(&tev[0]));
+    NEDY_CUDA(cudaEventCreate(&tev[1]));
+    NEDY_CUDA(cudaEventRecord(tev[0], s));
+  }
   if (BNsel == 64)
     launch<64, 4>(P, ma, mb, grid, s);
+  else if (BNsel == 128 && stages >= 4)
+    launch<128, 4>(P, ma, mb, grid, s);
+  else if (BNsel == 128 && stages == 3)
+    launch<128, 3>(P, ma, mb, grid, s);
   else if (BNsel == 128)
     launch<128, 2>(P, ma, mb, grid, s);
   else if (stages >= 3)
     launch<256, 3>(P, ma, mb, grid, s);
   else
     launch<256, 2>(P, ma, mb, grid, s);
+  if (te) {
+    NEDY_CUDA(cudaEventRecord(tev[1], s));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    te->pend.push_back({tune_c, g.nb, tev[0], tev[1]});
+    te->inflight[tune_c]++;
+  }
   if (ev[0]) {
     std::lock_guard<std::mutex> lk(g_stats_mu);
     NEDY_CUDA(cudaEventRecord(ev[1], s));

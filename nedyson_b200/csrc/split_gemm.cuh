@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "gemm_f64.cuh"
 #include <cuda_bf16.h>
+#include <string>
 
 namespace nedy {
 
@@ -54,6 +55,12 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
 // Accounting of split kernel launches: returns the algorithmic BF16 tensor-pipe FLOPs and
 // the summed device time (ms) since the last call, then turns the accounting on or off.
 void split_stats(bool on, double *flops, double *ms);
+
+// Autotuner of the tile shapes (on by default): each problem class (operand kinds, output
+// kind, M, N, padded K) tries its candidate shapes on its first launches and keeps the
+// fastest.  split_tune_report lists the classes, candidate timings and choices.
+void split_autotune(bool on);
+std::string split_tune_report();
 
 // Device error word of the split kernels (non-zero after a bounded wait gave up).
 int split_gemm_error(cudaStream_t s);
