@@ -176,11 +176,12 @@ __device__ __forceinline__ void store_pieces16(const Params &P, __nv_bfloat16 *o
     for (int p = 0; p < P.out_np; p++) {
       uint32_t w[8];
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * j]), h1 = __float2bfloat16_rn(x[2 * j + 1]);
-        x[2 * j] -= __bfloat162float(h0);
-        x[2 * j + 1] -= __bfloat162float(h1);
-        w[j] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      for (int j = 0; j < 8; j++) {  // two values per conversion instruction
+        const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * j], x[2 * j + 1]);
+        const float2 f = __bfloat1622float2(h);
+        x[2 * j] -= f.x;
+        x[2 * j + 1] -= f.y;
+        w[j] = *(const uint32_t *)&h;
       }
       uint4 *dst = (uint4 *)(o + (i64)p * P.plane + roff + cbase);
       dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
@@ -213,10 +214,13 @@ __device__ __forceinline__ void store_pieces16_rows(const Params &P, __nv_bfloat
   for (int j = 0; j < 16; j++) x[j] = al * v[j];
   for (int p = 0; p < P.out_np; p++) {
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-      const __nv_bfloat16 h = __float2bfloat16_rn(x[j]);
-      x[j] -= __bfloat162float(h);
-      sbuf[j * 32 + lane] = h;
+    for (int j = 0; j < 16; j += 2) {  // two values per conversion instruction
+      const __nv_bfloat162 h = __floats2bfloat162_rn(x[j], x[j + 1]);
+      const float2 f = __bfloat1622float2(h);
+      x[j] -= f.x;
+      x[j + 1] -= f.y;
+      sbuf[j * 32 + lane] = h.x;
+      sbuf[(j + 1) * 32 + lane] = h.y;
     }
     __syncwarp();
 #pragma unroll
@@ -543,7 +547,7 @@ void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 
 // and once each has TUNE_TRIALS timings the fastest (device time per batch) is kept.
 namespace {
 struct Cand {
-  int bn, stages;
+  int bn, stages, kdiv;  // kdiv: divide the automatic K split by this (FP64-accumulating outputs)
 };
 struct TuneKey {
   int dev, nA, nB, out_pieces, acc, M, N, kpad;
@@ -568,8 +572,12 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
 bool g_tune_on = true;
 
-std::vector<Cand> candidates(int nA, int nB, int N) {
+std::vector<Cand> candidates(int nA, int nB, int N, bool acc) {
   std::vector<Cand> c;
+  if (N <= 64 && acc) {  // one output tile per batch: the K split is what there is to tune
+    for (int kd : {1, 2, 4, 8}) c.push_back({64, 4, kd});
+    return c;
+  }
   for (int bn : {64, 128, 256}) {
     if (bn > 64 && N <= 64) continue;    // one 64-wide tile covers the output
     if (bn == 256 && N <= 128) continue;
@@ -577,12 +585,13 @@ std::vector<Cand> candidates(int nA, int nB, int N) {
     const int st = std::min(4, SMEM_LIMIT / sb);
     if (st < 2) continue;
     if (bn == 64) {
-      if (st >= 4) c.push_back({64, 4});
+      if (st >= 4) c.push_back({64, 4, 1});
     } else if (bn == 128) {
-      c.push_back({128, 2});
-      if (st >= 3) c.push_back({128, std::min(st, 4)});
+      c.push_back({128, 2, 1});
+      if (st >= 3) c.push_back({128, std::min(st, 4), 1});
     } else {
-      c.push_back({256, std::min(st, 3)});
+      c.push_back({256, std::min(st, 3), 1});
+      if (acc) c.push_back({256, std::min(st, 3), 2});
     }
   }
   return c;
@@ -632,7 +641,7 @@ std::string split_tune_report() {
          (k.nA == 2 ? (k.nB == 2 ? " cxc" : " cxr") : " rxc") + (k.out_pieces ? " pieces" : " fp64") + ":";
     for (size_t i = 0; i < e.cands.size(); i++) {
       char buf[96];
-      snprintf(buf, sizeof(buf), " %d/%d=%.1fus%s", e.cands[i].bn, e.cands[i].stages,
+      snprintf(buf, sizeof(buf), " %d/%d/k%d=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv,
                e.trials[i] ? e.best[i] * 1e3 : -1.0, (int)i == e.chosen ? "*" : "");
       r += buf;
     }
@@ -691,6 +700,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   // outputs 256-wide tiles, as many stages as fit
   int BNsel = g.N <= 64 ? 64 : g.out_pieces ? 128 : 256;
   int STsel = 0;  // 0: as many stages as fit
+  int KDsel = 1;
   int tune_c = -1;
   TuneEntry *te = nullptr;
   int dev = 0;
@@ -702,7 +712,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       auto it = g_tune.find(key);
       if (it == g_tune.end()) {
         TuneEntry e;
-        e.cands = candidates(P.nA, P.nB, g.N);
+        e.cands = candidates(P.nA, P.nB, g.N, g.accumulate && g.ksplit <= 0);
         e.best.assign(e.cands.size(), 1e30);
         e.trials.assign(e.cands.size(), 0);
         e.inflight.assign(e.cands.size(), 0);
@@ -722,6 +732,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       if (c >= 0) {
         BNsel = e.cands[c].bn;
         STsel = e.cands[c].stages;
+        KDsel = e.cands[c].kdiv;
       }
     }
   }
@@ -734,6 +745,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     ksplit = 1;
     if (g.accumulate) {
       while (tiles * ksplit < 2 * 148 && P.kblocks / (ksplit * 2) >= 4) ksplit *= 2;
+      ksplit = std::max(1, ksplit / KDsel);
       if (g.max_kblocks > 0)
         while ((P.kblocks + ksplit - 1) / ksplit > g.max_kblocks) ksplit++;
     }
