@@ -2,25 +2,29 @@
 """GF2 Kadanoff-Baym time steps per second at nao=64, naux=256: plain FP64 vs
 split precision + predictor at max|dG| <= 1e-8.
 
-One "step" is one full time step T of the restricted density-fitted GF2
-simulation (DecompSimulation::do_tstp, reference src/molNEsim_decomp_impl.h:85-104)
-through the C ABI.  Two forms run the same window from the same state:
+One "step" is one full time step T of the spin-unrestricted density-fitted GF2
+simulation (DecompSpinSimulation::do_tstp, reference
+src/molNEsim_decomp_spin_impl.h:86-108) through the C ABI: both spins' G rows.
+Two forms run the same window from the same state:
 
-  plain FP64       nedy_decomp_tstp: polynomial predictor, then CorrSteps = 5 x
-                   [density matrix, HF mean field, GF2 self-energy row T, Dyson step
-                   row T], every contraction in FP64 (the reference's algorithm);
-  split+predictor  nedy_decomp_tstp_tol on a context in NEDY_PREC_SPLIT_BF16X3: the
+  plain FP64       nedy_decomp_spin_tstp: polynomial predictor, then CorrSteps = 5 x
+                   [density matrices, unrestricted HF mean field, GF2 self-energy rows T
+                   of both spins, Dyson step row T per spin], every contraction in FP64
+                   (the reference's algorithm);
+  split+predictor  nedy_decomp_spin_tstp_tol on a context in NEDY_PREC_SPLIT_BF16X3: the
                    self-energy contractions as BF16 piece products on tcgen05, the
                    predictor, and the residual exit at tol = 1e-8 (at most 5 iterations).
 
 value is the split+predictor form (the headline); the plain form, the iterations per
-step and max|dG| between the two forms over the window are in the same line.
+step and max|dG| between the two forms over the window (per component and spin, and
+the GF2 correlation energy) are in the same line.  --restricted runs the restricted
+simulation (DecompSimulation::do_tstp, src/molNEsim_decomp_impl.h:85-104) instead.
 
-Workload: nao=64, naux=256, ntau=256, beta=20, k=5, dt=0.01, steps T = t0+W ...
-t0+W+K-1 on a synthetic pre-evolved state (the free propagation of the Hartree-Fock
-Fock matrix on rows 0..t0-1, a scaled copy of it as the self-energy history; seeded
-inputs, no dataset).  The history arrays (GBs) are far larger than L2, so no explicit
-flush is needed.
+Workload: nao=64, naux=256, independent random h0 per spin with the same B^Q, ntau=256,
+beta=20, k=5, dt=0.01, steps T = t0+W ... t0+W+K-1 on a GF2 trajectory from the
+unrestricted Hartree-Fock equilibrium (bootstrap, then t0-6 steps; seeded inputs, no
+dataset).  The history arrays (GBs) are far larger than L2, so no explicit flush is
+needed.
 
 Multi-GPU: one independent trajectory per GPU (replicas, no collective);
 value = total time steps of all ranks / max-over-ranks time.
@@ -48,11 +52,12 @@ if ROOT not in sys.path:
 METRIC = "GF2 timesteps/s, nao=64 naux=256: plain FP64 vs split+predictor at 1e-8"
 
 
-def flops_sigma(T, N, A, ntau):
-    """Algorithmic flops of one GF2 self-energy row (reference contraction order)."""
+def flops_sigma(T, N, A, ntau, nspin=1):
+    """Algorithmic flops of one GF2 self-energy row (reference contraction order); the
+    unrestricted row counts one restricted chain per spin."""
     nt1 = ntau + 1
-    return (T + 1) * (128 * N**3 * A + 44 * A * A * N * N + 36 * N**4 * A) + \
-        nt1 * (36 * N**3 * A + 12 * A * A * N * N + 12 * N**4 * A)
+    return nspin * ((T + 1) * (128 * N**3 * A + 44 * A * A * N * N + 36 * N**4 * A) +
+                    nt1 * (36 * N**3 * A + 12 * A * A * N * N + 12 * N**4 * A))
 
 
 def flops_dyson(T, N, ntau):
@@ -74,6 +79,8 @@ def parse():
     ap.add_argument("--corr", type=int, default=5)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--state", default="trajectory", choices=["trajectory", "synthetic"])
+    ap.add_argument("--restricted", action="store_true",
+                    help="restricted simulation instead of the spin-unrestricted one")
     ap.add_argument("--predictor", default="learned", choices=["learned", "poly"])
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
@@ -172,22 +179,29 @@ def cpu_sample(args, target_seconds=20.0):
     cores = min(os.cpu_count() or 1, 32)
     po.set_threads(cores)
     N, A = args.nao, args.naux
-    p = make_problem(N, A, args.seed)
+    ns = 1 if args.restricted else 2
+    p = make_problem(N, A, args.seed, spin=ns == 2)
     rng = np.random.default_rng(1)
     ntau_s = 8
     T_s = max(2, (cores - ntau_s - 1 + 1) // 2)
-    G = HostGF(T_s, ntau_s, N, -1)
-    for a in (G.les, G.ret, G.tv):
-        a[:] = 0.05 * (rng.uniform(-1, 1, a.shape) + 1j * rng.uniform(-1, 1, a.shape))
-    S = HostGF(T_s, ntau_s, N, -1)
+    Gs, Ss = [], []
+    for _ in range(ns):
+        G = HostGF(T_s, ntau_s, N, -1)
+        for a in (G.les, G.ret, G.tv):
+            a[:] = 0.05 * (rng.uniform(-1, 1, a.shape) + 1j * rng.uniform(-1, 1, a.shape))
+        Gs.append(G)
+        Ss.append(HostGF(T_s, ntau_s, N, -1))
     df = po.DF(p.Vija)
     t0 = time.perf_counter()
-    df.solve(T_s, S, G)
+    if ns == 2:
+        df.solve_spin(T_s, Ss, Gs)
+    else:
+        df.solve(T_s, Ss[0], Gs[0])
     ts = time.perf_counter() - t0
-    rate_s = flops_sigma(T_s, N, A, ntau_s) / ts
+    rate_s = flops_sigma(T_s, N, A, ntau_s, ns) / ts
     # Dyson sample
     T_d, ntau_d = 24, 16
-    F, mu = hf_equilibrium(p, args.beta)
+    F, mu = hf_equilibrium(make_problem(N, A, args.seed), args.beta)
     x, _ = po.colloc_nodes(ntau_d)
     Gd = HostGF(T_d, ntau_d, N, -1)
     les, ret, tv, mat = free_history(T_d, T_d + 1, ntau_d, x, mu, F, args.beta, args.dt)
@@ -207,22 +221,26 @@ def cpu_sample(args, target_seconds=20.0):
     td = time.perf_counter() - t0
     rate_d = flops_dyson(T_d, N, ntau_d) / td
     return dict(cores=cores, T_s=T_s, ntau_s=ntau_s, sigma_s=ts, rate_sigma=rate_s, T_d=T_d, ntau_d=ntau_d,
-                dyson_s=td, rate_dyson=rate_d)
+                dyson_s=td, rate_dyson=rate_d, nspin=ns)
 
 
 def cpu_step_seconds(smp, T, args):
-    return args.corr * (flops_sigma(T, args.nao, args.naux, args.ntau) / smp["rate_sigma"] +
-                        flops_dyson(T, args.nao, args.ntau) / smp["rate_dyson"])
+    """One step: CorrSteps x (self-energy rows of all spins + one Dyson step per spin)."""
+    ns = smp["nspin"]
+    return args.corr * (flops_sigma(T, args.nao, args.naux, args.ntau, ns) / smp["rate_sigma"] +
+                        ns * flops_dyson(T, args.nao, args.ntau) / smp["rate_dyson"])
 
 
 def cpu_baseline_obj(smp, value, args):
     return {"value": value, "unit": "timesteps/s", "cores": smp["cores"], "kind": "port",
-            "sample": (f"oracle (C++ restatement, OpenMP over slices, OpenBLAS) timed on one GF2 self-energy row "
+            "sample": (f"oracle (C++ restatement, OpenMP over slices, OpenBLAS) timed on one "
+                       f"{'unrestricted (both spins)' if smp['nspin'] == 2 else 'restricted'} GF2 self-energy row "
                        f"at nao={args.nao}, naux={args.naux}, T={smp['T_s']}, ntau={smp['ntau_s']} "
                        f"({smp['sigma_s']:.2f} s, {smp['rate_sigma'] / 1e9:.1f} GFLOP/s) and one Dyson step at "
                        f"T={smp['T_d']}, ntau={smp['ntau_d']} ({smp['dyson_s']:.2f} s, "
                        f"{smp['rate_dyson'] / 1e9:.1f} GFLOP/s), scaled by the flop model to one "
-                       f"{args.corr}-iteration step at T={args.t0 + args.warmup}, ntau={args.ntau}")}
+                       f"{args.corr}-iteration step ({smp['nspin']} Dyson steps per iteration) at T={args.t0 + args.warmup}, "
+                       f"ntau={args.ntau}")}
 
 
 # ------------------------------------------------------------------ peaks
@@ -264,78 +282,102 @@ def run_engine(args, dist: Dist):
     import torch
     from nedyson_b200 import api
     from nedyson_b200._lib import LES, RET, TV, MAT, PREC_FP64, PREC_SPLIT_BF16X3, check, lib
-    from nedyson_b200.inputs import make_problem, hf_equilibrium, free_history, drive
+    from nedyson_b200.inputs import make_problem, hf_equilibrium, uhf_equilibrium, free_history, drive
 
     dev = dist.local
     torch.cuda.set_device(dev)
     N, A, ntau, K, W = args.nao, args.naux, args.ntau, args.steps, args.warmup
+    spin = not args.restricted
+    ns = 2 if spin else 1
     t_first = args.t0
     nt = t_first + W + K
-    p = make_problem(N, A, args.seed + dist.rank)
-    F, mu = hf_equilibrium(p, args.beta)
+    p = make_problem(N, A, args.seed + dist.rank, spin=spin)
+    if spin:
+        Fs, mus = uhf_equilibrium(p, args.beta)
+    else:
+        F, mu = hf_equilibrium(p, args.beta)
+        Fs, mus = (F,), (mu,)
     ctx = api.Context(nt, ntau, N, 5, args.beta, args.dt, device=dev)
     x, _ = ctx.collocation()
-    G = api.green_func(ctx, nt, ntau, N, -1)
-    S = api.green_func(ctx, nt, ntau, N, -1)
-    solver = api.molGF2SolverDecomp(ctx, p.Vija)
-    hm = np.zeros((nt + 1, N, N), np.complex128)
+    G = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]
+    S = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]
+    solver = (api.molGF2SolverSpinDecomp if spin else api.molGF2SolverDecomp)(ctx, p.Vija)
     kk = 5
     traj = args.state == "trajectory"
-    # one-body Hamiltonian of every step, resident on the device.  Trajectory state: the
-    # Gaussian pulse E0 = 0.05, t0 = 2, sigma = 0.5 along D; synthetic state: 0.1 sin(2t).
+    # one-body Hamiltonian of every step and spin, resident on the device.  Trajectory state:
+    # the Gaussian pulse E0 = 0.05, t0 = 2, sigma = 0.5 along D; synthetic state: 0.1 sin(2t).
     dkind, dkw = ("gauss", {"E0": 0.05, "t0": 2.0, "sigma": 0.5}) if traj else ("sin", {})
-    hts = [api.DeviceBuffer.from_array(ctx, (p.h0 + drive(dkind, t * args.dt, kk, args.dt, **dkw) * p.D)
-                                       .astype(np.complex128)) for t in range(nt + 1)]
+
+    def h_of(t, s):
+        return (p.h0_of(s) + drive(dkind, t * args.dt, kk, args.dt, **dkw) * p.D).astype(np.complex128)
+
+    hts = [[api.DeviceBuffer.from_array(ctx, h_of(t, s)) for t in range(nt + 1)] for s in range(ns)]
+    hmf = []
     prep = {}
+
+    def step_tol(t, tol, ht=None, max_corr=None):
+        it = C.c_int()
+        h = [(ht[s] if ht else hts[s][t]) for s in range(ns)]
+        m = max_corr or args.corr
+        if spin:
+            check(lib().nedy_decomp_spin_tstp_tol(ctx.h, t, G[0].h, G[1].h, S[0].h, S[1].h, hmf[0].h, hmf[1].h,
+                                                  h[0].h, h[1].h, mus[0], mus[1], m, tol, C.byref(it), None))
+        else:
+            check(lib().nedy_decomp_tstp_tol(ctx.h, t, G[0].h, S[0].h, hmf[0].h, h[0].h, mus[0], m, tol,
+                                             C.byref(it), None))
+        return it.value
+
     if traj:
         # GF2 trajectory from the Hartree-Fock equilibrium: free propagation on rows 0..k as
         # the bootstrap guess, dyson_start to self-consistency, then time steps up to t0-1
         # (split form with the residual exit at 1e-10).
-        les, ret, tv, mat = free_history(nt, kk + 1, ntau, x, mu, F, args.beta, args.dt)
-        G.upload(LES, 0, les)
-        G.upload(RET, 0, ret)
-        G.upload(TV, 0, tv)
-        G.upload(MAT, 0, mat)
-        del les, ret, tv
-        hm[:kk + 1] = F
-        hmf = api.hmf_buffer(ctx, N, hm)
+        for s in range(ns):
+            les, ret, tv, mat = free_history(nt, kk + 1, ntau, x, mus[s], Fs[s], args.beta, args.dt)
+            G[s].upload(LES, 0, les)
+            G[s].upload(RET, 0, ret)
+            G[s].upload(TV, 0, tv)
+            G[s].upload(MAT, 0, mat)
+            del les, ret, tv
+            hm = np.zeros((nt + 1, N, N), np.complex128)
+            hm[:kk + 1] = Fs[s]
+            hmf.append(api.hmf_buffer(ctx, N, hm))
         dy = api.dyson(ctx)
         tp = time.time()
         for it in range(40):
             for t in range(kk + 1):
-                solver.solve(t, S, G)
-            berr = dy.dyson_start(G, S, hmf, mu)
+                solver.solve(t, S if spin else S[0], G if spin else G[0])
+            berr = sum(dy.dyson_start(G[s], S[s], hmf[s], mus[s]) for s in range(ns))
             if berr < 1e-12:
                 break
         ctx.set_precision(PREC_SPLIT_BF16X3)
-        itc = C.c_int()
         for t in range(kk + 1, t_first):
-            check(lib().nedy_decomp_tstp_tol(ctx.h, t, G.h, S.h, hmf.h, hts[t].h, mu, args.corr, 1e-10,
-                                             C.byref(itc), None))
+            step_tol(t, 1e-10)
         ctx.synchronize()
         prep = {"boot_iterations": it + 1, "boot_err": berr, "steps": t_first - kk - 1,
                 "seconds": time.time() - tp}
     else:
-        les, ret, tv, mat = free_history(nt, t_first, ntau, x, mu, F, args.beta, args.dt)
-        G.upload(LES, 0, les)
-        G.upload(RET, 0, ret)
-        G.upload(TV, 0, tv)
-        G.upload(MAT, 0, mat)
-        S.upload(LES, 0, 0.02 * les)
-        S.upload(RET, 0, 0.02 * ret)
-        S.upload(TV, 0, 0.02 * tv)
-        del les, ret, tv
-        hm[:t_first] = F
-        hmf = api.hmf_buffer(ctx, N, hm)
+        for s in range(ns):
+            les, ret, tv, mat = free_history(nt, t_first, ntau, x, mus[s], Fs[s], args.beta, args.dt)
+            G[s].upload(LES, 0, les)
+            G[s].upload(RET, 0, ret)
+            G[s].upload(TV, 0, tv)
+            G[s].upload(MAT, 0, mat)
+            S[s].upload(LES, 0, 0.02 * les)
+            S[s].upload(RET, 0, 0.02 * ret)
+            S[s].upload(TV, 0, 0.02 * tv)
+            del les, ret, tv
+            hm = np.zeros((nt + 1, N, N), np.complex128)
+            hm[:t_first] = Fs[s]
+            hmf.append(api.hmf_buffer(ctx, N, hm))
     # learned predictor: trained on small trajectories the engine generates (outside the timing)
     pred, pred_info = None, None
     if args.predictor == "learned":
         pred, pred_info = train_predictor(ctx, args)
-    # pinned host buffers for the end-to-end pass: h(t) in, new G row out
+    # pinned host buffers for the end-to-end pass: h(t) of each spin in, new G rows out
     row_blocks = 2 * (nt + 1) + (ntau + 1)
-    h_host = torch.empty((N, N), dtype=torch.complex128).pin_memory()
-    row_host = torch.empty((row_blocks, N, N), dtype=torch.complex128).pin_memory()
-    ht_e2e = api.DeviceBuffer(ctx, N * N * 16)
+    h_host = torch.empty((ns, N, N), dtype=torch.complex128).pin_memory()
+    row_host = torch.empty((ns, row_blocks, N, N), dtype=torch.complex128).pin_memory()
+    ht_e2e = [api.DeviceBuffer(ctx, N * N * 16) for _ in range(ns)]
     sp = C.c_void_p()
     check(lib().nedy_ctx_stream(ctx.h, C.byref(sp)))
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device(f"cuda:{dev}"))
@@ -343,16 +385,23 @@ def run_engine(args, dist: Dist):
 
     def step_plain(t):
         e = C.c_double()
-        check(lib().nedy_decomp_tstp(ctx.h, t, G.h, S.h, hmf.h, hts[t].h, mu, args.corr, C.byref(e)))
+        if spin:
+            check(lib().nedy_decomp_spin_tstp(ctx.h, t, G[0].h, G[1].h, S[0].h, S[1].h, hmf[0].h, hmf[1].h,
+                                              hts[0][t].h, hts[1][t].h, mus[0], mus[1], args.corr, C.byref(e)))
+        else:
+            check(lib().nedy_decomp_tstp(ctx.h, t, G[0].h, S[0].h, hmf[0].h, hts[0][t].h, mus[0], args.corr,
+                                         C.byref(e)))
 
     def step_split(t, ht=None):
-        it = C.c_int()
-        check(lib().nedy_decomp_tstp_tol(ctx.h, t, G.h, S.h, hmf.h, (ht or hts[t]).h, mu, args.corr, args.tol,
-                                         C.byref(it), None))
-        iters.append(it.value)
+        iters.append(step_tol(t, args.tol, ht))
 
     def window_rows(T_list):
-        return [np.concatenate([G.les_col(t).ravel(), G.ret_row(t).ravel(), G.tv_row(t).ravel()]) for t in T_list]
+        """Per step T and spin: the new row of each component (les column, ret row, tv row)."""
+        return [[(G[s].les_col(t), G[s].ret_row(t), G[s].tv_row(t)) for s in range(ns)] for t in T_list]
+
+    def energies(T_list):
+        dy = api.dyson(ctx)
+        return [[dy.energy_conv(t, S[s], G[s]) for s in range(ns)] for t in T_list]
 
     def timed(step, T_list, split):
         """K steps between CUDA events on the engine stream, phase times, launches, clocks."""
@@ -390,10 +439,11 @@ def run_engine(args, dist: Dist):
     for t in range(t_first, t_first + W):
         (step_split if args.split_only else step_plain)(t)
     ctx.synchronize()
-    plain, rows_plain = None, None
+    plain, rows_plain, e_plain = None, None, None
     if not args.split_only:
         plain = timed(step_plain, T_timed, False)
         rows_plain = window_rows(T_timed)
+        e_plain = energies(T_timed)
     # split+predictor: warm-up on the window rows (recomputed below from the same history)
     ctx.set_precision(PREC_SPLIT_BF16X3)
     if pred is not None:
@@ -405,39 +455,56 @@ def run_engine(args, dist: Dist):
     split = timed(step_split, T_timed, True)
     split_iters = list(iters)
     rows_split = window_rows(T_timed)
-    max_dg = max(float(np.abs(a - b).max()) for a, b in zip(rows_plain, rows_split)) if rows_plain else None
-    max_g = max(float(np.abs(a).max()) for a in rows_split)
+    e_split = energies(T_timed)
+    comps = ("les", "ret", "tv")
+    spins = ("up", "down") if spin else ("restricted",)
+    err = None
+    if rows_plain:
+        err = {}
+        for si, sn in enumerate(spins):
+            for ci, cn in enumerate(comps):
+                err[f"{cn}_{sn}"] = max(float(np.abs(a[si][ci] - b[si][ci]).max())
+                                        for a, b in zip(rows_plain, rows_split))
+            err[f"energy_{sn}"] = max(abs(a[si] - b[si]) for a, b in zip(e_plain, e_split))
+    max_dg = max(v for k, v in err.items() if not k.startswith("energy")) if err else None
+    max_g = max(float(np.abs(c).max()) for r in rows_split for sr in r for c in sr)
 
     # end-to-end pass through the C ABI with host buffers (split form): re-run the last timed
-    # step T_e (rows are recomputed in place), copying h(T_e) from pinned host memory in and
-    # the new G row (les column, ret row, tv row) back out, all inside the timed region.
+    # step T_e (rows are recomputed in place), copying h(T_e) of each spin from pinned host
+    # memory in and the new G rows (les column, ret row, tv row) back out, all inside the
+    # timed region.
     T_e = T_timed[-1]
-    hval = (p.h0 + drive("sin", T_e * args.dt, 5, args.dt) * p.D).astype(np.complex128)
-    h_host.copy_(torch.from_numpy(hval))
+    for s in range(ns):
+        h_host[s].copy_(torch.from_numpy(h_of(T_e, s)))
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    es = N * N * 16
     dist.barrier()
     torch.cuda.synchronize(dev)
     ee0.record(stream)
-    check(lib().nedy_buf_upload(ht_e2e.h, 0, N * N * 16, C.c_void_p(h_host.data_ptr())))
+    for s in range(ns):
+        check(lib().nedy_buf_upload(ht_e2e[s].h, 0, es, C.c_void_p(h_host.data_ptr() + s * es)))
     step_split(T_e, ht_e2e)
-    base = row_host.data_ptr()
-    es = N * N * 16
-    check(lib().nedy_gf_download(G.h, LES, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base)))
-    check(lib().nedy_gf_download(G.h, RET, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base + (T_e + 1) * es)))
-    check(lib().nedy_gf_download(G.h, TV, T_e * (ntau + 1), ntau + 1, C.c_void_p(base + 2 * (T_e + 1) * es)))
+    for s in range(ns):
+        base = row_host.data_ptr() + s * row_blocks * es
+        check(lib().nedy_gf_download(G[s].h, LES, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base)))
+        check(lib().nedy_gf_download(G[s].h, RET, T_e * (T_e + 1) // 2, T_e + 1,
+                                     C.c_void_p(base + (T_e + 1) * es)))
+        check(lib().nedy_gf_download(G[s].h, TV, T_e * (ntau + 1), ntau + 1,
+                                     C.c_void_p(base + 2 * (T_e + 1) * es)))
     ee1.record(stream)
     torch.cuda.synchronize(dev)
     dist.barrier()
     e2e_secs = dist.max(ee0.elapsed_time(ee1) / 1e3)
-    h2d = N * N * 16
-    d2h = (2 * (T_e + 1) + ntau + 1) * es
+    h2d = ns * es
+    d2h = ns * (2 * (T_e + 1) + ntau + 1) * es
     torch.cuda.synchronize(dev)
     pstats = ctx.predictor_stats() if pred is not None else None
     rep = C.create_string_buffer(16384)
     check(lib().nedy_split_tune_report(rep, 16384))
     tune = [x for x in rep.value.decode().split(";") if x]
-    return dict(plain=plain, split=split, split_iters=split_iters, max_dg=max_dg, max_g=max_g, T=T_timed,
-                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h, prep=prep, pred_info=pred_info, pred_stats=pstats, tune=tune)
+    return dict(plain=plain, split=split, split_iters=split_iters, max_dg=max_dg, err=err, max_g=max_g, T=T_timed,
+                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h, prep=prep, pred_info=pred_info, pred_stats=pstats, tune=tune,
+                mu=list(mus))
 
 
 def train_predictor(ctx, args):
@@ -476,11 +543,13 @@ def main():
     args = parse()
     dist = Dist(args.gpus)
     K, W = args.steps, args.warmup
-    cfg = {"workload": f"restricted density-fitted GF2 time step, nao={args.nao} naux={args.naux} ntau={args.ntau} "
+    kind = ("restricted density-fitted GF2 time step" if args.restricted else
+            "spin-unrestricted density-fitted GF2 time step (both spins, independent h0 per spin, same B^Q)")
+    cfg = {"workload": f"{kind}, nao={args.nao} naux={args.naux} ntau={args.ntau} "
                        f"beta={args.beta} k=5 dt={args.dt}, steps T={args.t0 + W}..{args.t0 + W + K - 1} on a "
                        f"pre-evolved {args.state} state; plain form {args.corr} corrector iterations in FP64, split form "
                        f"split-precision self-energy with the residual exit at {args.tol:g} (at most {args.corr})",
-           "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "t_window": [args.t0 + W, args.t0 + W + K - 1],
+           "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "nspin": 1 if args.restricted else 2, "t_window": [args.t0 + W, args.t0 + W + K - 1],
            "corr_steps": args.corr, "precision": "fp64", "predictor": "polynomial extrapolation (k=5)",
            "l2": "inputs (G, Sigma histories) larger than L2; no flush needed",
            "parallelism": f"replicas x{dist.world}"}
@@ -516,7 +585,8 @@ def main():
     cfg["precision"] = "split BF16x3 self-energy (tcgen05), FP64 Dyson/HF/density; plain form FP64 throughout"
     cfg["predictor"] = ("learned MLP correction of the k=5 extrapolation (polynomial fallback)" if args.predictor == "learned"
                         else "polynomial extrapolation (k=5)") + " + residual exit at max|dG| estimate <= tol"
-    cfg["state"] = ("GF2 trajectory from the HF equilibrium (Gaussian pulse E0=0.05 t0=2 sigma=0.5)"
+    cfg["state"] = (f"GF2 trajectory from the {'restricted' if args.restricted else 'unrestricted'} HF equilibrium "
+                    "(Gaussian pulse E0=0.05 t0=2 sigma=0.5)"
                     if args.state == "trajectory" else "synthetic free-propagation history, 0.1 sin(2t) drive")
     cfg["tol"] = args.tol
     line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": dist.world, "steps": K, "warmup": W,
@@ -528,7 +598,8 @@ def main():
         # achieved = algorithmic BF16 pipe FLOPs / its summed device time (CUDA events per launch)
         bf16_peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
         ach = sp["split_flops"] / (sp["split_ms"] / 1e3) / 1e12 if sp.get("split_ms") else None
-        sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau) for t in r["T"]) * args.corr
+        sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau, 1 if args.restricted else 2)
+                        for t in r["T"]) * args.corr
         line["roofline"] = {"bound": "tensor", "kernel": "split_gemm_kernel (BF16 piece products, tcgen05, TMEM)",
                             "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
                             "frac": (ach / bf16_peak) if ach else None, "traffic": None,
@@ -549,7 +620,8 @@ def main():
             "state_preparation": r["prep"], "predictor_training": r["pred_info"],
             "predictor_stats": r["pred_stats"], "split_tile_autotune": r["tune"],
             "speedup_split_vs_plain": value / plain_value if pl else None,
-            "max_abs_dG_split_vs_plain": r["max_dg"], "max_abs_G": r["max_g"]}
+            "max_abs_dG_split_vs_plain": r["max_dg"], "error_vs_fp64_per_component": r["err"],
+            "max_abs_G": r["max_g"], "mu": r["mu"]}
         line["clocks"] = sp["clocks"]
         line["clocks_plain"] = pl["clocks"] if pl else None
         line["gpu_launches"] = sp["launches"]

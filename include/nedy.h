@@ -224,6 +224,11 @@ int nedy_ctx_set_predictor(nedy_ctx *ctx, nedy_predictor *p);
  * last2: the last judged max changes from the learned and from the polynomial prediction */
 int nedy_ctx_predictor_stats(const nedy_ctx *ctx, int *active, long long *judged, long long *better, double *last2);
 
+/* The unrestricted step with the residual exit (the change is the max over both spins);
+ * both G rows get the learned correction when a predictor is set. */
+int nedy_decomp_spin_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
+                              nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
+                              double mu_up, double mu_dn, int max_corr, double tol, int *iters, double *err_hist);
 /* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122). */
 int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
                           nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,

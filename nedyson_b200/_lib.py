@@ -80,6 +80,8 @@ SIGNATURES = {
     "nedy_predict": ([_P, _I, _P, _I], _I),
     "nedy_ctx_set_predictor": ([_P, _P], _I),
     "nedy_ctx_predictor_stats": ([_P, C.POINTER(_I), C.POINTER(_LL), C.POINTER(_LL), _DP], _I),
+    "nedy_decomp_spin_tstp_tol": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double, _I, C.c_double,
+                                   C.POINTER(_I), C.POINTER(C.c_double)], _I),
     "nedy_decomp_tstp_tol": ([_P, _I, _P, _P, _P, _P, C.c_double, _I, C.c_double, C.POINTER(_I), C.POINTER(C.c_double)], _I),
     "nedy_hf_spin_decomp": ([_P, _I, _P, _P, _P], _I),
     "nedy_hf_full": ([_P, _I, _P, _P], _I),

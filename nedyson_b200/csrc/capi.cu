@@ -87,7 +87,7 @@ void *Arena::get(size_t bytes) {
 
 Ctx::~Ctx() {
   auto f = [](void *p) { if (p) cudaFree(p); };
-  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(Vanj_p); f(Vjkb_p); f(Vila_p); f(rowcopy); f(d_maxdiff); f(pred_corr); f(U); f(Uexch); f(mixK); f(Minv); f(greg); f(small);
+  f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(Vanj_p); f(Vjkb_p); f(Vila_p); f(rowcopy); f(d_maxdiff); f(pred_corr); f(U); f(Uexch); f(mixK); f(mixK_alt); f(Minv); f(greg); f(small);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -131,26 +131,31 @@ static RowRanges row_ranges(const DevGF &g, int T) {
   const i64 es = (i64)g.nao * g.nao;
   return RowRanges{{g.lesptr(0, T), g.retptr(T, 0), g.tvptr(T, 0)}, {(T + 1) * es, (T + 1) * es, (g.ntau + 1) * es}};
 }
-static void save_row(Ctx &c, const DevGF &g, int T) {
+// the copy of spin `slot` (0 or 1) starts at slot * (elements of one row)
+static i64 row_len(const DevGF &g, int T) {
+  RowRanges r = row_ranges(g, T);
+  return r.n[0] + r.n[1] + r.n[2];
+}
+static void save_row(Ctx &c, const DevGF &g, int T, int slot = 0) {
   RowRanges r = row_ranges(g, T);
   const i64 tot = r.n[0] + r.n[1] + r.n[2];
-  if (c.rowcopy_cap < tot) {
+  if (c.rowcopy_cap < 2 * tot) {
     if (c.rowcopy) cudaFree(c.rowcopy);
     c.rowcopy = nullptr;
-    NEDY_CUDA(cudaMalloc(&c.rowcopy, sizeof(double2) * tot));
-    c.rowcopy_cap = tot;
+    NEDY_CUDA(cudaMalloc(&c.rowcopy, sizeof(double2) * 2 * tot));
+    c.rowcopy_cap = 2 * tot;
   }
-  i64 o = 0;
+  i64 o = slot * tot;
   for (int k = 0; k < 3; k++) {
     NEDY_CUDA(cudaMemcpyAsync(c.rowcopy + o, r.p[k], sizeof(double2) * r.n[k], cudaMemcpyDeviceToDevice, c.stream));
     o += r.n[k];
   }
 }
-static double row_change(Ctx &c, const DevGF &g, int T) {
+static double row_change(Ctx &c, const DevGF &g, int T, int slot = 0) {
   if (!c.d_maxdiff) NEDY_CUDA(cudaMalloc(&c.d_maxdiff, sizeof(unsigned long long)));
   NEDY_CUDA(cudaMemsetAsync(c.d_maxdiff, 0, sizeof(unsigned long long), c.stream));
   RowRanges r = row_ranges(g, T);
-  i64 o = 0;
+  i64 o = slot * (r.n[0] + r.n[1] + r.n[2]);
   for (int k = 0; k < 3; k++) {
     const unsigned blocks = (unsigned)std::min<i64>((r.n[k] + 255) / 256, 148 * 8);
     maxdiff_kernel<<<blocks, 256, 0, c.stream>>>(r.n[k], r.p[k], c.rowcopy + o, c.d_maxdiff);
@@ -708,88 +713,129 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
   });
 }
 
+} // extern "C"
+
+namespace {
+// One time step with the residual exit for one (restricted) or two (unrestricted) spins.
+// After iteration k the change d_k = max over the spins' new rows of |G_k - G_{k-1}| is
+// measured; the step stops once d_k times the corrector's contraction is <= tol.  The
+// contraction is measured (4 x the ratio of successive changes) on steps that run two or
+// more iterations: the first step of a context, and every 8th after, run at least two.
+void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *const *S, nedy_buf *const *hmf,
+              const nedy_buf *const *h_t, const double *mu, int max_corr, double tol, int *iters, double *err_hist) {
+  NEDY_REQUIRE(max_corr >= 1 && tol >= 0.0, "max_corr must be >= 1 and tol >= 0");
+  for (int s = 0; s < nspin; s++) NEDY_REQUIRE(G[s] && S[s] && hmf[s] && h_t[s], "null argument");
+  set_dev(ctx);
+  Ctx &c = ctx->c;
+  const int N = G[0]->g.nao;
+  const i64 es = (i64)N * N;
+  double2 *hT[2];
+  for (int s = 0; s < nspin; s++) {
+    NEDY_REQUIRE(G[s]->g.nao == N && h_t[s]->bytes >= es * 16, "h_t buffer too small or nao mismatch");
+    hT[s] = hmf_row(hmf[s], ctx, tstp, N);
+    hmf_row(hmf[s], ctx, G[s]->g.nt, N);
+  }
+  PhaseTimer pt(c);
+  pt.mark(0);
+  for (int s = 0; s < nspin; s++) extrapolate(c, tstp, G[s]->g);
+  const i64 npred = c.pred ? Predictor::row_elements(G[0]->g, tstp) : 0;
+  const bool learned = c.pred && c.pred_active && npred > 0;
+  if (learned) {
+    if (c.pred_corr_cap < nspin * npred) {
+      if (c.pred_corr) cudaFree(c.pred_corr);
+      c.pred_corr = nullptr;
+      NEDY_CUDA(cudaMalloc(&c.pred_corr, sizeof(double2) * nspin * npred));
+      c.pred_corr_cap = nspin * npred;
+    }
+    for (int s = 0; s < nspin; s++) c.pred->apply(G[s]->g, tstp, c.pred_corr + s * npred);
+  }
+  const bool refresh = c.contraction >= 1.0 || c.steps_since_measure >= 8;
+  const i64 rl = row_len(G[0]->g, tstp);
+  int it = 0;
+  double prev = 0.0, ratio = 0.0;
+  for (; it < max_corr;) {
+    for (int s = 0; s < nspin; s++) save_row(c, G[s]->g, tstp, s);
+    c.ws.reset();
+    pt.mark(1);
+    double2 *rho = c.ws.alloc<double2>(nspin * es);
+    for (int s = 0; s < nspin; s++) {
+      get_dm(c, G[s]->g, tstp, rho + s * es);
+      NEDY_CUDA(cudaMemcpyAsync(hT[s], h_t[s]->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    hf_decomp(c, nspin, hT, rho);
+    DevGF *Ss[2] = {&S[0]->g, nspin > 1 ? &S[1]->g : nullptr};
+    const DevGF *Gs[2] = {&G[0]->g, nspin > 1 ? &G[1]->g : nullptr};
+    pt.mark(2);
+    sigma_df(c, tstp, nspin, Ss, Gs);
+    pt.mark(3);
+    double d = 0.0;
+    for (int s = 0; s < nspin; s++) {
+      double e[3] = {0, 0, 0};
+      dyson_step(c, tstp, G[s]->g, S[s]->g, (const double2 *)hmf[s]->p, mu[s], e);
+      d = std::max(d, row_change(c, G[s]->g, tstp, s));
+    }
+    if (err_hist) err_hist[it] = d;
+    if (learned && it == 0) {
+      // the first iteration judges the learned prediction against the polynomial one;
+      // once 8 steps are judged, fewer than 3 wins among the last 8 switch back to the
+      // polynomial predictor
+      double dl = 0, dp = 0;
+      for (int s = 0; s < nspin; s++) {
+        double a = 0, b = 0;
+        c.pred->judge(G[s]->g, tstp, c.rowcopy + s * rl, c.pred_corr + s * npred, a, b);
+        dl = std::max(dl, a);
+        dp = std::max(dp, b);
+      }
+      c.pred_last[0] = dl;
+      c.pred_last[1] = dp;
+      c.pred_judged++;
+      const bool won = dl <= dp;
+      if (won) c.pred_better++;
+      c.pred_window = (c.pred_window << 1) | (won ? 1u : 0u);
+      if (c.pred_judged >= 8 && __builtin_popcount(c.pred_window & 0xFFu) < 3) c.pred_active = false;
+    }
+    if (it > 0 && prev > 0.0) ratio = std::max(ratio, d / prev);
+    prev = d;
+    it++;
+    if (refresh && it < 2) continue;
+    if (d * std::min(1.0, c.contraction) <= tol || (ratio > 0.0 && d * std::min(1.0, 4.0 * ratio) <= tol)) break;
+  }
+  if (ratio > 0.0) {
+    c.contraction = std::min(1.0, 4.0 * ratio);
+    c.steps_since_measure = 0;
+  } else {
+    c.steps_since_measure++;
+  }
+  pt.mark(-1);
+  NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  pt.collect();
+  if (iters) *iters = it;
+}
+}  // namespace
+
+extern "C" {
+
 int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const nedy_buf *h_t,
                          double mu, int max_corr, double tol, int *iters, double *err_hist) {
   return guard([&] {
-    NEDY_REQUIRE(ctx && G && S && hmf && h_t, "null argument");
-    NEDY_REQUIRE(max_corr >= 1 && tol >= 0.0, "max_corr must be >= 1 and tol >= 0");
-    set_dev(ctx);
-    Ctx &c = ctx->c;
-    const int N = G->g.nao;
-    const i64 es = (i64)N * N;
-    NEDY_REQUIRE(h_t->bytes >= es * 16, "h_t buffer too small");
-    double2 *hT = hmf_row(hmf, ctx, tstp, N);
-    hmf_row(hmf, ctx, G->g.nt, N);
-    PhaseTimer pt(c);
-    pt.mark(0);
-    extrapolate(c, tstp, G->g);
-    const i64 npred = c.pred ? Predictor::row_elements(G->g, tstp) : 0;
-    const bool learned = c.pred && c.pred_active && npred > 0;
-    if (learned) {
-      if (c.pred_corr_cap < npred) {
-        if (c.pred_corr) cudaFree(c.pred_corr);
-        c.pred_corr = nullptr;
-        NEDY_CUDA(cudaMalloc(&c.pred_corr, sizeof(double2) * npred));
-        c.pred_corr_cap = npred;
-      }
-      c.pred->apply(G->g, tstp, c.pred_corr);
-    }
-    // Exit after iteration k once the estimated distance to the converged row, the
-    // change of iteration k times the corrector's contraction, is below tol.  The
-    // contraction is measured (ratio of successive changes, safety factor 4) whenever
-    // a step runs two or more iterations; until it is known, and every 8th step to keep
-    // it current, at least two iterations run.
-    const bool refresh = c.contraction >= 1.0 || c.steps_since_measure >= 8;
-    int it = 0;
-    double prev = 0.0, ratio = 0.0;
-    for (; it < max_corr;) {
-      save_row(c, G->g, tstp);
-      c.ws.reset();
-      pt.mark(1);
-      double2 *rho = c.ws.alloc<double2>(es);
-      get_dm(c, G->g, tstp, rho);
-      NEDY_CUDA(cudaMemcpyAsync(hT, h_t->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
-      double2 *h[1] = {hT};
-      hf_decomp(c, 1, h, rho);
-      DevGF *Ss[1] = {&S->g};
-      const DevGF *Gs[1] = {&G->g};
-      pt.mark(2);
-      sigma_df(c, tstp, 1, Ss, Gs);
-      pt.mark(3);
-      double e[3] = {0, 0, 0};
-      dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
-      const double d = row_change(c, G->g, tstp);
-      if (err_hist) err_hist[it] = d;
-      if (learned && it == 0) {
-        // the first iteration judges the learned prediction against the polynomial one;
-        // once 8 steps are judged, fewer than 3 wins among the last 8 switch back to the
-        // polynomial predictor
-        double dl = 0, dp = 0;
-        c.pred->judge(G->g, tstp, c.rowcopy, c.pred_corr, dl, dp);
-        c.pred_last[0] = dl;
-        c.pred_last[1] = dp;
-        c.pred_judged++;
-        const bool won = dl <= dp;
-        if (won) c.pred_better++;
-        c.pred_window = (c.pred_window << 1) | (won ? 1u : 0u);
-        if (c.pred_judged >= 8 && __builtin_popcount(c.pred_window & 0xFFu) < 3) c.pred_active = false;
-      }
-      if (it > 0 && prev > 0.0) ratio = std::max(ratio, d / prev);
-      prev = d;
-      it++;
-      if (refresh && it < 2) continue;
-      if (d * std::min(1.0, c.contraction) <= tol || (ratio > 0.0 && d * std::min(1.0, 4.0 * ratio) <= tol)) break;
-    }
-    if (ratio > 0.0) {
-      c.contraction = std::min(1.0, 4.0 * ratio);
-      c.steps_since_measure = 0;
-    } else {
-      c.steps_since_measure++;
-    }
-    pt.mark(-1);
-    NEDY_CUDA(cudaStreamSynchronize(c.stream));
-    pt.collect();
-    if (iters) *iters = it;
+    NEDY_REQUIRE(ctx, "null argument");
+    nedy_gf *Gs[1] = {G}, *Ss[1] = {S};
+    nedy_buf *hs[1] = {hmf};
+    const nedy_buf *hts[1] = {h_t};
+    step_tol(ctx, tstp, 1, Gs, Ss, hs, hts, &mu, max_corr, tol, iters, err_hist);
+  });
+}
+
+int nedy_decomp_spin_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
+                              nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
+                              double mu_up, double mu_dn, int max_corr, double tol, int *iters, double *err_hist) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx, "null argument");
+    nedy_gf *Gs[2] = {G_up, G_dn}, *Ss[2] = {S_up, S_dn};
+    nedy_buf *hs[2] = {hmf_up, hmf_dn};
+    const nedy_buf *hts[2] = {h_t_up, h_t_dn};
+    const double mus[2] = {mu_up, mu_dn};
+    step_tol(ctx, tstp, 2, Gs, Ss, hs, hts, mus, max_corr, tol, iters, err_hist);
   });
 }
 

@@ -657,6 +657,12 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
   const int N = G.nao, np = G.ntau + 1;
   const i64 es = (i64)N * N;
   if (c.mixK && c.mixK_src == G.mat && c.mixK_ver == G.mat_version && c.mixK_nao == N) return;
+  // two cached kernels: swap in the other one if it matches, else rebuild the older one
+  std::swap(c.mixK, c.mixK_alt);
+  std::swap(c.mixK_src, c.mixK_alt_src);
+  std::swap(c.mixK_ver, c.mixK_alt_ver);
+  std::swap(c.mixK_nao, c.mixK_alt_nao);
+  if (c.mixK && c.mixK_src == G.mat && c.mixK_ver == G.mat_version && c.mixK_nao == N) return;
   build_mixing_eval(c.col);
   const int Q2 = 2 * c.col.Q;
   if (c.mixK && c.mixK_nao != N) { cudaFree(c.mixK); c.mixK = nullptr; }

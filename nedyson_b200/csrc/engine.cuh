@@ -100,6 +100,11 @@ struct Ctx {
   const double2 *mixK_src = nullptr;
   unsigned long long mixK_ver = ~0ULL;
   int mixK_nao = 0;
+  // a second cached kernel (the other spin's G^M in unrestricted runs)
+  double2 *mixK_alt = nullptr;
+  const double2 *mixK_alt_src = nullptr;
+  unsigned long long mixK_alt_ver = ~0ULL;
+  int mixK_alt_nao = 0;
   // inverses of the time-local Dyson matrices M(t') = (i bd0/dt + mu) - hmf(t') - dt w0 Sig^R(t',t')
   // residual exit of the whole-step entry: copy of the new row before an iteration, the
   // measured contraction of the corrector (ratio of successive changes, with a safety

@@ -15,6 +15,11 @@ for the CPU oracle:
 * equilibrium: self-consistent restricted HF Fock matrix F and chemical
   potential mu at mid-gap; G^M(tau) and the first k+1 time steps of G are the
   free Green's function of F (G0_from_h0, reference src/dyson_free.h:226-297).
+* spin-unrestricted problems (``make_problem(..., spin=True)``): a second,
+  independent h0 for spin down, drawn after every restricted input so that the
+  spin-up problem equals the restricted one of the same seed; the same B^Q and
+  D for both spins; the equilibrium is the unrestricted HF one, with its own
+  Fock matrix and mid-gap mu per spin.
 """
 from __future__ import annotations
 
@@ -35,6 +40,14 @@ class Problem:
     D: np.ndarray
     seed: int
     meta: dict = field(default_factory=dict)
+    h0_dn: np.ndarray | None = None   # spin-down one-body Hamiltonian (unrestricted problems)
+
+    @property
+    def spin(self) -> bool:
+        return self.h0_dn is not None
+
+    def h0_of(self, s: int) -> np.ndarray:
+        return self.h0_dn if s == 1 else self.h0
 
     @property
     def U(self):
@@ -47,8 +60,7 @@ class Problem:
         return 2 * U.transpose(0, 2, 1, 3) - U
 
 
-def make_problem(nao: int, naux: int, seed: int, gap: float = 0.5, u_norm: float = 0.5) -> Problem:
-    rng = np.random.default_rng(seed)
+def _gapped_h0(rng, nao: int, gap: float) -> np.ndarray:
     a = rng.normal(size=(nao, nao))
     h0 = 0.5 * (a + a.T)
     w, v = np.linalg.eigh(h0)
@@ -58,7 +70,13 @@ def make_problem(nao: int, naux: int, seed: int, gap: float = 0.5, u_norm: float
         if g < gap:
             w[nocc:] += gap - g
     h0 = (v * w) @ v.T
-    h0 = 0.5 * (h0 + h0.T)
+    return 0.5 * (h0 + h0.T)
+
+
+def make_problem(nao: int, naux: int, seed: int, gap: float = 0.5, u_norm: float = 0.5,
+                 spin: bool = False) -> Problem:
+    rng = np.random.default_rng(seed)
+    h0 = _gapped_h0(rng, nao, gap)
     B = rng.normal(size=(naux, nao, nao))
     B = 0.5 * (B + B.transpose(0, 2, 1))
     # ||U||_F^2 = sum_{QP} (tr B^Q B^P)^2  (B symmetric)
@@ -68,7 +86,8 @@ def make_problem(nao: int, naux: int, seed: int, gap: float = 0.5, u_norm: float
     Vija = np.ascontiguousarray(B.transpose(1, 2, 0))
     d = rng.normal(size=(nao, nao))
     D = 0.5 * (d + d.T)
-    return Problem(nao, naux, h0, Vija, D, seed)
+    h0_dn = _gapped_h0(rng, nao, gap) if spin else None
+    return Problem(nao, naux, h0, Vija, D, seed, h0_dn=h0_dn)
 
 
 def drive(kind: str, t: float, k: int, dt: float, **kw) -> float:
@@ -107,6 +126,43 @@ def hf_fock(p: Problem, rho: np.ndarray) -> np.ndarray:
     Va = np.ascontiguousarray(V.transpose(2, 0, 1))  # V^a_ij
     K = (Va @ rho.T @ Va).sum(axis=0)                # K_ij = sum_a (V^a rho^T V^a)_ij
     return p.h0 + 2 * J - K
+
+
+def uhf_fock(p: Problem, rho_up: np.ndarray, rho_dn: np.ndarray):
+    """(F_up, F_dn) with F_s = h0_s + J[rho_up + rho_dn] - K[rho_s]
+    (molHFSolverSpinDecomp::solve_HF, reference src/molHFSolver.cpp:203-239)."""
+    V = p.Vija
+    X = np.einsum("kl,kla->a", rho_up + rho_dn, V)
+    J = np.einsum("ija,a->ij", V, X)
+    Va = np.ascontiguousarray(V.transpose(2, 0, 1))
+    out = []
+    for s, rho in enumerate((rho_up, rho_dn)):
+        K = (Va @ rho.T @ Va).sum(axis=0)
+        out.append(p.h0_of(s) + J - K)
+    return out[0], out[1]
+
+
+def uhf_equilibrium(p: Problem, beta: float, iters: int = 400, tol: float = 1e-13):
+    """Self-consistent unrestricted HF at inverse temperature beta: ((F_up, F_dn), (mu_up, mu_dn)),
+    nao//2 electrons per spin, each mu at the mid-gap of its own spin's spectrum."""
+    assert p.spin, "unrestricted equilibrium needs a spin problem"
+    N = p.nao
+    nocc = N // 2
+    F = [p.h0.astype(complex), p.h0_dn.astype(complex)]
+    mu = [0.0, 0.0]
+    for _ in range(iters):
+        rho = []
+        for s in range(2):
+            w, v = np.linalg.eigh(F[s])
+            mu[s] = 0.5 * (w[nocc - 1] + w[nocc]) if 0 < nocc < N else float(w.mean())
+            rho.append((v * fermi(beta, w - mu[s])) @ v.conj().T)
+        Fn = uhf_fock(p, rho[0], rho[1])
+        d = max(np.abs(Fn[s] - F[s]).max() for s in range(2))
+        F = list(Fn)
+        if d < tol:
+            break
+    F = [0.5 * (f + f.conj().T) for f in F]
+    return (F[0].real.copy(), F[1].real.copy()), (float(mu[0]), float(mu[1]))
 
 
 def hf_equilibrium(p: Problem, beta: float, iters: int = 200, tol: float = 1e-13):

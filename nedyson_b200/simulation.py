@@ -6,7 +6,9 @@
 (src/molNEsim_decomp_spin_impl.h:70-122).  The equilibrium state is the
 Hartree-Fock one of ``inputs.hf_equilibrium`` (the reference takes it from the
 external gfmol solver), and the external drive E(t) D is added to h0 inside
-h(t), gated to zero during the bootstrap window.
+h(t), gated to zero during the bootstrap window.  The unrestricted driver takes
+h(t) per spin (``Problem.h0_dn``); the reference uses one hcore for both spins,
+which is the case h0_dn == h0.
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import numpy as np
 
 from . import api
 from .greens import HostGF
-from .inputs import Problem, drive, g0_from_h0, hf_equilibrium
+from .inputs import Problem, drive, g0_from_h0, hf_equilibrium, uhf_equilibrium
 
 
 class DecompSimulation:
@@ -81,6 +83,93 @@ class DecompSimulation:
         hist = (C.c_double * m)()
         check(lib().nedy_decomp_tstp_tol(self.ctx.h, t, self.G.h, self.Sigma.h, self.hmf.h, self.ht.h, self.mu, m,
                                          float(tol), C.byref(it), hist))
+        return it.value, list(hist)[: it.value]
+
+    def run(self, nt: int | None = None, boot_iter: int = 50, boot_tol: float = 1e-12):
+        self.free_gf()
+        self.do_boot(boot_iter, boot_tol)
+        for t in range(self.k + 1, (nt if nt is not None else self.nt) + 1):
+            self.do_tstp(t)
+
+
+class DecompSpinSimulation:
+    """Spin-unrestricted density-fitted GF2 (reference src/molNEsim_decomp_spin_impl.h): free_gf
+    (:43-47) from the unrestricted HF equilibrium, do_boot (:63-84, the two dyson_start errors
+    summed), do_tstp (:86-108) through nedy_decomp_spin_tstp, do_tstp_tol through
+    nedy_decomp_spin_tstp_tol."""
+
+    def __init__(self, p: Problem, nt: int, ntau: int, beta: float, dt: float, k: int = 5,
+                 corr_steps: int = 5, drive_kind: str = "none", drive_kw: dict | None = None, device: int = 0,
+                 workspace_bytes: int = 0):
+        assert p.spin, "DecompSpinSimulation needs a spin problem (make_problem(..., spin=True))"
+        self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k
+        self.corr_steps = corr_steps
+        self.drive_kind, self.drive_kw = drive_kind, dict(drive_kw or {})
+        self.ctx = api.Context(nt, ntau, p.nao, k, beta, dt, device, workspace_bytes)
+        self.x, self.w = self.ctx.collocation()
+        N = p.nao
+        self.G = [api.green_func(self.ctx, nt, ntau, N, -1) for _ in range(2)]
+        self.Sigma = [api.green_func(self.ctx, nt, ntau, N, -1) for _ in range(2)]
+        self.solver = api.molGF2SolverSpinDecomp(self.ctx, p.Vija)
+        self.dyson = api.dyson(self.ctx)
+        self.hmf = [api.hmf_buffer(self.ctx, N) for _ in range(2)]
+        self.ht = [api.DeviceBuffer(self.ctx, N * N * 16) for _ in range(2)]
+        self.F, self.mu = uhf_equilibrium(p, beta)
+        self.boot_err = None
+
+    def h_of_t(self, t: int, s: int) -> np.ndarray:
+        E = drive(self.drive_kind, t * self.dt, self.k, self.dt, **self.drive_kw)
+        return (self.p.h0_of(s) + E * self.p.D).astype(np.complex128)
+
+    def initial_state(self, s: int) -> HostGF:
+        g = HostGF(self.nt, self.ntau, self.p.nao, -1)
+        g0_from_h0(g, self.x, self.mu[s], self.F[s], self.beta, self.dt, self.k)
+        return g
+
+    def free_gf(self):
+        for s in range(2):
+            self.G[s].from_host(self.initial_state(s))
+            hm = np.zeros((self.nt + 1, self.p.nao, self.p.nao), np.complex128)
+            hm[: self.k + 1] = self.F[s]
+            self.hmf[s].upload(hm)
+
+    def do_boot(self, max_iter: int = 50, tol: float = 1e-12) -> float:
+        err = None
+        for _ in range(max_iter + 1):
+            for t in range(self.k + 1):
+                self.solver.solve(t, self.Sigma, self.G)
+            err = sum(self.dyson.dyson_start(self.G[s], self.Sigma[s], self.hmf[s], self.mu[s]) for s in range(2))
+            if err < tol:
+                break
+        self.boot_err = err
+        return err
+
+    def _upload_h(self, t):
+        for s in range(2):
+            self.ht[s].upload(self.h_of_t(t, s))
+
+    def do_tstp(self, t: int) -> float:
+        import ctypes as C
+        from ._lib import check, lib
+        self._upload_h(t)
+        e = C.c_double()
+        check(lib().nedy_decomp_spin_tstp(self.ctx.h, t, self.G[0].h, self.G[1].h, self.Sigma[0].h,
+                                          self.Sigma[1].h, self.hmf[0].h, self.hmf[1].h, self.ht[0].h,
+                                          self.ht[1].h, self.mu[0], self.mu[1], self.corr_steps, C.byref(e)))
+        return e.value
+
+    def do_tstp_tol(self, t: int, tol: float, max_corr: int | None = None):
+        """One step with the residual exit over both spins: (iterations, changes per iteration)."""
+        import ctypes as C
+        from ._lib import check, lib
+        self._upload_h(t)
+        m = max_corr or self.corr_steps
+        it = C.c_int()
+        hist = (C.c_double * m)()
+        check(lib().nedy_decomp_spin_tstp_tol(self.ctx.h, t, self.G[0].h, self.G[1].h, self.Sigma[0].h,
+                                              self.Sigma[1].h, self.hmf[0].h, self.hmf[1].h, self.ht[0].h,
+                                              self.ht[1].h, self.mu[0], self.mu[1], m, float(tol), C.byref(it),
+                                              hist))
         return it.value, list(hist)[: it.value]
 
     def run(self, nt: int | None = None, boot_iter: int = 50, boot_tol: float = 1e-12):

@@ -131,3 +131,29 @@ def test_hf_forms_equal_loops():
     f.hf(g1, rho)
     f.hf_loop(g2, rho)
     assert np.linalg.norm(g1 - g2) < 1e-10
+
+
+def test_uhf_fock_matches_oracle_hf_spin():
+    from nedyson_b200.inputs import make_problem, uhf_fock
+    p = make_problem(5, 9, seed=41, spin=True)
+    rng = np.random.default_rng(3)
+    rho = []
+    for _ in range(2):
+        x = rng.standard_normal((5, 5)) + 1j * rng.standard_normal((5, 5))
+        rho.append(0.5 * (x + x.conj().T))
+    Fu, Fd = uhf_fock(p, rho[0], rho[1])
+    hu, hd = p.h0.astype(complex), p.h0_dn.astype(complex)
+    po.DF(p.Vija).hf_spin(hu, hd, np.stack(rho))
+    assert np.abs(Fu - hu).max() < 1e-12 and np.abs(Fd - hd).max() < 1e-12
+
+
+def test_uhf_equilibrium_with_equal_spins_is_rhf():
+    from nedyson_b200.inputs import make_problem, uhf_equilibrium, hf_equilibrium
+    p = make_problem(8, 16, seed=43, spin=True)
+    q = make_problem(8, 16, seed=43)
+    assert np.array_equal(p.h0, q.h0) and np.array_equal(p.Vija, q.Vija)
+    p.h0_dn = p.h0.copy()
+    (Fu, Fd), (mu_u, mu_d) = uhf_equilibrium(p, 10.0)
+    F, mu = hf_equilibrium(q, 10.0)
+    assert np.abs(Fu - F).max() < 1e-10 and np.abs(Fd - F).max() < 1e-10
+    assert abs(mu_u - mu) < 1e-10 and abs(mu_d - mu) < 1e-10
