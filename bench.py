@@ -11,8 +11,9 @@ Two forms run the same window from the same state:
                    [density matrices, unrestricted HF mean field, GF2 self-energy rows T
                    of both spins, Dyson step row T per spin], every contraction in FP64
                    (the reference's algorithm);
-  split+predictor  nedy_decomp_spin_tstp_tol on a context in NEDY_PREC_SPLIT_BF16X3: the
-                   self-energy contractions as BF16 piece products on tcgen05, the
+  split+predictor  nedy_decomp_spin_tstp_tol on a context in NEDY_PREC_SPLIT_BF16X2 (or
+                   _BF16X3 with --split-mode bf16x3): the self-energy contractions as
+                   BF16 piece products on tcgen05, the
                    predictor, and the residual exit at tol = 1e-8 (at most 5 iterations).
 
 value is the split+predictor form (the headline); the plain form, the iterations per
@@ -82,6 +83,8 @@ def parse():
     ap.add_argument("--restricted", action="store_true",
                     help="restricted simulation instead of the spin-unrestricted one")
     ap.add_argument("--predictor", default="learned", choices=["learned", "poly"])
+    ap.add_argument("--split-mode", default="bf16x2", choices=["bf16x3", "bf16x2"],
+                    help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
     ap.add_argument("--beta", type=float, default=20.0)
@@ -281,8 +284,9 @@ def fp64_gemm_peak(device: int) -> float:
 def run_engine(args, dist: Dist):
     import torch
     from nedyson_b200 import api
-    from nedyson_b200._lib import LES, RET, TV, MAT, PREC_FP64, PREC_SPLIT_BF16X3, check, lib
+    from nedyson_b200._lib import LES, RET, TV, MAT, PREC_FP64, PREC_SPLIT_BF16X3, PREC_SPLIT_BF16X2, check, lib
     from nedyson_b200.inputs import make_problem, hf_equilibrium, uhf_equilibrium, free_history, drive
+    PREC_SPLIT = PREC_SPLIT_BF16X2 if args.split_mode == "bf16x2" else PREC_SPLIT_BF16X3
 
     dev = dist.local
     torch.cuda.set_device(dev)
@@ -349,7 +353,7 @@ def run_engine(args, dist: Dist):
             berr = sum(dy.dyson_start(G[s], S[s], hmf[s], mus[s]) for s in range(ns))
             if berr < 1e-12:
                 break
-        ctx.set_precision(PREC_SPLIT_BF16X3)
+        ctx.set_precision(PREC_SPLIT_BF16X3)  # the same state for either split mode
         for t in range(kk + 1, t_first):
             step_tol(t, 1e-10)
         ctx.synchronize()
@@ -435,7 +439,7 @@ def run_engine(args, dist: Dist):
 
     T_timed = list(range(t_first + W, t_first + W + K))
     # shared warm-up: W plain steps define the starting state of both forms
-    ctx.set_precision(PREC_SPLIT_BF16X3 if args.split_only else PREC_FP64)
+    ctx.set_precision(PREC_SPLIT if args.split_only else PREC_FP64)
     for t in range(t_first, t_first + W):
         (step_split if args.split_only else step_plain)(t)
     ctx.synchronize()
@@ -445,7 +449,7 @@ def run_engine(args, dist: Dist):
         rows_plain = window_rows(T_timed)
         e_plain = energies(T_timed)
     # split+predictor: warm-up on the window rows (recomputed below from the same history)
-    ctx.set_precision(PREC_SPLIT_BF16X3)
+    ctx.set_precision(PREC_SPLIT)
     if pred is not None:
         ctx.set_predictor(pred)
     for t in T_timed[:W]:
@@ -582,7 +586,9 @@ def main():
     plain_value = total_steps / pl["secs"] if pl else None
     T_mid = r["T"][len(r["T"]) // 2]
     peaks, src = measured_peaks()
-    cfg["precision"] = "split BF16x3 self-energy (tcgen05), FP64 Dyson/HF/density; plain form FP64 throughout"
+    cfg["precision"] = ({"bf16x2": "split self-energy, two BF16 pieces per operand, products hi*hi + hi*lo + lo*hi",
+                         "bf16x3": "split self-energy, three BF16 pieces per operand, six products"}[args.split_mode] +
+                        " (tcgen05, FP32 accumulation), FP64 Dyson/HF/density; plain form FP64 throughout")
     cfg["predictor"] = ("learned MLP correction of the k=5 extrapolation (polynomial fallback)" if args.predictor == "learned"
                         else "polynomial extrapolation (k=5)") + " + residual exit at max|dG| estimate <= tol"
     cfg["state"] = (f"GF2 trajectory from the {'restricted' if args.restricted else 'unrestricted'} HF equilibrium "

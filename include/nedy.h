@@ -45,11 +45,15 @@ enum nedy_status {
 enum nedy_component { NEDY_LES = 0, NEDY_RET = 1, NEDY_TV = 2, NEDY_MAT = 3 };
 /* Arithmetic of the self-energy contractions (nedy_ctx_set_precision).
  * FP64: every product in FP64 on the DMMA tensor cores (the reference's arithmetic).
- * SPLIT_BF16X3: the exchange contractions (the nao^4*naux part) as BF16 piece
- *   products on tcgen05: each FP64 operand is split into three BF16 pieces, the six
- *   piece products with combined weight >= 2^-16 are accumulated in FP32.  The Dyson
- *   solves, the mean field, the density matrix and the residuals stay FP64. */
-enum nedy_precision { NEDY_PREC_FP64 = 0, NEDY_PREC_SPLIT_BF16X3 = 1 };
+ * SPLIT_BF16X3: the density-fitted self-energy contractions as BF16 piece products on
+ *   tcgen05: each operand is split into three BF16 pieces, the six piece products with
+ *   combined weight >= 2^-16 are accumulated in FP32.
+ * SPLIT_BF16X2: the same with two pieces per operand (hi, lo) and the three products
+ *   hi*hi + hi*lo + lo*hi (about 2^-17 relative per product instead of FP32 rounding):
+ *   half the tensor work of SPLIT_BF16X3.
+ * In every mode the Dyson solves, the mean field, the density matrix and the residuals
+ * stay FP64; the full-U self-energy is always FP64. */
+enum nedy_precision { NEDY_PREC_FP64 = 0, NEDY_PREC_SPLIT_BF16X3 = 1, NEDY_PREC_SPLIT_BF16X2 = 2 };
 
 typedef struct nedy_ctx nedy_ctx;
 typedef struct nedy_gf nedy_gf;

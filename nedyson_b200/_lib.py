@@ -13,7 +13,7 @@ LIBPATH = os.path.join(HERE, "libnedy_b200.so")
 
 NEDY_OK = 0
 LES, RET, TV, MAT = 0, 1, 2, 3
-PREC_FP64, PREC_SPLIT_BF16X3 = 0, 1
+PREC_FP64, PREC_SPLIT_BF16X3, PREC_SPLIT_BF16X2 = 0, 1, 2
 
 
 class NedyConfig(C.Structure):

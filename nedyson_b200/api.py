@@ -56,7 +56,7 @@ class Context:
         check(lib().nedy_ctx_synchronize(self.h))
 
     def set_precision(self, mode):
-        """Self-energy arithmetic: _lib.PREC_FP64 (default) or _lib.PREC_SPLIT_BF16X3."""
+        """Self-energy arithmetic: _lib.PREC_FP64 (default), _lib.PREC_SPLIT_BF16X3 or _lib.PREC_SPLIT_BF16X2."""
         check(lib().nedy_ctx_set_precision(self.h, int(mode)))
 
     def set_predictor(self, pred: "Predictor | None"):

@@ -295,7 +295,8 @@ int nedy_ctx_stream(nedy_ctx *ctx, void **stream) {
 int nedy_ctx_set_precision(nedy_ctx *ctx, int mode) {
   return guard([&] {
     NEDY_REQUIRE(ctx, "null context");
-    NEDY_REQUIRE(mode == NEDY_PREC_FP64 || mode == NEDY_PREC_SPLIT_BF16X3, "unknown precision mode");
+    NEDY_REQUIRE(mode == NEDY_PREC_FP64 || mode == NEDY_PREC_SPLIT_BF16X3 || mode == NEDY_PREC_SPLIT_BF16X2,
+                 "unknown precision mode");
     ctx->c.precision = mode;
   });
 }

@@ -167,18 +167,21 @@ struct DF {
     gemm(g, s);
   }
   // BF16 pieces of Vija as the shared B operand of the split S contraction (rows (q,j), K = b).
+  // Real static operands are split once into 3 pieces; piece p of a real array is plane p, so
+  // the same planes serve a 2-piece view.
   Pieces vpieces(int np) {
     Pieces v;
-    v.rows = (int)es; v.kpad = kpad64(A); v.nb = 1; v.ncomp = 1; v.np = np;
-    if (!c.Vp || c.Vp_np != np) {
+    v.rows = (int)es; v.kpad = kpad64(A); v.nb = 1; v.ncomp = 1; v.np = 3;
+    if (!c.Vp || c.Vp_np != 3) {
       if (c.Vp) cudaFree(c.Vp);
       c.Vp = nullptr;
       NEDY_CUDA(cudaMalloc(&c.Vp, v.elems() * 2));
-      c.Vp_np = np;
+      c.Vp_np = 3;
       v.p = (__nv_bfloat16 *)c.Vp;
       split_pieces(rowmajor(c.Vija, A), false, false, A, v, s);
     }
     v.p = (__nv_bfloat16 *)c.Vp;
+    v.np = np;
     return v;
   }
   // Bubble contractions in split precision (same results as P() and W()):
@@ -220,13 +223,14 @@ struct DF {
   // array written directly by the producing contraction in the layout its consumer reads.
   Pieces static_pieces(void *&slot, const View &v, int rows, int K, int np) {
     Pieces x;
-    x.rows = rows; x.kpad = kpad64(K); x.nb = 1; x.ncomp = 1; x.np = np;
+    x.rows = rows; x.kpad = kpad64(K); x.nb = 1; x.ncomp = 1; x.np = 3;
     if (!slot) {
       NEDY_CUDA(cudaMalloc(&slot, x.elems() * 2));
       x.p = (__nv_bfloat16 *)slot;
       split_pieces(v, false, false, K, x, s);
     }
     x.p = (__nv_bfloat16 *)slot;
+    x.np = np;
     return x;
   }
   Pieces vanj(int np) {  // rows (a,n), K = j: V^a_nj = Vija[n][j][a]
@@ -486,10 +490,10 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
     NEDY_CUDA(cudaMemsetAsync(Sig[s]->lesptr(0, T), 0, sizeof(double2) * (T + 1) * es, c.stream));
     NEDY_CUDA(cudaMemsetAsync(Sig[s]->tvptr(T, 0), 0, sizeof(double2) * (ntau + 1) * es, c.stream));
   }
-  const bool split = c.precision == NEDY_PREC_SPLIT_BF16X3;
+  const bool split = c.precision != NEDY_PREC_FP64;
   int chunk, sub;
   chunking(c, chunk, sub, split);
-  const int np = 3;
+  const int np = c.precision == NEDY_PREC_SPLIT_BF16X2 ? 2 : 3;
   if (split) NEDY_REQUIRE(kpad64((int)es) <= 65535 * 64, "split self-energy: nao too large");
 
   // ---------------- lesser and mixed rows: one bubble unit + one exchange unit per slice.

@@ -550,10 +550,10 @@ struct Cand {
   int bn, stages, kdiv;  // kdiv: divide the automatic K split by this (FP64-accumulating outputs)
 };
 struct TuneKey {
-  int dev, nA, nB, out_pieces, acc, M, N, kpad;
+  int dev, np, nA, nB, out_pieces, acc, M, N, kpad;
   bool operator<(const TuneKey &o) const {
-    return std::tie(dev, nA, nB, out_pieces, acc, M, N, kpad) <
-           std::tie(o.dev, o.nA, o.nB, o.out_pieces, o.acc, o.M, o.N, o.kpad);
+    return std::tie(dev, np, nA, nB, out_pieces, acc, M, N, kpad) <
+           std::tie(o.dev, o.np, o.nA, o.nB, o.out_pieces, o.acc, o.M, o.N, o.kpad);
   }
 };
 struct Pending {
@@ -638,7 +638,7 @@ std::string split_tune_report() {
     poll(e);
     const TuneKey &k = kv.first;
     r += "M=" + std::to_string(k.M) + " N=" + std::to_string(k.N) + " K=" + std::to_string(k.kpad) +
-         (k.nA == 2 ? (k.nB == 2 ? " cxc" : " cxr") : " rxc") + (k.out_pieces ? " pieces" : " fp64") + ":";
+         (k.nA == 2 ? (k.nB == 2 ? " cxc" : " cxr") : " rxc") + (k.out_pieces ? " pieces" : " fp64") + " np=" + std::to_string(k.np) + ":";
     for (size_t i = 0; i < e.cands.size(); i++) {
       char buf[96];
       snprintf(buf, sizeof(buf), " %d/%d/k%d=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv,
@@ -708,7 +708,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (g_tune_on) {
-      const TuneKey key{dev, P.nA, P.nB, g.out_pieces ? 1 : 0, g.accumulate ? 1 : 0, g.M, g.N, g.A.kpad};
+      const TuneKey key{dev, P.np, P.nA, P.nB, g.out_pieces ? 1 : 0, g.accumulate ? 1 : 0, g.M, g.N, g.A.kpad};
       auto it = g_tune.find(key);
       if (it == g_tune.end()) {
         TuneEntry e;
