@@ -87,6 +87,8 @@ def parse():
                     help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="fixed split GEMM tiles (profiling runs: the tuner's timings are meaningless under ncu)")
     ap.add_argument("--beta", type=float, default=20.0)
     ap.add_argument("--dt", type=float, default=0.01)
     ap.add_argument("--seed", type=int, default=7)
@@ -290,6 +292,8 @@ def run_engine(args, dist: Dist):
 
     dev = dist.local
     torch.cuda.set_device(dev)
+    if args.no_autotune:
+        check(lib().nedy_split_autotune(0))
     N, A, ntau, K, W = args.nao, args.naux, args.ntau, args.steps, args.warmup
     spin = not args.restricted
     ns = 2 if spin else 1
