@@ -95,6 +95,16 @@ int nedy_split_stats(int on, double *pipe_flops, double *ms);
  * computes the same result.  The report lists classes, candidate times and choices. */
 int nedy_split_autotune(int on);
 int nedy_split_tune_report(char *buf, int len);
+/* Check of one split GEMM kernel instance (test hook, no reference counterpart):
+ * C (nb x M x N) = 0.75 * op(A) op(B)^T (+ C when accumulate) on seeded uniform operands
+ * (complex when *_cplx, conjugated when conj_*), split into npieces BF16 pieces, with the
+ * given instance: tile_n 64/128/256 output columns per CTA, stages, k_block 0 for the
+ * per-product kernel or 32/64 for the one-load kernel, kdiv the K-split divisor.
+ * *rel_err = max |C - C_fp64| / max |C_fp64|; NEDY_ERR_ARG for an instance that does not
+ * exist or does not fit in shared memory. */
+int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, int b_cplx, int conj_a, int conj_b,
+                          int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,
+                          unsigned long long seed, double *rel_err);
 int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
 /* Number of engine kernel launches issued by this process so far. */
 unsigned long long nedy_launch_count(void);

@@ -315,6 +315,31 @@ int nedy_split_tune_report(char *buf, int len) {
   });
 }
 
+int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, int b_cplx, int conj_a, int conj_b,
+                          int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,
+                          unsigned long long seed, double *rel_err) {
+  return guard([&] {
+    NEDY_REQUIRE(rel_err, "null argument");
+    NEDY_CUDA(cudaSetDevice(device));
+    SplitCheck k;
+    k.M = M; k.N = N; k.K = K; k.nb = nb;
+    k.a_cplx = a_cplx; k.b_cplx = b_cplx; k.conjA = conj_a; k.conjB = conj_b; k.np = npieces;
+    k.out_pieces = out_pieces; k.accumulate = accumulate;
+    k.bn = tile_n; k.stages = stages; k.bk = k_block; k.kdiv = kdiv;
+    k.seed = seed;
+    k.alpha = 0.75;
+    cudaStream_t st = nullptr;
+    NEDY_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    try {
+      *rel_err = split_gemm_check(k, st);
+    } catch (...) {
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamDestroy(st);
+  });
+}
+
 int nedy_split_stats(int on, double *pipe_flops, double *ms) {
   return guard([&] { split_stats(on != 0, pipe_flops, ms); });
 }

@@ -17,6 +17,7 @@
 #include "split_gemm.cuh"
 #include <cuda.h>
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -41,6 +42,7 @@ struct Params {
   int a_nb, b_nb;  // batches stored in the A / B maps (1: shared)
   int a_b0, b_b0;  // first stored batch used
   int nA, nB, nmma, nprod, np, stage_bytes;
+  int fuse;  // one-load kernel, real x complex: one N = 2 BN product covers both parts
   int a_comp[2], b_comp[2];  // plane group (0 real, 1 imaginary) of each A / B slot
   Mma mma[4];
   int pa[6], pb[6];  // piece products
@@ -113,6 +115,21 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
   d |= (uint64_t)2 << 61;                        // SWIZZLE_128B
   return d;
+}
+// K-major operand tile, 64-byte swizzle: rows of 32 BF16 (64 B), 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;                        // SWIZZLE_64B
+  return d;
+}
+template <int BKT>
+__device__ __forceinline__ uint64_t op_desc(uint32_t saddr) {
+  static_assert(BKT == 64 || BKT == 32, "K block of 32 or 64");
+  return BKT == 64 ? sw128_desc(saddr) : sw64_desc(saddr);
 }
 
 // kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major, M = 128, N = bn.
@@ -233,13 +250,24 @@ __device__ __forceinline__ void store_pieces16_rows(const Params &P, __nv_bfloat
   }
 }
 
-template <int BN, int STAGES>
+// OL = false: one stage holds one piece product of one K block (the A and B tiles of that
+//   product), BKT = 64;
+// OL = true ("one load"): one stage holds every piece of one K block (BKT = 32 or 64), and
+//   the MMA warp issues all piece products from it, so each piece tile crosses L2 -> SM
+//   once per K block instead of once per product it takes part in.  A slots are ordered
+//   piece-major (slot p nA + component), B slots likewise, so the real and imaginary B
+//   tiles of one piece are adjacent: for real x complex products one MMA with N = 2 BN
+//   writes both parts (TMEM columns [0, BN) real, [BN, 2 BN) imaginary).
+template <int BN, int STAGES, int BKT, bool OL>
 __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ Params P) {
-  constexpr int B_BYTES = BN * BK * 2;
+  static_assert(OL || BKT == BK, "the per-product kernel uses 64-wide K blocks");
+  constexpr int A_TILE = BM * BKT * 2;
+  constexpr int B_BYTES = BN * BKT * 2;
   constexpr uint32_t TCOLS = 2 * BN;
   constexpr uint32_t IDESC = idesc_for(BN);
+  constexpr uint32_t IDESC2 = idesc_for(BN * 2 <= 256 ? BN * 2 : BN);
   extern __shared__ uint8_t sraw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)sraw + 1023) & ~(uintptr_t)1023);
   uint64_t *bar = (uint64_t *)(smem + STAGES * P.stage_bytes);  // full[STAGES], empty[STAGES], done
@@ -251,7 +279,7 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
   const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
   const int kb0 = ks * P.kb_per_split;
   const int nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
-  int iters = nkb * P.nprod;
+  int iters = OL ? nkb : nkb * P.nprod;
   const uint32_t full0 = smem_u32(bar), empty0 = smem_u32(bar + STAGES), done = smem_u32(bar + 2 * STAGES);
 
   if (threadIdx.x == 0) {
@@ -283,15 +311,29 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
       if (it >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) break;
-      const int pr = it / nkb, kb = kb0 + it % nkb;
       const uint32_t base = smem_u32(smem + s * P.stage_bytes);
       mbar_expect_tx(full0 + 8 * s, P.stage_bytes);
-      for (int i = 0; i < P.nA; i++)
-        tma_load_3d(base + i * A_BYTES, &tmA, full0 + 8 * s, kb * BK, m0,
-                    (P.a_comp[i] * P.np + P.pa[pr]) * P.a_nb + (P.a_nb > 1 ? P.a_b0 + b : 0));
-      for (int j = 0; j < P.nB; j++)
-        tma_load_3d(base + P.nA * A_BYTES + j * B_BYTES, &tmB, full0 + 8 * s, kb * BK, n0,
-                    (P.b_comp[j] * P.np + P.pb[pr]) * P.b_nb + (P.b_nb > 1 ? P.b_b0 + b : 0));
+      const int ab = P.a_nb > 1 ? P.a_b0 + b : 0, bb = P.b_nb > 1 ? P.b_b0 + b : 0;
+      if (OL) {
+        const int kb = kb0 + it;
+        const uint32_t bbase = base + P.np * P.nA * A_TILE;
+        for (int p = 0; p < P.np; p++) {
+          for (int i = 0; i < P.nA; i++)
+            tma_load_3d(base + (p * P.nA + i) * A_TILE, &tmA, full0 + 8 * s, kb * BKT, m0,
+                        (P.a_comp[i] * P.np + p) * P.a_nb + ab);
+          for (int j = 0; j < P.nB; j++)
+            tma_load_3d(bbase + (p * P.nB + j) * B_BYTES, &tmB, full0 + 8 * s, kb * BKT, n0,
+                        (P.b_comp[j] * P.np + p) * P.b_nb + bb);
+        }
+      } else {
+        const int pr = it / nkb, kb = kb0 + it % nkb;
+        for (int i = 0; i < P.nA; i++)
+          tma_load_3d(base + i * A_TILE, &tmA, full0 + 8 * s, kb * BKT, m0,
+                      (P.a_comp[i] * P.np + P.pa[pr]) * P.a_nb + ab);
+        for (int j = 0; j < P.nB; j++)
+          tma_load_3d(base + P.nA * A_TILE + j * B_BYTES, &tmB, full0 + 8 * s, kb * BKT, n0,
+                      (P.b_comp[j] * P.np + P.pb[pr]) * P.b_nb + bb);
+      }
     }
   } else if (warp == 5 && lane == 0) {
     // ---- MMA issuer
@@ -302,20 +344,35 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
       if (!mbar_wait(full0 + 8 * s, ph, P.err, 2)) break;
       tc_fence_after();
       const uint32_t base = smem_u32(smem + s * P.stage_bytes);
-      for (int q = 0; q < P.nmma; q++) {
-        const Mma mq = P.mma[q];
-        const uint64_t da = sw128_desc(base + mq.sa * A_BYTES);
-        const uint64_t db = sw128_desc(base + P.nA * A_BYTES + mq.sb * B_BYTES);
-        const uint32_t idesc = IDESC | (mq.neg ? (1u << 13) : 0u);
-        const uint32_t tacc = tmem + (uint32_t)(mq.acc * BN);
+      const int nprod = OL ? P.nprod : 1;
+      for (int pr = 0; pr < nprod; pr++) {
+        // slots of this product's A / B tiles inside the stage
+        const int sa0 = OL ? P.pa[pr] * P.nA : 0, sb0 = OL ? P.pb[pr] * P.nB : 0;
+        const uint32_t bbase = base + (OL ? P.np : 1) * P.nA * A_TILE;
+        if (OL && BN * 2 <= 256 && P.fuse) {
+          const uint64_t da = op_desc<BKT>(base + sa0 * A_TILE);
+          const uint64_t db = op_desc<BKT>(bbase + sb0 * B_BYTES);
 #pragma unroll
-        for (int k = 0; k < BK / 16; k++)  // K = 16 per instruction: +32 bytes inside the swizzle atom
-          mma_bf16(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
-                   ((mq.acc ? started1 : started0) || k > 0) ? 1u : 0u);
-        if (mq.acc)
-          started1 = true;
-        else
-          started0 = true;
+          for (int k = 0; k < BKT / 16; k++)
+            mma_bf16(tmem, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), IDESC2, (started0 || k > 0) ? 1u : 0u);
+          started0 = started1 = true;
+          continue;
+        }
+        for (int q = 0; q < P.nmma; q++) {
+          const Mma mq = P.mma[q];
+          const uint64_t da = op_desc<BKT>(base + (sa0 + mq.sa) * A_TILE);
+          const uint64_t db = op_desc<BKT>(bbase + (sb0 + mq.sb) * B_BYTES);
+          const uint32_t idesc = IDESC | (mq.neg ? (1u << 13) : 0u);
+          const uint32_t tacc = tmem + (uint32_t)(mq.acc * BN);
+#pragma unroll
+          for (int k = 0; k < BKT / 16; k++)  // K = 16 per instruction: +32 bytes inside the swizzle atom
+            mma_bf16(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                     ((mq.acc ? started1 : started0) || k > 0) ? 1u : 0u);
+          if (mq.acc)
+            started1 = true;
+          else
+            started0 = true;
+        }
       }
       mma_commit(empty0 + 8 * s);
     }
@@ -446,16 +503,18 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-CUtensorMap make_map(const Pieces &x, int box_rows) {
+CUtensorMap make_map(const Pieces &x, int box_rows, int bk) {
   NEDY_REQUIRE(x.p && x.kpad % 64 == 0 && x.rows > 0, "split gemm: bad piece planes");
   NEDY_REQUIRE(((uintptr_t)x.p & 15) == 0, "split gemm: piece planes not 16-byte aligned");
   CUtensorMap m;
   const cuuint64_t dims[3] = {(cuuint64_t)x.kpad, (cuuint64_t)x.rows, (cuuint64_t)x.ncomp * x.np * x.nb};
   const cuuint64_t strides[2] = {(cuuint64_t)x.kpad * 2, (cuuint64_t)x.kpad * 2 * x.rows};
-  const cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
+  NEDY_REQUIRE(bk == 64 || bk == 32, "split gemm: K block of 32 or 64");
+  const cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)box_rows, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)x.p, dims, strides, box, es,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   NEDY_REQUIRE(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return m;
@@ -524,7 +583,7 @@ void split_stats(bool on, double *flops, double *ms) {
   g_stats_on = on;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int BKT = BK, bool OL = false>
 void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 grid, cudaStream_t s) {
   static bool attr[64] = {false};
   int dev = 0;
@@ -533,11 +592,11 @@ void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 
   const int bytes = smem_bytes(P.stage_bytes, STAGES);
   NEDY_REQUIRE(STAGES * P.stage_bytes <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
   if (!attr[dev]) {
-    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   smem_bytes(SMEM_LIMIT / STAGES, STAGES)));
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<BN, STAGES, BKT, OL>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(SMEM_LIMIT / STAGES, STAGES)));
     attr[dev] = true;
   }
-  split_gemm_kernel<BN, STAGES><<<grid, THREADS, bytes, s>>>(ma, mb, P);
+  split_gemm_kernel<BN, STAGES, BKT, OL><<<grid, THREADS, bytes, s>>>(ma, mb, P);
   NEDY_CHECK_LAUNCH();
 }
 
@@ -548,6 +607,7 @@ void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 
 namespace {
 struct Cand {
   int bn, stages, kdiv;  // kdiv: divide the automatic K split by this (FP64-accumulating outputs)
+  int bk;                // 0: per-product kernel (64-wide K blocks); 32 / 64: one-load kernel
 };
 struct TuneKey {
   int dev, np, nA, nB, out_pieces, acc, M, N, kpad;
@@ -572,26 +632,43 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
 bool g_tune_on = true;
 
-std::vector<Cand> candidates(int nA, int nB, int N, bool acc) {
+// shared memory of one stage
+int stage_bytes_for(int nA, int nB, int np, int bn, int bk) {
+  return bk == 0 ? nA * A_BYTES + nB * bn * BK * 2 : np * (nA * BM * bk * 2 + nB * bn * bk * 2);
+}
+
+std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
   std::vector<Cand> c;
   if (N <= 64 && acc) {  // one output tile per batch: the K split is what there is to tune
-    for (int kd : {1, 2, 4, 8}) c.push_back({64, 4, kd});
+    for (int kd : {1, 2, 4, 8}) c.push_back({64, 4, kd, 0});
     return c;
   }
   for (int bn : {64, 128, 256}) {
     if (bn > 64 && N <= 64) continue;    // one 64-wide tile covers the output
     if (bn == 256 && N <= 128) continue;
-    const int sb = nA * A_BYTES + nB * bn * BK * 2;
+    const int sb = stage_bytes_for(nA, nB, np, bn, 0);
     const int st = std::min(4, SMEM_LIMIT / sb);
     if (st < 2) continue;
     if (bn == 64) {
-      if (st >= 4) c.push_back({64, 4, 1});
+      if (st >= 4) c.push_back({64, 4, 1, 0});
     } else if (bn == 128) {
-      c.push_back({128, 2, 1});
-      if (st >= 3) c.push_back({128, std::min(st, 4), 1});
+      c.push_back({128, 2, 1, 0});
+      if (st >= 3) c.push_back({128, std::min(st, 4), 1, 0});
     } else {
-      c.push_back({256, std::min(st, 3), 1});
-      if (acc) c.push_back({256, std::min(st, 3), 2});
+      c.push_back({256, std::min(st, 3), 1, 0});
+      if (acc) c.push_back({256, std::min(st, 3), 2, 0});
+    }
+  }
+  // one-load kernel: every piece of a K block per stage
+  for (int bn : {128, 256}) {
+    if (N <= 64 || (bn == 256 && N <= 128)) continue;
+    for (int bk : {32, 64}) {
+      const int sb = stage_bytes_for(nA, nB, np, bn, bk);
+      const int st = std::min(4, SMEM_LIMIT / sb);
+      if (st < 2) continue;
+      c.push_back({bn, 2, 1, bk});
+      if (st >= 3) c.push_back({bn, std::min(st, 4), 1, bk});
+      if (acc && bn == 256) c.push_back({bn, 2, 2, bk});
     }
   }
   return c;
@@ -641,7 +718,9 @@ std::string split_tune_report() {
          (k.nA == 2 ? (k.nB == 2 ? " cxc" : " cxr") : " rxc") + (k.out_pieces ? " pieces" : " fp64") + " np=" + std::to_string(k.np) + ":";
     for (size_t i = 0; i < e.cands.size(); i++) {
       char buf[96];
-      snprintf(buf, sizeof(buf), " %d/%d/k%d=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv,
+      char ol[16] = "";
+      if (e.cands[i].bk) snprintf(ol, sizeof(ol), "/ol%d", e.cands[i].bk);
+      snprintf(buf, sizeof(buf), " %d/%d/k%d%s=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv, ol,
                e.trials[i] ? e.best[i] * 1e3 : -1.0, (int)i == e.chosen ? "*" : "");
       r += buf;
     }
@@ -664,7 +743,6 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   memset(&P, 0, sizeof(P));
   P.M = g.M;
   P.N = g.N;
-  P.kblocks = g.A.kpad / BK;
   P.nb = g.nb;
   P.a_nb = g.A.nb;
   P.b_nb = g.B.nb;
@@ -701,18 +779,30 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   int BNsel = g.N <= 64 ? 64 : g.out_pieces ? 128 : 256;
   int STsel = 0;  // 0: as many stages as fit
   int KDsel = 1;
+  int BKsel = 0;  // per-product kernel
   int tune_c = -1;
   TuneEntry *te = nullptr;
   int dev = 0;
   NEDY_CUDA(cudaGetDevice(&dev));
-  {
+  if (g.force_bn > 0) {  // a given instance (the candidate checks of the test suite)
+    NEDY_REQUIRE(g.force_bn == 64 || g.force_bn == 128 || g.force_bn == 256, "split_gemm: bad forced tile width");
+    NEDY_REQUIRE(g.force_bk == 0 || g.force_bk == 32 || g.force_bk == 64, "split_gemm: bad forced K block");
+    NEDY_REQUIRE(g.force_bk == 0 || g.force_bn >= 128, "split_gemm: the one-load kernel has 128 or 256 wide tiles");
+    NEDY_REQUIRE(g.force_stages >= 2 && g.force_stages <= 4 && g.force_kdiv >= 1, "split_gemm: bad forced stages");
+    NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 64 || g.force_stages == 4, "split_gemm: 64-wide tiles use 4 stages");
+    NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
+    BNsel = g.force_bn;
+    STsel = g.force_stages;
+    KDsel = g.force_kdiv;
+    BKsel = g.force_bk;
+  } else {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (g_tune_on) {
       const TuneKey key{dev, P.np, P.nA, P.nB, g.out_pieces ? 1 : 0, g.accumulate ? 1 : 0, g.M, g.N, g.A.kpad};
       auto it = g_tune.find(key);
       if (it == g_tune.end()) {
         TuneEntry e;
-        e.cands = candidates(P.nA, P.nB, g.N, g.accumulate && g.ksplit <= 0);
+        e.cands = candidates(P.nA, P.nB, P.np, g.N, g.accumulate && g.ksplit <= 0);
         e.best.assign(e.cands.size(), 1e30);
         e.trials.assign(e.cands.size(), 0);
         e.inflight.assign(e.cands.size(), 0);
@@ -733,10 +823,15 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
         BNsel = e.cands[c].bn;
         STsel = e.cands[c].stages;
         KDsel = e.cands[c].kdiv;
+        BKsel = e.cands[c].bk;
       }
     }
   }
-  P.stage_bytes = P.nA * A_BYTES + P.nB * BNsel * BK * 2;
+  const int bkt = BKsel ? BKsel : BK;
+  P.stage_bytes = stage_bytes_for(P.nA, P.nB, P.np, BNsel, BKsel);
+  // real x complex without conjugation: one N = 2 BN product writes both parts
+  P.fuse = (BKsel && !ac && bc && !g.conjB && 2 * BNsel <= 256) ? 1 : 0;
+  P.kblocks = g.A.kpad / 64;  // 64-wide blocks while the K split is chosen
   const int ntn = (g.N + BNsel - 1) / BNsel, ntm = (g.M + BM - 1) / BM;
   // K split: bounded FP32 accumulation length, and enough CTAs for the GPU
   int ksplit = g.ksplit;
@@ -752,7 +847,9 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   }
   NEDY_REQUIRE(ksplit == 1 || (g.accumulate && !g.out_pieces), "split_gemm: K split needs an accumulating FP64 output");
   P.ksplit = ksplit;
-  P.kb_per_split = (P.kblocks + ksplit - 1) / ksplit;
+  // in units of the kernel's K block
+  P.kb_per_split = (P.kblocks + ksplit - 1) / ksplit * (64 / bkt);
+  P.kblocks *= 64 / bkt;
   NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && ntm <= 65535, "split_gemm: grid too large");
   P.out_pieces = g.out_pieces ? 1 : 0;
   P.accumulate = g.accumulate ? 1 : 0;
@@ -775,7 +872,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   P.cdiv = g.C.cdiv;
   P.bs = g.C.bs1;
   P.err = err_word();
-  const CUtensorMap ma = make_map(g.A, BM), mb = make_map(g.B, BNsel);
+  const CUtensorMap ma = make_map(g.A, BM, bkt), mb = make_map(g.B, BNsel, bkt);
   dim3 grid(ntn, ntm, g.nb * ksplit);
   cudaEvent_t ev[2] = {nullptr, nullptr};
   {
@@ -788,24 +885,34 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     }
   }
   const int stages = STsel ? STsel : BNsel == 128 ? 2 : std::min(4, SMEM_LIMIT / P.stage_bytes);
+  NEDY_REQUIRE(stages >= 2 && stages * P.stage_bytes <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
   cudaEvent_t tev[2] = {nullptr, nullptr};
   if (te) {
     NEDY_CUDA(cudaEventCreate(&tev[0]));
     NEDY_CUDA(cudaEventCreate(&tev[1]));
     NEDY_CUDA(cudaEventRecord(tev[0], s));
   }
-  if (BNsel == 64)
-    launch<64, 4>(P, ma, mb, grid, s);
-  else if (BNsel == 128 && stages >= 4)
-    launch<128, 4>(P, ma, mb, grid, s);
-  else if (BNsel == 128 && stages == 3)
-    launch<128, 3>(P, ma, mb, grid, s);
-  else if (BNsel == 128)
-    launch<128, 2>(P, ma, mb, grid, s);
-  else if (stages >= 3)
-    launch<256, 3>(P, ma, mb, grid, s);
-  else
-    launch<256, 2>(P, ma, mb, grid, s);
+  using LaunchFn = void (*)(const Params &, const CUtensorMap &, const CUtensorMap &, dim3, cudaStream_t);
+  struct Inst {
+    int bk, bn, st;
+    LaunchFn fn;
+  };
+  static const Inst insts[] = {
+      {0, 64, 4, launch<64, 4>},          {0, 128, 2, launch<128, 2>},        {0, 128, 3, launch<128, 3>},
+      {0, 128, 4, launch<128, 4>},        {0, 256, 2, launch<256, 2>},        {0, 256, 3, launch<256, 3>},
+      {32, 128, 2, launch<128, 2, 32, true>}, {32, 128, 3, launch<128, 3, 32, true>},
+      {32, 128, 4, launch<128, 4, 32, true>}, {32, 256, 2, launch<256, 2, 32, true>},
+      {32, 256, 3, launch<256, 3, 32, true>}, {64, 128, 2, launch<128, 2, 64, true>},
+      {64, 128, 3, launch<128, 3, 64, true>}};
+  int st_run = stages;
+  if (BKsel == 0) {  // per-product kernel: the instance nearest to the requested stages
+    st_run = BNsel == 64 ? 4 : BNsel == 128 ? std::min(std::max(stages, 2), 4) : std::min(std::max(stages, 2), 3);
+  }
+  LaunchFn fn = nullptr;
+  for (const Inst &x : insts)
+    if (x.bk == BKsel && x.bn == BNsel && x.st == st_run) fn = x.fn;
+  NEDY_REQUIRE(fn != nullptr, "split_gemm: no kernel instance for this tile shape");
+  fn(P, ma, mb, grid, s);
   if (te) {
     NEDY_CUDA(cudaEventRecord(tev[1], s));
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -817,6 +924,150 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_CUDA(cudaEventRecord(ev[1], s));
     g_stats_ev.push_back({ev[0], ev[1]});
   }
+}
+
+// ---- check of one kernel instance against an FP64 product on seeded operands
+namespace {
+__device__ __forceinline__ double check_uniform(unsigned long long x) {
+  // splitmix64 finaliser -> uniform in [-1, 1)
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+__global__ void check_fill_kernel(i64 n, unsigned long long seed, double *out) {
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    out[i] = check_uniform(seed * 0x100000001B3ULL + (unsigned long long)i);
+}
+// ref[b][m][n] += alpha * sum_k op(A[b][m][k]) op(B[b][n][k]); real operands have one double per element
+__global__ void check_ref_kernel(int M, int N, int K, int nb, int ac, int bc, int cA, int cB, const double *A,
+                                 const double *B, double alpha, double2 *ref) {
+  const i64 tot = (i64)nb * M * N;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < tot; idx += (i64)gridDim.x * blockDim.x) {
+    const int n = (int)(idx % N);
+    const i64 bm = idx / N;
+    const int m = (int)(bm % M), b = (int)(bm / M);
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < K; k++) {
+      const i64 ia = ((i64)b * M + m) * K + k, ib = ((i64)b * N + n) * K + k;
+      const double ar = ac ? A[2 * ia] : A[ia], ai = ac ? (cA ? -A[2 * ia + 1] : A[2 * ia + 1]) : 0.0;
+      const double br = bc ? B[2 * ib] : B[ib], bi = bc ? (cB ? -B[2 * ib + 1] : B[2 * ib + 1]) : 0.0;
+      re += ar * br - ai * bi;
+      im += ar * bi + ai * br;
+    }
+    ref[idx].x += alpha * re;
+    ref[idx].y += alpha * im;
+  }
+}
+// got[b][m][n] = sum of the BF16 pieces of the piece output (planes [comp][piece])
+__global__ void check_unpieces_kernel(int M, int N, int nb, int kpad, int np, i64 plane, const __nv_bfloat16 *cp,
+                                      double2 *got) {
+  const i64 tot = (i64)nb * M * N;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < tot; idx += (i64)gridDim.x * blockDim.x) {
+    const int n = (int)(idx % N);
+    const i64 bm = idx / N;
+    const i64 off = bm * kpad + n;
+    double v[2] = {0.0, 0.0};
+    for (int c = 0; c < 2; c++)
+      for (int p = 0; p < np; p++) v[c] += (double)__bfloat162float(cp[(i64)(c * np + p) * plane + off]);
+    got[idx] = make_double2(v[0], v[1]);
+  }
+}
+// maxima of |got - ref| and |ref| as ordered bit patterns of non-negative doubles
+__global__ void check_err_kernel(i64 n, const double2 *ref, const double2 *got, unsigned long long *mx) {
+  unsigned long long d = 0, r = 0;
+  for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const double dd = fmax(fabs(got[i].x - ref[i].x), fabs(got[i].y - ref[i].y));
+    const double rr = fmax(fabs(ref[i].x), fabs(ref[i].y));
+    d = max(d, (unsigned long long)__double_as_longlong(dd));
+    r = max(r, (unsigned long long)__double_as_longlong(rr));
+  }
+  atomicMax(&mx[0], d);
+  atomicMax(&mx[1], r);
+}
+}  // namespace
+
+double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
+  NEDY_REQUIRE(k.M > 0 && k.N > 0 && k.K > 0 && k.nb > 0 && (k.a_cplx || k.b_cplx) && k.np >= 1 && k.np <= 3,
+               "split_gemm_check: bad sizes");
+  NEDY_REQUIRE((i64)k.nb * k.M * k.N <= (1LL << 24) && (i64)k.nb * (k.M + k.N) * k.K <= (1LL << 26),
+               "split_gemm_check: sizes too large for the check");
+  std::vector<void *> held;
+  auto dalloc = [&](size_t bytes) {
+    void *p = nullptr;
+    NEDY_CUDA(cudaMalloc(&p, bytes));
+    held.push_back(p);
+    return p;
+  };
+  double result = 0.0;
+  try {
+    const int ca = k.a_cplx ? 2 : 1, cb = k.b_cplx ? 2 : 1;
+    const i64 na = (i64)k.nb * k.M * k.K * ca, nbv = (i64)k.nb * k.N * k.K * cb, nc = (i64)k.nb * k.M * k.N;
+    double *A = (double *)dalloc(sizeof(double) * na), *B = (double *)dalloc(sizeof(double) * nbv);
+    double2 *C = (double2 *)dalloc(sizeof(double2) * nc), *ref = (double2 *)dalloc(sizeof(double2) * nc);
+    check_fill_kernel<<<592, 256, 0, s>>>(na, k.seed * 3 + 1, A);
+    check_fill_kernel<<<592, 256, 0, s>>>(nbv, k.seed * 3 + 2, B);
+    if (k.accumulate)
+      check_fill_kernel<<<592, 256, 0, s>>>(2 * nc, k.seed * 3 + 3, (double *)C);
+    else
+      NEDY_CUDA(cudaMemsetAsync(C, 0, sizeof(double2) * nc, s));
+    NEDY_CUDA(cudaMemcpyAsync(ref, C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, s));
+    NEDY_CHECK_LAUNCH();
+    check_ref_kernel<<<592, 256, 0, s>>>(k.M, k.N, k.K, k.nb, k.a_cplx, k.b_cplx, k.conjA, k.conjB, A, B, k.alpha,
+                                         ref);
+    NEDY_CHECK_LAUNCH();
+    Pieces ap, bp;
+    ap.rows = k.M; ap.kpad = kpad64(k.K); ap.nb = k.nb; ap.ncomp = ca; ap.np = k.np;
+    bp.rows = k.N; bp.kpad = ap.kpad; bp.nb = k.nb; bp.ncomp = cb; bp.np = k.np;
+    ap.p = (__nv_bfloat16 *)dalloc(ap.elems() * 2);
+    bp.p = (__nv_bfloat16 *)dalloc(bp.elems() * 2);
+    View va = rowmajor(A, k.K); va.bs1 = (i64)k.M * k.K;
+    View vb = rowmajor(B, k.K); vb.bs1 = (i64)k.N * k.K;
+    split_pieces(va, k.a_cplx != 0, false, k.K, ap, s);
+    split_pieces(vb, k.b_cplx != 0, false, k.K, bp, s);
+    SplitGemmArgs g;
+    g.M = k.M; g.N = k.N; g.K = k.K; g.nb = k.nb;
+    g.A = ap; g.B = bp;
+    g.conjA = k.conjA != 0; g.conjB = k.conjB != 0;
+    g.alpha = k.alpha;
+    g.force_bn = k.bn; g.force_stages = k.stages; g.force_bk = k.bk; g.force_kdiv = k.kdiv;
+    double2 *got = C;
+    if (k.out_pieces) {
+      Pieces cp;
+      cp.rows = k.M; cp.kpad = kpad64(k.N); cp.nb = k.nb; cp.ncomp = 2; cp.np = k.np;
+      cp.p = (__nv_bfloat16 *)dalloc(cp.elems() * 2);
+      NEDY_CUDA(cudaMemsetAsync(cp.p, 0, cp.elems() * 2, s));
+      g.out_pieces = true;
+      g.Cp = cp;
+      g.C.rs_lo = cp.kpad; g.C.cs_lo = 1; g.C.bs1 = (i64)k.M * cp.kpad;
+      split_gemm(g, s);
+      check_unpieces_kernel<<<592, 256, 0, s>>>(k.M, k.N, k.nb, cp.kpad, k.np, cp.plane(), cp.p, C);
+      NEDY_CHECK_LAUNCH();
+    } else {
+      g.C = rowmajor(C, k.N); g.C.bs1 = (i64)k.M * k.N;
+      g.accumulate = k.accumulate != 0;
+      split_gemm(g, s);
+    }
+    unsigned long long *mx = (unsigned long long *)dalloc(2 * sizeof(unsigned long long));
+    NEDY_CUDA(cudaMemsetAsync(mx, 0, 2 * sizeof(unsigned long long), s));
+    check_err_kernel<<<592, 256, 0, s>>>(nc, ref, got, mx);
+    NEDY_CHECK_LAUNCH();
+    unsigned long long h[2] = {0, 0};
+    NEDY_CUDA(cudaMemcpyAsync(h, mx, sizeof(h), cudaMemcpyDeviceToHost, s));
+    NEDY_CUDA(cudaStreamSynchronize(s));
+    NEDY_REQUIRE(split_gemm_error(s) == 0, "split_gemm_check: a bounded device wait timed out");
+    double d, r;
+    memcpy(&d, &h[0], 8);
+    memcpy(&r, &h[1], 8);
+    result = d / (r > 0 ? r : 1.0);
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    for (void *p : held) cudaFree(p);
+    throw;
+  }
+  for (void *p : held) cudaFree(p);
+  return result;
 }
 
 int split_gemm_error(cudaStream_t s) {

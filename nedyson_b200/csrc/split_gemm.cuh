@@ -5,9 +5,9 @@
 // a*b is then the sum of the piece products a_i b_j with i + j < npieces (6
 // products for 3 pieces, 3 for 2), which the tensor cores form exactly and
 // accumulate in FP32 in tensor memory.  Complex operands are separate real and
-// imaginary piece planes; one output tile holds either the real or the
-// imaginary part, so a complex x complex product is 2 x npieces(npieces+1)/2
-// real BF16 GEMMs per output part.
+// imaginary piece planes; one output tile holds both parts (two TMEM
+// accumulators), so a complex x complex product is 4 real BF16 GEMMs per piece
+// product, a real x complex one 2.
 //
 // Storage of an operand ("piece planes"): BF16, [comp][piece][batch][row][kpad],
 // K contiguous and padded with zeros to kpad, a multiple of 64 (one 128-byte
@@ -48,9 +48,24 @@ struct SplitGemmArgs {
   bool accumulate = false;  // FP64 output only: C += alpha * A B^T
   int ksplit = 0;           // 0: choose; > 1 needs accumulate (FP64 atomics)
   int max_kblocks = 0;      // upper bound on 64-wide K blocks accumulated in FP32 per tile (0: none)
+  // a given kernel instance instead of the autotuner's (force_bn 0: autotuner); force_bk 0
+  // is the per-product kernel, 32 / 64 the one-load kernel with that K block
+  int force_bn = 0, force_stages = 0, force_bk = 0, force_kdiv = 1;
 };
 
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
+
+// One kernel instance (tile width bn, stages, K block bk: 0 per-product kernel, 32 / 64
+// one-load kernel; kdiv as in the autotuner) on seeded uniform operands: returns
+// max |split - FP64| / max |FP64| over the output (piece outputs summed back).
+struct SplitCheck {
+  int M = 0, N = 0, K = 0, nb = 1;
+  int a_cplx = 1, b_cplx = 1, conjA = 0, conjB = 0, np = 3, out_pieces = 0, accumulate = 0;
+  int bn = 128, stages = 2, bk = 0, kdiv = 1;
+  double alpha = 1.0;
+  unsigned long long seed = 1;
+};
+double split_gemm_check(const SplitCheck &k, cudaStream_t s);
 
 // Accounting of split kernel launches: returns the algorithmic BF16 tensor-pipe FLOPs and
 // the summed device time (ms) since the last call, then turns the accounting on or off.
