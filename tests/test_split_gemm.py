@@ -1,10 +1,11 @@
 """Every instance of the split-precision GEMM (BF16 pieces on tcgen05, FP32 accumulation)
 against an FP64 product on seeded operands, through nedy_split_gemm_check.
 
-Tolerance: max |C_split - C_fp64| <= tol * max |C_fp64| with tol = 1e-5 for three
-pieces per operand and 5e-5 for two (uniform [-1, 1) operands, K <= 2048; the pieces
-represent each operand to 2^-24 resp. 2^-17 relative and FP32 accumulation adds
-about 2^-24 sqrt(K)).  A layout or descriptor error gives O(1) errors.
+Tolerance: max |C_split - C_fp64| <= 1e-4 * max |C_fp64| (uniform [-1, 1) operands).
+The pieces represent each operand to 2^-24 (three pieces) or 2^-17 (two) relative;
+the FP32 accumulation over the K range of one tile dominates: its worst-case bound
+K 2^-24 is 6e-5 at K = 1024 (measured 4e-6 .. 1.5e-5, larger for the instances that
+split K less).  A layout or descriptor error gives O(1) errors.
 """
 import ctypes as C
 
@@ -15,7 +16,7 @@ from nedyson_b200 import _lib
 pytestmark = pytest.mark.gpu
 
 NEDY_OK, NEDY_ERR_ARG = 0, 1
-TOL = {2: 5e-5, 3: 1e-5}
+TOL = {2: 1e-4, 3: 1e-4}
 
 # (M, N, K, nb, a_cplx, b_cplx, conj_a, conj_b, out_pieces, accumulate)
 SHAPES = {
