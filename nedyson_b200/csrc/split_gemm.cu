@@ -162,6 +162,28 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 64 consecutive TMEM columns of this warp's 32 lanes (one load, one wait)
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,"
+      "%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+        "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+        "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+        "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+        "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
+}
+
 // column offsets of a 16-column chunk: one division when the chunk stays inside one cdiv
 // segment (fast), then base + j * cs_lo
 __device__ __forceinline__ bool chunk_base(const Params &P, int nf, i64 &cbase) {
@@ -248,6 +270,75 @@ __device__ __forceinline__ void store_pieces16_rows(const Params &P, __nv_bfloat
     }
     __syncwarp();
   }
+}
+
+// Staged epilogue stores.  A lane owns one output row; rows of a warp are generally far
+// apart in memory, so per-lane stores send 32 scattered requests per instruction.  These
+// helpers stage the warp's 32 rows in a warp-private shared buffer and write them back
+// so that each store instruction covers whole row segments (4 x 128 B of BF16 pieces,
+// or 2 x 256 B of FP64 complex).
+constexpr int STAGE_LD64 = 72;        // BF16 elements per staged row of 64 (padded, 144 B)
+constexpr int STAGE_LD16 = 17;        // double2 per staged row of 16 (padded, 272 B)
+constexpr int STAGE_WARP_BYTES = 32 * STAGE_LD16 * 16;  // >= 32 * STAGE_LD64 * 2
+
+// BF16 pieces of 64 contiguous columns (x: this lane's row, scaled; consumed)
+__device__ __forceinline__ void store_pieces64_staged(const Params &P, __nv_bfloat16 *o, i64 roff, int mok,
+                                                      i64 cbase, float (&x)[64], __nv_bfloat16 *sbuf, int lane) {
+  for (int p = 0; p < P.out_np; p++) {
+#pragma unroll
+    for (int j = 0; j < 64; j += 8) {
+      uint32_t w[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) {  // two values per conversion instruction
+        const __nv_bfloat162 h = __floats2bfloat162_rn(x[j + 2 * t], x[j + 2 * t + 1]);
+        const float2 f = __bfloat1622float2(h);
+        x[j + 2 * t] -= f.x;
+        x[j + 2 * t + 1] -= f.y;
+        w[t] = *(const uint32_t *)&h;
+      }
+      *(uint4 *)(sbuf + lane * STAGE_LD64 + j) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int idx = i * 32 + lane, r = idx >> 3, c8 = (idx & 7) * 8;
+      const i64 ro = __shfl_sync(0xffffffffu, roff, r);
+      const int okr = __shfl_sync(0xffffffffu, mok, r);
+      if (okr)
+        *(uint4 *)(o + (i64)p * P.plane + ro + cbase + c8) = *(const uint4 *)(sbuf + r * STAGE_LD64 + c8);
+    }
+    __syncwarp();
+  }
+}
+
+// FP64 complex outputs of 16 contiguous columns (store, accumulate or atomic add)
+__device__ __forceinline__ void store_fp64_16_staged(const Params &P, i64 roff, int mok, i64 cbase,
+                                                     const float (&vr)[16], const float (&vi)[16], double2 *sb,
+                                                     int lane) {
+#pragma unroll
+  for (int j = 0; j < 16; j++) sb[lane * STAGE_LD16 + j] = make_double2(P.alpha * (double)vr[j], P.alpha * (double)vi[j]);
+  __syncwarp();
+#pragma unroll 4
+  for (int i = 0; i < 16; i++) {
+    const int idx = i * 32 + lane, r = idx >> 4, j = idx & 15;
+    const i64 ro = __shfl_sync(0xffffffffu, roff, r);
+    const int okr = __shfl_sync(0xffffffffu, mok, r);
+    if (!okr) continue;
+    double2 *o = (double2 *)P.out + ro + cbase + j;
+    const double2 v = sb[r * STAGE_LD16 + j];
+    if (P.atomic) {
+      atomicAdd(&o->x, v.x);
+      atomicAdd(&o->y, v.y);
+    } else if (P.accumulate) {
+      double2 t = *o;
+      t.x += v.x;
+      t.y += v.y;
+      *o = t;
+    } else {
+      *o = v;
+    }
+  }
+  __syncwarp();
 }
 
 // OL = false: one stage holds one piece product of one K block (the A and B tiles of that
@@ -390,16 +481,39 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
     const i64 roff =
         (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    // piece outputs whose 32 rows of this warp are contiguous use the staged store
+    // piece outputs whose 32 rows of this warp are contiguous use the row-staged store
     const int r0 = m0 + warp * 32;
     bool rows_contig = P.out_pieces && P.rs_lo == 1 && r0 + 32 <= P.M;
     if (rows_contig && P.rdiv) rows_contig = (r0 % P.rdiv) + 32 <= P.rdiv;
     const i64 roff0 = __shfl_sync(0xffffffffu, roff, 0);
     rows_contig = rows_contig && (roff0 & 7) == 0;
-    __nv_bfloat16 *sbuf = (__nv_bfloat16 *)(smem + warp * 1024);  // stages are idle in the epilogue
+    // every row offset a multiple of 8 elements (16-byte stores of BF16 pieces)
+    const bool rows_al8 = __all_sync(0xffffffffu, (roff & 7) == 0);
+    uint8_t *wbuf = smem + warp * STAGE_WARP_BYTES;  // stages are idle in the epilogue
+    __nv_bfloat16 *sbuf = (__nv_bfloat16 *)wbuf;
+    const int imok = mok ? 1 : 0;
     if (ok) {
-      for (int c0 = 0; c0 < BN; c0 += 16) {
+      for (int c0 = 0; c0 < BN;) {
         if (n0 + c0 >= P.N) break;  // uniform across the warp
+        const int nf = n0 + c0;
+        if (P.out_pieces && !rows_contig && rows_al8 && c0 + 64 <= BN && nf + 64 <= P.N && P.cs_lo == 1 &&
+            (P.cdiv == 0 || (nf % P.cdiv) + 64 <= P.cdiv)) {
+          // 64 contiguous columns of each part, staged
+          const i64 cbase = P.cdiv ? (i64)(nf / P.cdiv) * P.cs_hi + (i64)(nf % P.cdiv) : (i64)nf;
+          if ((cbase & 7) == 0) {
+            __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
+            const float al = (float)P.alpha;
+            for (int part = 0; part < 2; part++) {
+              float x[64];
+              tmem_ld64(trow + (uint32_t)(part * BN + c0), x);
+#pragma unroll
+              for (int j = 0; j < 64; j++) x[j] = iters == 0 ? 0.f : al * x[j];
+              store_pieces64_staged(P, o + (i64)part * P.out_np * P.plane, roff, imok, cbase, x, sbuf, lane);
+            }
+            c0 += 64;
+            continue;
+          }
+        }
         float vr[16], vi[16];
         tmem_ld16(trow + (uint32_t)c0, vr);
         tmem_ld16(trow + (uint32_t)(BN + c0), vi);
@@ -407,10 +521,14 @@ __global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
 #pragma unroll
           for (int j = 0; j < 16; j++) vr[j] = vi[j] = 0.f;
         }
-        if (!mok) continue;
-        const int nf = n0 + c0;
+        c0 += 16;
         i64 cbase;
         const bool fast = chunk_base(P, nf, cbase);
+        if (!P.out_pieces && fast && P.cs_lo == 1) {  // warp-uniform
+          store_fp64_16_staged(P, roff, imok, cbase, vr, vi, (double2 *)wbuf, lane);
+          continue;
+        }
+        if (!mok) continue;
         if (P.out_pieces) {
           __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
           if (rows_contig && fast && (cbase & 7) == 0 && (P.cs_lo & 7) == 0) {
