@@ -680,19 +680,28 @@ namespace {
 std::mutex g_stats_mu;
 bool g_stats_on = false;
 double g_stats_flops = 0.0;
-std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_stats_ev;
+struct StatEv {
+  cudaEvent_t e0, e1;
+  std::string cls;  // problem class of the launch
+};
+std::vector<StatEv> g_stats_ev;
+std::map<std::string, std::pair<int, double>> g_class_ms;  // last window: launches, ms per class
 }  // namespace
 
 void split_stats(bool on, double *flops, double *ms) {
   std::lock_guard<std::mutex> lk(g_stats_mu);
   double t = 0.0;
+  if (!g_stats_ev.empty()) g_class_ms.clear();
   for (auto &e : g_stats_ev) {
-    NEDY_CUDA(cudaEventSynchronize(e.second));
+    NEDY_CUDA(cudaEventSynchronize(e.e1));
     float x = 0.f;
-    NEDY_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
+    NEDY_CUDA(cudaEventElapsedTime(&x, e.e0, e.e1));
     t += x;
-    cudaEventDestroy(e.first);
-    cudaEventDestroy(e.second);
+    auto &c = g_class_ms[e.cls];
+    c.first++;
+    c.second += x;
+    cudaEventDestroy(e.e0);
+    cudaEventDestroy(e.e1);
   }
   g_stats_ev.clear();
   if (flops) *flops = g_stats_flops;
@@ -826,8 +835,17 @@ void split_autotune(bool on) {
 }
 
 std::string split_tune_report() {
-  std::lock_guard<std::mutex> lk(g_tune_mu);
   std::string r;
+  {
+    std::lock_guard<std::mutex> lk(g_stats_mu);
+    for (auto &kv : g_class_ms) {
+      char buf[160];
+      snprintf(buf, sizeof(buf), "time %s: %d launches %.2f ms;", kv.first.c_str(), kv.second.first,
+               kv.second.second);
+      r += buf;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
   for (auto &kv : g_tune) {
     TuneEntry &e = kv.second;
     poll(e);
@@ -1040,7 +1058,10 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   if (ev[0]) {
     std::lock_guard<std::mutex> lk(g_stats_mu);
     NEDY_CUDA(cudaEventRecord(ev[1], s));
-    g_stats_ev.push_back({ev[0], ev[1]});
+    char cls[96];
+    snprintf(cls, sizeof(cls), "M=%d N=%d K=%d %s %s np=%d", g.M, g.N, g.A.kpad,
+             P.nA == 2 ? (P.nB == 2 ? "cxc" : "cxr") : "rxc", g.out_pieces ? "pieces" : "fp64", P.np);
+    g_stats_ev.push_back({ev[0], ev[1], cls});
   }
 }
 
