@@ -65,7 +65,7 @@ typedef struct {
   int nt, ntau, nao, k;
   double beta, dt;
   int device;                 /* CUDA device ordinal */
-  long long workspace_bytes;  /* self-energy chunk budget; 0 = default (4 GiB) */
+  long long workspace_bytes;  /* self-energy chunk budget; 0 = default (8 GiB) */
 } nedy_config;
 
 int nedy_abi_version(void);

@@ -69,7 +69,7 @@ struct Ctx {
   int nt = 0, ntau = 0, nao = 0, k = 5;
   double beta = 1.0, dt = 0.01;
   Arena ws;
-  i64 ws_budget = 4LL << 30;  // bytes the self-energy may use for chunk intermediates
+  i64 ws_budget = 8LL << 30;  // bytes the self-energy may use for chunk intermediates
   std::vector<std::pair<int *, int>> pending_status;  // device status words of batched solves
   // Gregory weights w(n, j) for n, j <= nt (row-major and transposed), small tables
   double *greg = nullptr, *gregT = nullptr;

@@ -470,6 +470,39 @@ static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
   sub = (int)std::max<i64>(1, std::min<i64>(16, (budget / 3) / n4));
   chunk = (int)std::max<i64>(1, std::min<i64>(64, (budget - sub * n4) / std::max<i64>(per, 1)));
   if (chunk < sub) sub = chunk;
+  if (!split || !c.V_sym) return;
+  // all-split chain (les-form units only): the intermediates are BF16 pieces
+  const i64 np = c.precision == NEDY_PREC_SPLIT_BF16X2 ? 2 : 3, pb = 4 * np;  // bytes per complex element
+  const i64 es = N * N, kpN = kpad64((int)es), kpA = kpad64((int)A), kpNA = kpad64((int)(N * A));
+  const i64 unit = pb * (es * kpN + es * kpA + N * kpNA) + n2a;  // S', MT and Q pieces, Q (FP64)
+  per = 6 * pb * A * kpN + n2a + A * A * 16 + 8 * es * 16;
+  const int sub_max = (int)std::max<i64>(1, std::min<i64>(48, (budget / 2) / unit));
+  // units per exchange launch: the Q contraction has ceil(nao^2 / 128) row tiles per unit;
+  // take the largest count whose tiles fill at least 95% of their last wave of CTAs (one
+  // per SM), else the best filled one
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const i64 tiles = (es + 127) / 128;
+  int pick = 0;
+  double best = -1.0;
+  int best_u = 1;
+  for (int u = sub_max; u >= 1; u--) {
+    const double w = (double)(tiles * u) / std::max(1, sms), eff = w / std::ceil(w);
+    if (eff >= 0.95) {
+      pick = u;
+      break;
+    }
+    if (eff > best) {
+      best = eff;
+      best_u = u;
+    }
+  }
+  sub = pick ? pick : best_u;
+  chunk = (int)std::max<i64>(1, std::min<i64>(64, (budget - sub * unit) / std::max<i64>(per, 1)));
+  if (chunk >= sub)
+    chunk -= chunk % sub;
+  else
+    sub = chunk;
 }
 
 void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G) {
@@ -568,7 +601,7 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
         }
         // exchange per spin
         double2 *Q = c.ws.alloc<double2>(nsl * N2A);
-        double2 *S = c.ws.alloc<double2>((i64)sub * es * es);
+        void *S = c.ws.get(DF::arr_bytes((int)es, (int)es, sub, np));
         void *vyp = c.ws.get(vyk);
         void *Mb = c.ws.get(DF::arr_bytes((int)es, A, sub, np));
         void *Qb = c.ws.get(DF::arr_bytes(N, (int)NA, sub, np));
