@@ -87,6 +87,8 @@ def parse():
                     help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
+    ap.add_argument("--workspace-gb", type=float, default=0.0,
+                    help="self-energy chunk workspace in GiB (0: the library default); small for profiling runs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="fixed split GEMM tiles (profiling runs: the tuner's timings are meaningless under ncu)")
     ap.add_argument("--beta", type=float, default=20.0)
@@ -305,7 +307,8 @@ def run_engine(args, dist: Dist):
     else:
         F, mu = hf_equilibrium(p, args.beta)
         Fs, mus = (F,), (mu,)
-    ctx = api.Context(nt, ntau, N, 5, args.beta, args.dt, device=dev)
+    ctx = api.Context(nt, ntau, N, 5, args.beta, args.dt, device=dev,
+                      workspace_bytes=int(args.workspace_gb * (1 << 30)))
     x, _ = ctx.collocation()
     G = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]
     S = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]

@@ -909,13 +909,19 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     P.mma[0] = Mma{0, 0, 0, 0};
     P.mma[1] = Mma{0, 1, 1, cB};  // negating A negates the product
   }
-  // instance: outputs at most 64 wide use 64-wide tiles; piece outputs 128-wide tiles (two
-  // CTAs per SM overlap one CTA's store-heavy epilogue with the other's main loop); FP64
-  // outputs 256-wide tiles, as many stages as fit
+  // instance without the autotuner: outputs at most 64 wide use 64-wide tiles; piece
+  // outputs 128-wide tiles (two CTAs per SM overlap one CTA's store-heavy epilogue with
+  // the other's main loop); FP64 outputs 256-wide tiles; wider tiles take the one-load
+  // kernel with 32-wide K blocks and two stages when those fit (the usual choice of the
+  // autotuner), else the per-product kernel with as many stages as fit
   int BNsel = g.N <= 64 ? 64 : g.out_pieces ? 128 : 256;
   int STsel = 0;  // 0: as many stages as fit
   int KDsel = 1;
   int BKsel = 0;  // per-product kernel
+  if (BNsel >= 128 && 2 * stage_bytes_for(P.nA, P.nB, P.np, BNsel, 32) <= SMEM_LIMIT) {
+    BKsel = 32;
+    STsel = 2;
+  }
   int tune_c = -1;
   TuneEntry *te = nullptr;
   int dev = 0;
