@@ -101,18 +101,27 @@ def parse():
 
 # ------------------------------------------------------------------ distributed
 class Dist:
-    def __init__(self, n):
+    """One process per GPU (replicas: no data-path collective).  The process group carries
+    only the barriers around the timed region and the max over ranks of the device time;
+    NCCL on GPUs, gloo where no GPU is visible (the CPU tests of this logic)."""
+
+    def __init__(self, n, backend=None, timeout_s=600):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = None
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
             self.pg = dist
+            self.backend = backend
 
     def barrier(self):
         if self.pg:
@@ -122,13 +131,25 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def replica_value(steps_per_rank: int, world: int, max_secs: float) -> float:
+    """Whole-job time steps per second: every rank runs its own trajectory (weak scaling),
+    timed by the slowest rank."""
+    return steps_per_rank * world / max_secs
+
+
+def rank_seed(seed: int, rank: int) -> int:
+    """Seed of a rank's inputs: each replica runs an independent molecule."""
+    return seed + rank
 
 
 # ------------------------------------------------------------------ clocks
@@ -303,7 +324,7 @@ def run_engine(args, dist: Dist):
     ns = 2 if spin else 1
     t_first = args.t0
     nt = t_first + W + K
-    p = make_problem(N, A, args.seed + dist.rank, spin=spin)
+    p = make_problem(N, A, rank_seed(args.seed, dist.rank), spin=spin)
     if spin:
         Fs, mus = uhf_equilibrium(p, args.beta)
     else:
@@ -592,10 +613,9 @@ def main():
 
     fp64 = fp64_gemm_peak(dist.local) if dist.rank == 0 else None
     r = run_engine(args, dist)
-    total_steps = K * dist.world
     sp, pl = r["split"], r["plain"]
-    value = total_steps / sp["secs"]
-    plain_value = total_steps / pl["secs"] if pl else None
+    value = replica_value(K, dist.world, sp["secs"])
+    plain_value = replica_value(K, dist.world, pl["secs"]) if pl else None
     T_mid = r["T"][len(r["T"]) // 2]
     peaks, src = measured_peaks()
     cfg["precision"] = ({"bf16x2": "split self-energy, two BF16 pieces per operand, products hi*hi + hi*lo + lo*hi",
