@@ -350,7 +350,7 @@ __device__ __forceinline__ void store_fp64_16_staged(const Params &P, i64 roff, 
 //   tiles of one piece are adjacent: for real x complex products one MMA with N = 2 BN
 //   writes both parts (TMEM columns [0, BN) real, [BN, 2 BN) imaginary).
 template <int BN, int STAGES, int BKT, bool OL>
-__global__ void __launch_bounds__(THREADS, BN == 128 ? 2 : 1)
+__global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 2)) ? 2 : 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ Params P) {
   static_assert(OL || BKT == BK, "the per-product kernel uses 64-wide K blocks");
@@ -768,6 +768,7 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
   std::vector<Cand> c;
   if (N <= 64 && acc) {  // one output tile per batch: the K split is what there is to tune
     for (int kd : {1, 2, 4, 8}) c.push_back({64, 4, kd, 0});
+    for (int kd : {1, 2}) c.push_back({64, 2, kd, 0});  // two CTAs per SM
     return c;
   }
   for (int bn : {64, 128, 256}) {
@@ -778,6 +779,7 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
     if (st < 2) continue;
     if (bn == 64) {
       if (st >= 4) c.push_back({64, 4, 1, 0});
+      c.push_back({64, 2, 1, 0});  // two CTAs per SM: one's epilogue beside the other's main loop
     } else if (bn == 128) {
       c.push_back({128, 2, 1, 0});
       if (st >= 3) c.push_back({128, std::min(st, 4), 1, 0});
@@ -931,7 +933,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_REQUIRE(g.force_bk == 0 || g.force_bk == 32 || g.force_bk == 64, "split_gemm: bad forced K block");
     NEDY_REQUIRE(g.force_bk == 0 || g.force_bn >= 128, "split_gemm: the one-load kernel has 128 or 256 wide tiles");
     NEDY_REQUIRE(g.force_stages >= 2 && g.force_stages <= 4 && g.force_kdiv >= 1, "split_gemm: bad forced stages");
-    NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 64 || g.force_stages == 4, "split_gemm: 64-wide tiles use 4 stages");
+    NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 64 || g.force_stages == 4 || g.force_stages == 2,
+                 "split_gemm: 64-wide tiles use 2 or 4 stages");
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
     BNsel = g.force_bn;
     STsel = g.force_stages;
@@ -1040,7 +1043,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     LaunchFn fn;
   };
   static const Inst insts[] = {
-      {0, 64, 4, launch<64, 4>},          {0, 128, 2, launch<128, 2>},        {0, 128, 3, launch<128, 3>},
+      {0, 64, 4, launch<64, 4>},          {0, 64, 2, launch<64, 2>},          {0, 128, 2, launch<128, 2>},        {0, 128, 3, launch<128, 3>},
       {0, 128, 4, launch<128, 4>},        {0, 256, 2, launch<256, 2>},        {0, 256, 3, launch<256, 3>},
       {32, 128, 2, launch<128, 2, 32, true>}, {32, 128, 3, launch<128, 3, 32, true>},
       {32, 128, 4, launch<128, 4, 32, true>}, {32, 256, 2, launch<256, 2, 32, true>},
@@ -1048,7 +1051,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       {64, 128, 3, launch<128, 3, 64, true>}};
   int st_run = stages;
   if (BKsel == 0) {  // per-product kernel: the instance nearest to the requested stages
-    st_run = BNsel == 64 ? 4 : BNsel == 128 ? std::min(std::max(stages, 2), 4) : std::min(std::max(stages, 2), 3);
+    st_run = BNsel == 64 ? (stages <= 2 ? 2 : 4)
+                         : BNsel == 128 ? std::min(std::max(stages, 2), 4) : std::min(std::max(stages, 2), 3);
   }
   LaunchFn fn = nullptr;
   for (const Inst &x : insts)

@@ -27,7 +27,7 @@ SHAPES = {
     "cxc_n64_acc": (64, 64, 2048, 3, 1, 1, 0, 1, 0, 1),    # one 64-wide tile per batch
 }
 # (tile_n, stages, k_block, kdiv); k_block 0: per-product kernel, 32 / 64: one-load kernel
-INSTANCES = [(64, 4, 0, 1), (64, 4, 0, 2), (64, 4, 0, 4), (128, 2, 0, 1), (128, 3, 0, 1), (128, 4, 0, 1),
+INSTANCES = [(64, 4, 0, 1), (64, 4, 0, 2), (64, 4, 0, 4), (64, 2, 0, 1), (64, 2, 0, 2), (128, 2, 0, 1), (128, 3, 0, 1), (128, 4, 0, 1),
              (256, 2, 0, 1), (256, 3, 0, 1), (256, 2, 0, 2), (128, 2, 32, 1), (128, 3, 32, 1), (128, 4, 32, 1),
              (256, 2, 32, 1), (256, 3, 32, 1), (256, 2, 32, 2), (128, 2, 64, 1), (128, 3, 64, 1)]
 
