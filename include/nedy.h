@@ -95,6 +95,13 @@ int nedy_split_stats(int on, double *pipe_flops, double *ms);
  * computes the same result.  The report lists classes, candidate times and choices. */
 int nedy_split_autotune(int on);
 int nedy_split_tune_report(char *buf, int len);
+/* Work partition of the density-fitted self-energy for a workspace budget (bytes):
+ * *chunk slices per chunk and *sub exchange units per launch, as the solver chooses them
+ * (planning helper, no reference counterpart; host arithmetic, no device access).
+ * precision: nedy_precision; real_symmetric: every B^Q real symmetric; sms: streaming
+ * multiprocessors of the device (148 on a B200). */
+int nedy_sigma_chunk_plan(int nao, int naux, long long budget, int precision, int real_symmetric, int sms, int *chunk,
+                          int *sub);
 /* Check of one split GEMM kernel instance (test hook, no reference counterpart):
  * C (nb x M x N) = 0.75 * op(A) op(B)^T (+ C when accumulate) on seeded uniform operands
  * (complex when *_cplx, conjugated when conj_*), split into npieces BF16 pieces, with the

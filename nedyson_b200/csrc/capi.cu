@@ -315,6 +315,19 @@ int nedy_split_tune_report(char *buf, int len) {
   });
 }
 
+int nedy_sigma_chunk_plan(int nao, int naux, long long budget, int precision, int real_symmetric, int sms, int *chunk,
+                          int *sub) {
+  return guard([&] {
+    NEDY_REQUIRE(chunk && sub, "null argument");
+    NEDY_REQUIRE(nao > 0 && naux > 0 && budget > 0 && sms > 0, "bad sizes");
+    NEDY_REQUIRE(precision == NEDY_PREC_FP64 || precision == NEDY_PREC_SPLIT_BF16X3 ||
+                     precision == NEDY_PREC_SPLIT_BF16X2,
+                 "unknown precision mode");
+    chunk_plan(nao, naux, budget, precision != NEDY_PREC_FP64, real_symmetric != 0,
+               precision == NEDY_PREC_SPLIT_BF16X2 ? 2 : 3, sms, *chunk, *sub);
+  });
+}
+
 int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, int b_cplx, int conj_a, int conj_b,
                           int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,
                           unsigned long long seed, double *rel_err) {

@@ -6,6 +6,10 @@ namespace nedy {
 
 // molGF2SolverDecomp::solve (nspin = 1) / molGF2SolverSpinDecomp::solve (nspin = 2)
 void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G);
+// Slices per chunk and exchange units per launch of sigma_df for a workspace budget
+// (bytes); vsym: real symmetric B^Q (the all-split chain when split); np_pieces: BF16
+// pieces per operand; sms: streaming multiprocessors of the device.
+void chunk_plan(i64 N, i64 A, i64 budget, bool split, bool vsym, int np_pieces, int sms, int &chunk, int &sub);
 // molGF2Solver::solve (full U_ijkl, restricted)
 void sigma_full(Ctx &c, int T, DevGF &Sig, const DevGF &G);
 

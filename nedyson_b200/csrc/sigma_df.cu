@@ -458,21 +458,20 @@ void prep(Ctx &c, int mode, int nsl, const double2 *L0, i64 Ls, const double2 *R
 
 } // namespace
 
-// Chunk sizes: slices per chunk and exchange units per S buffer, from the workspace budget.
-static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
-  i64 N = c.df_nao, A = c.df_naux;
+// Chunk sizes: slices per chunk and exchange units per S buffer, from the workspace budget
+// (host arithmetic only; sms = streaming multiprocessors of the device).
+void chunk_plan(i64 N, i64 A, i64 budget, bool split, bool vsym, int np_pieces, int sms, int &chunk, int &sub) {
   i64 n2a = N * N * A * 16;  // bytes of one [n][a][q] intermediate
   i64 n4 = N * N * N * N * 16;
-  i64 budget = c.ws_budget;
   // per slice (retarded, the largest): 5 VZ/VYt + 3 VY + 2 M + Q + 2 P/W + prep
   i64 per = 13 * n2a + 2 * A * A * 16;
   if (split) per += 6 * n2a;  // BF16 pieces of the operands (12 bytes per complex element each)
   sub = (int)std::max<i64>(1, std::min<i64>(16, (budget / 3) / n4));
   chunk = (int)std::max<i64>(1, std::min<i64>(64, (budget - sub * n4) / std::max<i64>(per, 1)));
   if (chunk < sub) sub = chunk;
-  if (!split || !c.V_sym) return;
+  if (!split || !vsym) return;
   // all-split chain (les-form units only): the intermediates are BF16 pieces
-  const i64 np = c.precision == NEDY_PREC_SPLIT_BF16X2 ? 2 : 3, pb = 4 * np;  // bytes per complex element
+  const i64 np = np_pieces, pb = 4 * np;  // bytes per complex element
   const i64 es = N * N, kpN = kpad64((int)es), kpA = kpad64((int)A), kpNA = kpad64((int)(N * A));
   const i64 unit = pb * (es * kpN + es * kpA + N * kpNA) + n2a;  // S', MT and Q pieces, Q (FP64)
   per = 6 * pb * A * kpN + n2a + A * A * 16 + 8 * es * 16;
@@ -480,8 +479,6 @@ static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
   // units per exchange launch: the Q contraction has ceil(nao^2 / 128) row tiles per unit;
   // take the largest count whose tiles fill at least 95% of their last wave of CTAs (one
   // per SM), else the best filled one
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const i64 tiles = (es + 127) / 128;
   int pick = 0;
   double best = -1.0;
@@ -503,6 +500,14 @@ static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
     chunk -= chunk % sub;
   else
     sub = chunk;
+}
+
+static void chunking(const Ctx &c, int &chunk, int &sub, bool split) {
+  int dev = 0, sms = 148;
+  if (split && c.V_sym && cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  chunk_plan(c.df_nao, c.df_naux, c.ws_budget, split, c.V_sym, c.precision == NEDY_PREC_SPLIT_BF16X2 ? 2 : 3, sms,
+             chunk, sub);
 }
 
 void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G) {
