@@ -54,3 +54,19 @@ def test_null_arguments_are_rejected_not_crashing(libpath):
     assert L.nedy_ctx_create(None, None) == 1  # NEDY_ERR_ARG
     assert b"null" in L.nedy_last_error()
     assert L.nedy_gf_destroy(None) == 0
+
+
+def test_step_entry_points_reject_null_handles(libpath):
+    """The whole-step entry points check their handles before touching a device."""
+    import ctypes as C
+    from nedyson_b200 import _lib
+    L = _lib.lib()
+    it = C.c_int()
+    e = C.c_double()
+    assert L.nedy_decomp_tstp_tol(None, 6, None, None, None, None, 0.0, 5, 1e-8, C.byref(it), None) == 1
+    assert L.nedy_decomp_spin_tstp_tol(None, 6, None, None, None, None, None, None, None, None, 0.0, 0.0, 5, 1e-8,
+                                       C.byref(it), None) == 1
+    assert b"null" in L.nedy_last_error()
+    assert L.nedy_decomp_spin_tstp(None, 6, None, None, None, None, None, None, None, None, 0.0, 0.0, 5,
+                                   C.byref(e)) == 1
+    assert L.nedy_ctx_set_precision(None, 2) == 1
