@@ -239,14 +239,18 @@ int nedy_predictor_loss_grad(nedy_predictor *p, const float *x, const float *t, 
 /* the prediction of row tstp alone: dyson::Extrapolate, plus the learned correction of
  * the context's predictor when learned != 0 */
 int nedy_predict(nedy_ctx *ctx, int tstp, nedy_gf *G, int learned);
-/* use p in nedy_decomp_tstp_tol of ctx (NULL: polynomial extrapolation only) */
+/* use p in nedy_decomp_tstp_tol / nedy_decomp_spin_tstp_tol of ctx (NULL: polynomial
+ * extrapolation only) */
 int nedy_ctx_set_predictor(nedy_ctx *ctx, nedy_predictor *p);
 /* active: learned predictor in use; judged / better: steps judged and won by it;
  * last2: the last judged max changes from the learned and from the polynomial prediction */
 int nedy_ctx_predictor_stats(const nedy_ctx *ctx, int *active, long long *judged, long long *better, double *last2);
 
-/* The unrestricted step with the residual exit (the change is the max over both spins);
- * both G rows get the learned correction when a predictor is set. */
+/* DecompSpinSimulation::do_tstp (src/molNEsim_decomp_spin_impl.h:86-108) with the residual
+ * exit of nedy_decomp_tstp_tol in place of the fixed CorrSteps loop: the change d_k is the
+ * max over both spins' new rows; h_t_up / h_t_dn are the one-body Hamiltonians of each spin
+ * at tstp (the reference uses one hcore for both), mu_up / mu_dn the chemical potentials.
+ * Both G rows get the learned correction when a predictor is set (use in context). */
 int nedy_decomp_spin_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
                               nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
                               double mu_up, double mu_dn, int max_corr, double tol, int *iters, double *err_hist);
