@@ -113,6 +113,12 @@ int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, i
                           int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,
                           unsigned long long seed, double *rel_err);
 int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
+/* Test hook of the bounded device waits (no reference counterpart): presets the error
+ * word of the context's split-precision GEMMs as a wait that gave up would set it
+ * (code != 0).  The CTAs of the next split launches then skip their work and the call
+ * that launched them returns NEDY_ERR_TIMEOUT; reporting clears the word, so the call
+ * after that runs normally.  Lets a test drive the timeout path without a device fault. */
+int nedy_ctx_inject_split_error(nedy_ctx *ctx, int code);
 /* Number of engine kernel launches issued by this process so far. */
 unsigned long long nedy_launch_count(void);
 /* Collocation nodes x_m in [-1,1] and weights (ntau+1 values each). */
@@ -176,9 +182,10 @@ int nedy_hf_full(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
  * naux=256 fits); larger sizes are rejected with NEDY_ERR_ARG.
  * The first call on a device looks up that array's device address (set-up);
  * make that first call before any stream capture starts.  All calls on a device
- * share the array: calls that overlap on the GPU (other host threads, other
- * contexts on the same device) race.  Returns after the context's stream has
- * finished the update, like nedy_hf_decomp. */
+ * share the array and find the previous call's values in it (nothing there is
+ * read before it is written): calls that overlap on the GPU (other host threads,
+ * other contexts on the same device) race.  Each call synchronises the context's
+ * stream and returns after the update has finished, like nedy_hf_decomp. */
 #define NEDY_NOALLOC_SCRATCH_BYTES (24LL << 20)
 int nedy_hf_decomp_noalloc(nedy_ctx *ctx, int tstp, nedy_buf *hmf, const nedy_buf *rho);
 
@@ -201,6 +208,14 @@ int nedy_energy_conv(nedy_ctx *ctx, int tstp, const nedy_gf *Sigma, const nedy_g
  * err: residual of the last dyson_step (sum of the three components). */
 int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
                      double mu, int corr_steps, double *err);
+/* One whole time step of the full-U simulation (Simulation::do_tstp,
+ * src/molNEsim_impl.h:89-124): predictor, then corr_steps x [rho, hmf(tstp) = h_t +
+ * HF(rho) with U (molHFSolver::solve_HF), the GF2 self-energy row with U and Uexch
+ * (molGF2Solver::solve), dyson_step].  nedy_set_full_tensor must have been called.
+ * h_t: nao x nao complex one-body Hamiltonian at tstp (h0 plus the drive, which the
+ * reference adds through Ed_contractions, :56-61).  err: residual of the last dyson_step. */
+int nedy_full_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *Sigma, nedy_buf *hmf, const nedy_buf *h_t,
+                   double mu, int corr_steps, double *err);
 /* The same step with a residual exit (the reference always runs CorrSteps iterations;
  * the exit is the engine's addition).  After iteration k the change d_k = max |G_k - G_{k-1}|
  * over the new row (les column, ret row, tv row) is measured; the iterations stop once

@@ -43,6 +43,7 @@ SIGNATURES = {
     "nedy_ctx_stream": ([_P, _PP], _I),
     "nedy_ctx_set_timing": ([_P, _I], _I),
     "nedy_ctx_phase_times": ([_P, _DP], _I),
+    "nedy_ctx_inject_split_error": ([_P, _I], _I),
     "nedy_launch_count": ([], C.c_ulonglong),
     "nedy_gf_create": ([_P, _I, _I, _I, _I, _PP], _I),
     "nedy_gf_destroy": ([_P], _I),
@@ -92,6 +93,7 @@ SIGNATURES = {
     "nedy_dyson_start": ([_P, _P, _P, _P, _D, _DP], _I),
     "nedy_energy_conv": ([_P, _I, _P, _P, _DP], _I),
     "nedy_decomp_tstp": ([_P, _I, _P, _P, _P, _P, _D, _I, _DP], _I),
+    "nedy_full_tstp": ([_P, _I, _P, _P, _P, _P, _D, _I, _DP], _I),
     "nedy_decomp_spin_tstp": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I, _DP], _I),
 }
 

@@ -365,6 +365,14 @@ int nedy_ctx_set_timing(nedy_ctx *ctx, int on) {
   });
 }
 
+int nedy_ctx_inject_split_error(nedy_ctx *ctx, int code) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && code != 0, "null context or zero code");
+    set_dev(ctx);
+    split_gemm_set_error(ctx->c.stream, code);
+  });
+}
+
 int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4) {
   return guard([&] {
     NEDY_REQUIRE(ctx && ms4, "null argument");
@@ -742,6 +750,42 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
       const DevGF *Gs[1] = {&G->g};
       pt.mark(2);
       sigma_df(c, tstp, 1, Ss, Gs);
+      pt.mark(3);
+      dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
+    }
+    pt.mark(-1);
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+    pt.collect();
+    if (err) *err = e[0] + e[1] + e[2];
+  });
+}
+
+int nedy_full_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const nedy_buf *h_t, double mu,
+                   int corr_steps, double *err) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && G && S && hmf && h_t, "null argument");
+    NEDY_REQUIRE(corr_steps >= 1, "corr_steps must be >= 1");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    NEDY_REQUIRE(c.U && c.u_nao == G->g.nao, "nedy_full_tstp: full U tensor not set for this nao");
+    const int N = G->g.nao;
+    const i64 es = (i64)N * N;
+    NEDY_REQUIRE(h_t->bytes >= es * 16, "h_t buffer too small");
+    double2 *hT = hmf_row(hmf, ctx, tstp, N);
+    hmf_row(hmf, ctx, G->g.nt, N);
+    PhaseTimer pt(c);
+    pt.mark(0);
+    extrapolate(c, tstp, G->g);
+    double e[3] = {0, 0, 0};
+    for (int it = 0; it < corr_steps; it++) {
+      c.ws.reset();
+      pt.mark(1);
+      double2 *rho = c.ws.alloc<double2>(es);
+      get_dm(c, G->g, tstp, rho);
+      NEDY_CUDA(cudaMemcpyAsync(hT, h_t->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      hf_full(c, hT, rho);
+      pt.mark(2);
+      sigma_full(c, tstp, S->g, G->g);
       pt.mark(3);
       dyson_step(c, tstp, G->g, S->g, (const double2 *)hmf->p, mu, e);
     }

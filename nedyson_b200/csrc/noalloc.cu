@@ -66,8 +66,9 @@ extern "C" int nedy_hf_decomp_noalloc(nedy_ctx *ctx, int tstp, nedy_buf *hmf, co
     double2 *T1 = (double2 *)(base + xa_bytes);
     double2 *h = (double2 *)hmf->p + (i64)tstp * es;
     const double2 *r = (const double2 *)rho->p;
-    // the array holds the previous call's values: start this one from zeros
-    NEDY_CUDA(cudaMemsetAsync(base, 0, (size_t)need, c.stream));
+    // The array holds the previous call's values.  Nothing below reads them: Xa and T1 are
+    // written by GEMMs with beta = 0, which never read C (a K-split launch first stores
+    // exact zeros and then accumulates), so no clearing is needed.
     {  // Xa = rho_flat (1 x N^2) * Vija (N^2 x A)
       GemmArgs g;
       g.M = 1; g.N = A; g.K = (int)es;

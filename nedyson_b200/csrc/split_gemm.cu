@@ -97,6 +97,19 @@ __device__ bool mbar_wait(uint32_t a, uint32_t parity, int *err, int code) {
     }
   }
 }
+// Wait for asynchronous work this CTA issued itself (TMA loads, MMAs) before it releases
+// shared or tensor memory: an error reported elsewhere does not end it, only the time limit.
+__device__ bool mbar_wait_drain(uint32_t a, uint32_t parity, int *err, int code) {
+  if (mbar_try(a, parity)) return true;
+  const unsigned long long t0 = gtime();
+  for (unsigned it = 1;; it++) {
+    if (mbar_try(a, parity)) return true;
+    if ((it & 255) == 0 && gtime() - t0 > WAIT_NS) {
+      atomicCAS(err, 0, code);
+      return false;
+    }
+  }
+}
 
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t mbar, int x, int y, int z) {
   asm volatile(
@@ -398,12 +411,14 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
     // ---- TMA producer
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    int issued = 0;
     for (int it = 0; it < iters; it++) {
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
       if (it >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) break;
       const uint32_t base = smem_u32(smem + s * P.stage_bytes);
       mbar_expect_tx(full0 + 8 * s, P.stage_bytes);
+      issued = it + 1;
       const int ab = P.a_nb > 1 ? P.a_b0 + b : 0, bb = P.b_nb > 1 ? P.b_b0 + b : 0;
       if (OL) {
         const int kb = kb0 + it;
@@ -426,6 +441,12 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
                       (P.b_comp[j] * P.np + P.pb[pr]) * P.b_nb + bb);
       }
     }
+    // The loads of the last STAGES issued stages may still be in flight (the MMA warp may
+    // have given up before consuming them): wait until each has landed, so that no TMA
+    // write reaches this CTA's shared memory after it exits.  Earlier stages were
+    // consumed, which their empty barriers showed.
+    for (int j = max(0, issued - STAGES); j < issued; j++)
+      mbar_wait_drain(full0 + 8 * (j % STAGES), (uint32_t)(j / STAGES) & 1u, P.err, 4);
   } else if (warp == 5 && lane == 0) {
     // ---- MMA issuer
     bool started0 = false, started1 = false;  // accumulator written once (then accumulate)
@@ -471,8 +492,11 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
   } else if (warp < 4) {
     // ---- epilogue
     // lane 0 waits and tells the warp, so the .sync.aligned TMEM loads stay convergent
+    // `done` tracks every MMA the issuer started, also when it gave up early, so this
+    // wait ends once they have finished and TMEM can be read and released.  Accumulators
+    // of a CTA whose producer or issuer gave up are incomplete: nothing is stored then.
     int okl = 0;
-    if (lane == 0) okl = mbar_wait(done, 0, P.err, 3) ? 1 : 0;
+    if (lane == 0) okl = (mbar_wait_drain(done, 0, P.err, 3) && *(volatile int *)P.err == 0) ? 1 : 0;
     __syncwarp();
     const bool ok = __shfl_sync(0xffffffffu, okl, 0) != 0 && !skip;
     tc_fence_after();
@@ -638,19 +662,22 @@ CUtensorMap make_map(const Pieces &x, int box_rows, int bk) {
   return m;
 }
 
-// per-device error word
-int *err_word() {
-  static int *w[64] = {nullptr};
+// Error word of the split kernels launched on one stream (one per engine context), so
+// that a wait that gives up in one context does not stop the work of another.  The word
+// is cleared when split_gemm_error reports it.
+int *err_word(cudaStream_t s) {
+  static std::map<std::pair<int, cudaStream_t>, int *> words;
   static std::mutex mu;
   int dev = 0;
   NEDY_CUDA(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
-  NEDY_REQUIRE(dev < 64, "device index out of range");
-  if (!w[dev]) {
-    NEDY_CUDA(cudaMalloc(&w[dev], sizeof(int)));
-    NEDY_CUDA(cudaMemset(w[dev], 0, sizeof(int)));
+  int *&w = words[{dev, s}];
+  if (!w) {
+    NEDY_CUDA(cudaMalloc(&w, sizeof(int)));
+    NEDY_CUDA(cudaMemsetAsync(w, 0, sizeof(int), s));
+    NEDY_CUDA(cudaStreamSynchronize(s));
   }
-  return w[dev];
+  return w;
 }
 
 void products(int np, int (&pa)[6], int (&pb)[6], int &n) {
@@ -1016,7 +1043,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   P.cs_lo = g.C.cs_lo;
   P.cdiv = g.C.cdiv;
   P.bs = g.C.bs1;
-  P.err = err_word();
+  P.err = err_word(s);
   const CUtensorMap ma = make_map(g.A, BM, bkt), mb = make_map(g.B, BNsel, bkt);
   dim3 grid(ntn, ntm, g.nb * ksplit);
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -1220,11 +1247,21 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
 }
 
 int split_gemm_error(cudaStream_t s) {
-  int *w = err_word();
+  int *w = err_word(s);
   int h = 0;
   NEDY_CUDA(cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, s));
   NEDY_CUDA(cudaStreamSynchronize(s));
+  if (h != 0) {  // reported once: the next launch on this stream starts clean
+    NEDY_CUDA(cudaMemsetAsync(w, 0, sizeof(int), s));
+    NEDY_CUDA(cudaStreamSynchronize(s));
+  }
   return h;
+}
+
+void split_gemm_set_error(cudaStream_t s, int code) {
+  int *w = err_word(s);
+  NEDY_CUDA(cudaMemcpyAsync(w, &code, sizeof(int), cudaMemcpyHostToDevice, s));
+  NEDY_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace nedy

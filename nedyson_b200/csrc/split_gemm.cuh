@@ -77,7 +77,11 @@ void split_stats(bool on, double *flops, double *ms);
 void split_autotune(bool on);
 std::string split_tune_report();
 
-// Device error word of the split kernels (non-zero after a bounded wait gave up).
+// Error word of the split kernels launched on stream s: non-zero after a bounded wait gave
+// up (1 producer, 2 MMA issuer, 3 epilogue, 4 drain); reading a non-zero word clears it.
+// While it is set, the CTAs of later launches on s skip their work.
 int split_gemm_error(cudaStream_t s);
+// Test hook: preset the error word of stream s (CTAs then skip, as after a timeout).
+void split_gemm_set_error(cudaStream_t s, int code);
 
 }  // namespace nedy

@@ -92,6 +92,68 @@ class DecompSimulation:
             self.do_tstp(t)
 
 
+class FullSimulation:
+    """Full-U restricted GF2 (reference src/molNEsim_impl.h): free_gf (:44-46), do_boot
+    (:65-87, including the mixing-kernel construction set_conv_tensor at :66) and do_tstp
+    (:89-124) through nedy_full_tstp.  U_ijkl = sum_Q B^Q_ij B^Q_kl and
+    Uexch(j,l,n,q) = 2 U(j,n,l,q) - U(j,l,n,q) come from the problem's B^Q."""
+
+    def __init__(self, p: Problem, nt: int, ntau: int, beta: float, dt: float, k: int = 5,
+                 corr_steps: int = 5, drive_kind: str = "none", drive_kw: dict | None = None, device: int = 0):
+        self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k
+        self.corr_steps = corr_steps
+        self.drive_kind, self.drive_kw = drive_kind, dict(drive_kw or {})
+        self.ctx = api.Context(nt, ntau, p.nao, k, beta, dt, device)
+        self.x, self.w = self.ctx.collocation()
+        N = p.nao
+        self.G = api.green_func(self.ctx, nt, ntau, N, -1)
+        self.Sigma = api.green_func(self.ctx, nt, ntau, N, -1)
+        self.solver = api.molGF2Solver(self.ctx, p.U, p.Uexch)
+        self.dyson = api.dyson(self.ctx)
+        self.hmf = api.hmf_buffer(self.ctx, N)
+        self.ht = api.DeviceBuffer(self.ctx, N * N * 16)
+        self.F, self.mu = hf_equilibrium(p, beta)
+        self.boot_err = None
+
+    def h_of_t(self, t: int) -> np.ndarray:
+        E = drive(self.drive_kind, t * self.dt, self.k, self.dt, **self.drive_kw)
+        return (self.p.h0 + E * self.p.D).astype(np.complex128)
+
+    def free_gf(self):
+        g = HostGF(self.nt, self.ntau, self.p.nao, -1)
+        g0_from_h0(g, self.x, self.mu, self.F, self.beta, self.dt, self.k)
+        self.G.from_host(g)
+        hm = np.zeros((self.nt + 1, self.p.nao, self.p.nao), np.complex128)
+        hm[: self.k + 1] = self.F
+        self.hmf.upload(hm)
+
+    def do_boot(self, max_iter: int = 50, tol: float = 1e-12) -> float:
+        err = None
+        for _ in range(max_iter + 1):
+            for t in range(self.k + 1):
+                self.solver.solve(t, self.Sigma, self.G)
+            err = self.dyson.dyson_start(self.G, self.Sigma, self.hmf, self.mu)
+            if err < tol:
+                break
+        self.boot_err = err
+        return err
+
+    def do_tstp(self, t: int) -> float:
+        import ctypes as C
+        from ._lib import check, lib
+        self.ht.upload(self.h_of_t(t))
+        e = C.c_double()
+        check(lib().nedy_full_tstp(self.ctx.h, t, self.G.h, self.Sigma.h, self.hmf.h, self.ht.h, self.mu,
+                                   self.corr_steps, C.byref(e)))
+        return e.value
+
+    def run(self, nt: int | None = None, boot_iter: int = 50, boot_tol: float = 1e-12):
+        self.free_gf()
+        self.do_boot(boot_iter, boot_tol)
+        for t in range(self.k + 1, (nt if nt is not None else self.nt) + 1):
+            self.do_tstp(t)
+
+
 class DecompSpinSimulation:
     """Spin-unrestricted density-fitted GF2 (reference src/molNEsim_decomp_spin_impl.h): free_gf
     (:43-47) from the unrestricted HF equilibrium, do_boot (:63-84, the two dyson_start errors

@@ -1,9 +1,9 @@
 """Regenerate the committed golden fixtures from the reference tree.
 
-Run once, in a container that has the reference checkout (default location
-/root/reference, override with NEDY_REFERENCE):
+Run once, in a container that has the reference checkout, naming its
+location by argument or by the NEDY_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <path-to-NEdyson-checkout>
 
 It writes, next to this script:
 
@@ -23,7 +23,7 @@ import re
 import struct
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("NEDY_REFERENCE", "/root/reference")
+REF = None  # the reference checkout, from the command line or NEDY_REFERENCE (see main)
 
 
 # ---------------------------------------------------------------- HDF5 (tiny)
@@ -168,6 +168,11 @@ def parse_integrals(path):
 
 
 def main():
+    global REF
+    import sys
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NEDY_REFERENCE")
+    if not REF:
+        sys.exit("usage: make_golden.py <path-to-NEdyson-checkout>  (or set NEDY_REFERENCE)")
     h5 = H5(os.path.join(REF, "tests/data/calccoeff.h5"))
     ds = h5.datasets()
     keep = {k: ds[k] for k in ("PInterp", "PDiff", "PInteg", "BD", "Start", "Sigma", "w") if k in ds}

@@ -55,6 +55,28 @@ class OracleDecompSim:
         return e
 
 
+class OracleFullSim(OracleDecompSim):
+    """Full-U driver (reference src/molNEsim_impl.h:65-124) on the oracle: the same sequence
+    as OracleDecompSim with molGF2Solver / molHFSolver in place of the density-fitted ones."""
+
+    def __init__(self, p: Problem, nt, ntau, beta, dt, k=5, corr_steps=5, drive_kind="none", drive_kw=None):
+        super().__init__(p, nt, ntau, beta, dt, k, corr_steps, drive_kind, drive_kw)
+        self.df = _FullAsDF(po.Full(p.U, p.Uexch))
+
+
+class _FullAsDF:
+    """po.Full under the method names the restricted driver calls."""
+
+    def __init__(self, full):
+        self.full = full
+
+    def solve(self, t, S, G):
+        self.full.solve(t, S, G)
+
+    def hf(self, hmf_t, rho):
+        self.full.hf(hmf_t, rho)
+
+
 class OracleDecompSpinSim:
     def __init__(self, p: Problem, nt, ntau, beta, dt, k=5, corr_steps=5, drive_kind="none", drive_kw=None):
         self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k

@@ -1,0 +1,160 @@
+"""Parity of the CUDA path with the CPU oracle at the sizes the benchmark and the
+configurations run, through the C ABI.
+
+* the self-energy row of the headline workload (spin-unrestricted, nao=64, naux=256,
+  the same B^Q and independent h0 per spin) at a small time T with ntau=64, so that
+  the mixed row fills a whole slice chunk and the exchange launches pack the same
+  number of units as in the benchmark; in FP64 (1e-10) and in both split modes
+  (5e-4 with two BF16 pieces, 5e-5 with three, of the largest element);
+* one Dyson step at the headline nao=64 with ntau=256 (the benchmark's grid), and
+  at config 1's nao=32, ntau=256;
+* config 0 as written: the full-U trajectory (nao=4, naux=16, ntau=128, beta=10,
+  k=5, dt=0.02, nt=100, h(t) = h0 + 0.1 sin(2t) D), every step against the oracle;
+* config 1 at its sizes (nao=32, naux=128, ntau=256, beta=20, dt=0.01, Gaussian
+  pulse E0=0.05, t0=2, sigma=0.5) with nt cut to 10 so that the oracle finishes.
+
+The FP64 tolerance is max |GPU - oracle| <= 1e-10 * max(1, max |oracle|).
+"""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from nedyson_b200 import _lib, api
+from nedyson_b200.greens import HostGF
+from nedyson_b200.inputs import make_problem, uhf_equilibrium, g0_from_h0
+from nedyson_b200.simulation import DecompSimulation, FullSimulation
+from simref import OracleDecompSim, OracleFullSim
+from test_gpu_parity import _state
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+SPLIT_TOL = {_lib.PREC_SPLIT_BF16X3: 5e-5, _lib.PREC_SPLIT_BF16X2: 5e-4}
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(1.0, np.abs(b).max()))
+
+
+def relmax(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.fixture(scope="module")
+def headline_sigma():
+    """Oracle self-energy row T=4 of both spins at nao=64, naux=256, ntau=64 on the free
+    (unrestricted Hartree-Fock) G of the headline workload's problem."""
+    N, A, T, ntau, beta, dt = 64, 256, 4, 64, 20.0, 0.01
+    p = make_problem(N, A, seed=7, spin=True)
+    F, mu = uhf_equilibrium(p, beta)
+    x, _ = po.colloc_nodes(ntau)
+    G = []
+    for s in range(2):
+        g = HostGF(T, ntau, N, -1)
+        g0_from_h0(g, x, mu[s], F[s], beta, dt, T)
+        G.append(g)
+    S = [HostGF(T, ntau, N, -1) for _ in range(2)]
+    po.DF(p.Vija).solve_spin(T, S, G)
+    return p, G, S, T, ntau
+
+
+def _row(g: HostGF, T):
+    return {"les": g.les_col(T), "ret": g.ret_row(T), "tv": g.tv[T]}
+
+
+@pytest.mark.parametrize("prec", [_lib.PREC_FP64, _lib.PREC_SPLIT_BF16X2, _lib.PREC_SPLIT_BF16X3])
+def test_sigma_row_headline_size(headline_sigma, prec):
+    p, G, So, T, ntau = headline_sigma
+    N = p.nao
+    ctx = api.Context(max(T, 5), ntau, N, 5, 20.0, 0.01)  # default 8 GiB workspace, as in the benchmark
+    ctx.set_precision(prec)
+    Gd = [api.green_func(ctx, T, ntau, N, -1).from_host(g) for g in G]
+    Sd = [api.green_func(ctx, T, ntau, N, -1) for _ in range(2)]
+    api.molGF2SolverSpinDecomp(ctx, p.Vija).solve(T, Sd, Gd)
+    for s in range(2):
+        got, ref = _row(Sd[s].to_host(), T), _row(So[s], T)
+        for comp in ("les", "ret", "tv"):
+            if prec == _lib.PREC_FP64:
+                e = rel(got[comp], ref[comp])
+                print(f"fp64 spin {s} {comp}: {e:.3e}")
+                assert e < TOL, (s, comp, e)
+            else:
+                e = relmax(got[comp], ref[comp])
+                print(f"split {prec} spin {s} {comp}: {e:.3e} of the largest element")
+                assert 0.0 < e < SPLIT_TOL[prec], (s, comp, e)
+    ctx.close()
+
+
+@pytest.mark.parametrize("nao,T,ntau", [(64, 24, 256), (32, 12, 256)])
+def test_dyson_step_benchmark_grid(nao, T, ntau):
+    nt, beta, dt, k = T, 20.0, 0.01, 5
+    p, G, S, hmf, mu = _state(nao, 4, nt, ntau, beta, dt, k, seed=nao + T, sigma_scale=0.02)
+    ctx = api.Context(nt, ntau, nao, k, beta, dt)
+    Gd = api.green_func(ctx, nt, ntau, nao, -1).from_host(G)
+    Sd = api.green_func(ctx, nt, ntau, nao, -1).from_host(S)
+    hb = api.hmf_buffer(ctx, nao, hmf)
+    eo, _ = po.Dyson(nt, ntau, nao, k).dyson_step(T, G, S, hmf, mu, beta, dt)
+    eg, _ = api.dyson(ctx).dyson_step(T, Gd, Sd, hb, mu)
+    Gh = Gd.to_host()
+    for name, a, b in (("ret", Gh.ret_row(T), G.ret_row(T)), ("tv", Gh.tv[T], G.tv[T]),
+                       ("les", Gh.les_col(T), G.les_col(T))):
+        e = rel(a, b)
+        print(f"dyson nao={nao} T={T} ntau={ntau} {name}: {e:.3e}")
+        assert e < TOL, (name, e)
+    assert abs(eg - eo) <= 1e-8 * max(1.0, abs(eo))
+    ctx.close()
+
+
+def _cmp_all(gpu: HostGF, ref: HostGF, tol=TOL):
+    for comp in ("les", "ret", "tv"):
+        e = rel(getattr(gpu, comp), getattr(ref, comp))
+        assert e < tol, (comp, e)
+    return max(rel(getattr(gpu, c), getattr(ref, c)) for c in ("les", "ret", "tv"))
+
+
+def test_config0_full_u_trajectory():
+    """Config 0 as written, every time step of the trajectory against the oracle."""
+    p = make_problem(4, 16, seed=3)
+    kw = dict(nt=100, ntau=128, beta=10.0, dt=0.02, k=5, corr_steps=5, drive_kind="sin",
+              drive_kw=dict(E0=0.1, omega=2.0))
+    ref = OracleFullSim(p, **kw)
+    ref.free_gf()
+    ref.do_boot(max_iter=30)
+    gpu = FullSimulation(p, **kw)
+    gpu.free_gf()
+    gpu.do_boot(max_iter=30)
+    _cmp_all(gpu.G.to_host(), ref.G)
+    worst = 0.0
+    for t in range(6, 101):
+        ref.do_tstp(t)
+        gpu.do_tstp(t)
+        if t % 10 == 0 or t == 100:
+            worst = max(worst, _cmp_all(gpu.G.to_host(), ref.G))
+    _cmp_all(gpu.Sigma.to_host(), ref.S)
+    e_ref = po.Dyson(100, 128, 4, 5).energy_conv(100, ref.S, ref.G, 10.0, 0.02)
+    e_gpu = gpu.dyson.energy_conv(100, gpu.Sigma, gpu.G)
+    print(f"config 0: max rel |GPU - oracle| over the trajectory {worst:.3e}; E_corr(100) {e_gpu:.12f} vs {e_ref:.12f}")
+    assert abs(e_gpu - e_ref) <= 1e-10 * max(1.0, abs(e_ref))
+    gpu.ctx.close()
+
+
+def test_config1_trajectory_truncated():
+    """Config 1's sizes (nao=32, naux=128, ntau=256, beta=20, dt=0.01, Gaussian pulse) with nt cut to
+    10: bootstrap (three iterations) and steps 6..10 with two corrector iterations each."""
+    p = make_problem(32, 128, seed=11)
+    kw = dict(nt=10, ntau=256, beta=20.0, dt=0.01, k=5, corr_steps=2, drive_kind="gauss",
+              drive_kw=dict(E0=0.05, t0=2.0, sigma=0.5))
+    ref = OracleDecompSim(p, **kw)
+    ref.free_gf()
+    ref.do_boot(max_iter=2, tol=0.0)
+    gpu = DecompSimulation(p, **kw)
+    gpu.free_gf()
+    gpu.do_boot(max_iter=2, tol=0.0)
+    _cmp_all(gpu.G.to_host(), ref.G)
+    for t in range(6, 11):
+        ref.do_tstp(t)
+        gpu.do_tstp(t)
+    worst = _cmp_all(gpu.G.to_host(), ref.G)
+    _cmp_all(gpu.Sigma.to_host(), ref.S)
+    print(f"config 1 (nt cut to 10): max rel |GPU - oracle| {worst:.3e}")
+    gpu.ctx.close()

@@ -57,3 +57,48 @@ def test_split_gemm_check_rejects_missing_instance():
     err = C.c_double()
     rc = _lib.lib().nedy_split_gemm_check(0, 128, 128, 64, 1, 1, 1, 0, 0, 2, 0, 0, 96, 2, 0, 1, 1, C.byref(err))
     assert rc == NEDY_ERR_ARG
+
+
+def test_split_timeout_path_reports_and_recovers():
+    """The bounded-wait give-up path without a fault: the context's error word is preset as a
+    wait that gave up would set it, so every CTA of the next split launches skips its work.
+    The self-energy call must return NEDY_ERR_TIMEOUT, and the call after it (the report
+    cleared the word) must run normally and reproduce the first result."""
+    import numpy as np
+    from nedyson_b200 import api
+    from nedyson_b200.greens import HostGF
+    rng = np.random.default_rng(5)
+    nao, naux, nt, ntau = 8, 24, 3, 4
+    V = rng.uniform(-1, 1, (nao, nao, naux)) / np.sqrt(naux)
+    V = 0.5 * (V + V.transpose(1, 0, 2))
+    G = HostGF(nt, ntau, nao, -1)
+    for a in (G.les, G.ret, G.tv, G.mat):
+        a[:] = rng.uniform(-1, 1, a.shape) + 1j * rng.uniform(-1, 1, a.shape)
+    ctx = api.Context(5, ntau, nao, 5, 1.0, 0.01)
+    ctx.set_precision(_lib.PREC_SPLIT_BF16X2)
+    Gd = api.green_func(ctx, nt, ntau, nao, -1).from_host(G)
+    Sd = api.green_func(ctx, nt, ntau, nao, -1)
+    s = api.molGF2SolverDecomp(ctx, V)
+    lib = _lib.lib()
+    lib.nedy_split_autotune(0)  # one fixed instance per class: the two good calls run the same kernels
+    try:
+        _timeout_roundtrip(lib, ctx, s, Sd, Gd, nt)
+    finally:
+        lib.nedy_split_autotune(1)
+        ctx.close()
+
+
+def _timeout_roundtrip(lib, ctx, s, Sd, Gd, nt):
+    import numpy as np
+    NEDY_ERR_TIMEOUT = 4
+    s.solve(nt, Sd, Gd)
+    first = Sd.to_host()
+    assert lib.nedy_ctx_inject_split_error(ctx.h, 2) == NEDY_OK
+    rc = lib.nedy_gf2_decomp_solve(ctx.h, nt, Sd.h, Gd.h)
+    assert rc == NEDY_ERR_TIMEOUT, (rc, lib.nedy_last_error())
+    assert b"timed out" in lib.nedy_last_error()
+    s.solve(nt, Sd, Gd)  # raises if the word were still set
+    again = Sd.to_host()
+    for comp in ("les", "ret", "tv"):  # equal up to the order of FP64 atomic sums
+        a, b = getattr(again, comp), getattr(first, comp)
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max(), comp

@@ -1,8 +1,13 @@
 """nedy_hf_decomp_noalloc against nedy_hf_decomp, through the C ABI.
 
-The no-allocation entry point keeps its intermediates in one static device
-array shared by every call, so two calls in a row (different time slices,
-different densities) must both reproduce the allocating entry point.
+Some host programs cannot let the engine allocate device memory once their
+simulation runs: their own pool allocator already holds the free memory, or a
+cudaMalloc/cudaFree would synchronise a device they keep busy.  The
+no-allocation entry point keeps its intermediates in one static device array
+shared by every call, so two calls in a row (different time slices, different
+densities) must both reproduce the allocating entry point, and after the first
+call (which only looks up the array's address) the device's free memory must
+not move.
 """
 import numpy as np
 import pytest
@@ -13,6 +18,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-10
 NEDY_ERR_ARG = 1
+ALLOC_GRANULE = 2 << 20  # a device allocation takes free memory in steps of at least 2 MiB
 
 
 def rel(a, b):
@@ -24,27 +30,47 @@ def _hermitian(rng, n):
     return 0.5 * (x + x.conj().T)
 
 
+def _free_bytes():
+    import torch
+    return torch.cuda.mem_get_info(0)[0]
+
+
 @pytest.mark.parametrize("nao,naux", [(6, 11), (64, 256)])
 def test_hf_noalloc_matches_hf_decomp_twice(nao, naux):
     rng = np.random.default_rng(1000 + nao)
     nt = 4
-    ctx = api.Context(nt, 4, nao, 1, 1.0, 0.01)
     V = rng.standard_normal((nao, nao, naux)) * 0.1
     V = 0.5 * (V + V.transpose(1, 0, 2))
-    api.molGF2SolverDecomp(ctx, V)
     h0 = np.stack([_hermitian(rng, nao) for _ in range(nt + 1)])
-    h_ref = api.hmf_buffer(ctx, nao, h0)
-    h_new = api.hmf_buffer(ctx, nao, h0)
+    rhos = [np.ascontiguousarray(_hermitian(rng, nao)) for _ in range(2)]
     lib = _lib.lib()
-    for tstp in (3, 1):
-        rho = api.DeviceBuffer.from_array(ctx, np.ascontiguousarray(_hermitian(rng, nao)))
-        _lib.check(lib.nedy_hf_decomp(ctx.h, tstp, h_ref.h, rho.h))
-        _lib.check(lib.nedy_hf_decomp_noalloc(ctx.h, tstp, h_new.h, rho.h))
+    # the allocating entry point on a context of its own
+    ref_ctx = api.Context(nt, 4, nao, 1, 1.0, 0.01)
+    api.molGF2SolverDecomp(ref_ctx, V)
+    h_ref = api.hmf_buffer(ref_ctx, nao, h0)
+    refs = []
+    for tstp, rho in zip((3, 1), rhos):
+        rb = api.DeviceBuffer.from_array(ref_ctx, rho)
+        _lib.check(lib.nedy_hf_decomp(ref_ctx.h, tstp, h_ref.h, rb.h))
+        refs.append(h_ref.download((nt + 1, nao, nao))[tstp])
+    ref_ctx.close()
+    # the no-allocation entry point on a fresh context: every buffer exists before the calls
+    ctx = api.Context(nt, 4, nao, 1, 1.0, 0.01)
+    api.molGF2SolverDecomp(ctx, V)
+    h_new = api.hmf_buffer(ctx, nao, h0)
+    rbs = [api.DeviceBuffer.from_array(ctx, rho) for rho in rhos]
+    free = []
+    for (tstp, rb), ref in zip(zip((3, 1), rbs), refs):
+        _lib.check(lib.nedy_hf_decomp_noalloc(ctx.h, tstp, h_new.h, rb.h))
+        free.append(_free_bytes())
         a = h_new.download((nt + 1, nao, nao))
-        b = h_ref.download((nt + 1, nao, nao))
-        assert rel(a[tstp], b[tstp]) < TOL
-        assert np.max(np.abs(b[tstp] - h0[tstp])) > 0.0  # the update did something
-        assert np.array_equal(np.delete(a, [1, 3], axis=0), np.delete(h0, [1, 3], axis=0))
+        assert rel(a[tstp], ref) < TOL
+        assert np.max(np.abs(ref - h0[tstp])) > 0.0  # the update did something
+    # untouched time slices stay as they were
+    a = h_new.download((nt + 1, nao, nao))
+    assert np.array_equal(np.delete(a, [1, 3], axis=0), np.delete(h0, [1, 3], axis=0))
+    # the second call allocated nothing
+    assert abs(free[1] - free[0]) < ALLOC_GRANULE, free
     ctx.close()
 
 
