@@ -5,21 +5,25 @@ split precision + predictor at max|dG| <= 1e-8.
 One "step" is one full time step T of the spin-unrestricted density-fitted GF2
 simulation (DecompSpinSimulation::do_tstp, reference
 src/molNEsim_decomp_spin_impl.h:86-108) through the C ABI: both spins' G rows.
-Two forms run the same window from the same state:
+Four forms run the same window from the same state (the W warm-up steps):
 
-  plain FP64       nedy_decomp_spin_tstp: polynomial predictor, then CorrSteps = 5 x
-                   [density matrices, unrestricted HF mean field, GF2 self-energy rows T
-                   of both spins, Dyson step row T per spin], every contraction in FP64
-                   (the reference's algorithm);
-  split+predictor  nedy_decomp_spin_tstp_tol on a context in NEDY_PREC_SPLIT_BF16X2 (or
-                   _BF16X3 with --split-mode bf16x3): the self-energy contractions as
-                   BF16 piece products on tcgen05, the
-                   predictor, and the residual exit at tol = 1e-8 (at most 5 iterations).
+  split_learned_exit  the headline (value): nedy_decomp_spin_tstp_tol on a context in
+                      NEDY_PREC_SPLIT_BF16X2 (or _BF16X3 with --split-mode bf16x3): the
+                      self-energy contractions as BF16 piece products on tcgen05, the learned
+                      predictor, and the residual exit at tol = 1e-8 (at most 5 iterations);
+  split_poly_exit     the same with the polynomial predictor only;
+  plain_fp64_exit     FP64 throughout with the residual exit (the exit without the precision);
+  plain_fp64          nedy_decomp_spin_tstp: polynomial predictor, then CorrSteps = 5 x
+                      [density matrices, unrestricted HF mean field, GF2 self-energy rows T of
+                      both spins, Dyson step row T per spin], every contraction in FP64 (the
+                      reference's algorithm).
 
-value is the split+predictor form (the headline); the plain form, the iterations per
-step and max|dG| between the two forms over the window (per component and spin, and
-the GF2 correlation energy) are in the same line.  --restricted runs the restricted
-simulation (DecompSimulation::do_tstp, src/molNEsim_decomp_impl.h:85-104) instead.
+The plain forms run the first --plain-steps steps of the window; every form's new rows
+over those steps are compared with plain_fp64 (max |dG| per component and spin, and the
+GF2 correlation energy).  e2e runs the headline form over the whole window again through
+the C ABI with h(t) copied in from pinned host memory and the new G rows copied out,
+inside the timed region.  --restricted runs the restricted simulation
+(DecompSimulation::do_tstp, src/molNEsim_decomp_impl.h:85-104) instead.
 
 Workload: nao=64, naux=256, independent random h0 per spin with the same B^Q, ntau=256,
 beta=20, k=5, dt=0.01, steps T = t0+W ... t0+W+K-1 on a GF2 trajectory from the
@@ -30,8 +34,11 @@ needed.
 Multi-GPU: one independent trajectory per GPU (replicas, no collective);
 value = total time steps of all ranks / max-over-ranks time.
 
---impl reference times the CPU restatement of the reference solver (oracle/)
-on the host cores on a bounded sample and reports the same metric.
+--impl reference times the CPU restatement of the reference solver (oracle/) on the
+host cores: one complete corrector iteration of the plain step at the window's first T
+and the metric's ntau, measured in K parts (one per step); timesteps/s = 1 / (CorrSteps x
+iteration time).  The engine arm's cpu_baseline is a bounded sample of the same
+iteration (measured time per slice of each kind x slice counts, plus a Dyson step).
 """
 from __future__ import annotations
 
@@ -87,6 +94,8 @@ def parse():
                     help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
+    ap.add_argument("--plain-steps", type=int, default=4,
+                    help="window steps of the plain FP64 forms (and of the error comparison between the forms)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
                     help="self-energy chunk workspace in GiB (0: the library default); small for profiling runs")
     ap.add_argument("--no-autotune", action="store_true",
@@ -193,83 +202,151 @@ class Clocks:
                 "samples": len(sm)}
 
 
-# ------------------------------------------------------------------ CPU sample (oracle)
-def cpu_sample(args, target_seconds=20.0):
-    """Time the CPU restatement of the reference on a bounded sample and scale to one step at T.
-
-    Sample: one GF2 self-energy row at (nao, naux) with small T_s / ntau_s (enough slices for
-    every core), and one Dyson step at T_d = 24, ntau_d = 16; each is scaled to the bench
-    step by the flop models above (time per flop assumed constant)."""
-    from oracle import pyoracle as po
-    from nedyson_b200.greens import HostGF
-    from nedyson_b200.inputs import make_problem, hf_equilibrium, free_history
-    # every OpenMP thread holds one nao^4 exchange intermediate (268 MB at nao = 64): cap the threads
-    cores = min(os.cpu_count() or 1, 32)
-    po.set_threads(cores)
-    N, A = args.nao, args.naux
-    ns = 1 if args.restricted else 2
-    p = make_problem(N, A, args.seed, spin=ns == 2)
-    rng = np.random.default_rng(1)
-    ntau_s = 8
-    T_s = max(2, (cores - ntau_s - 1 + 1) // 2)
-    Gs, Ss = [], []
-    for _ in range(ns):
-        G = HostGF(T_s, ntau_s, N, -1)
-        for a in (G.les, G.ret, G.tv):
-            a[:] = 0.05 * (rng.uniform(-1, 1, a.shape) + 1j * rng.uniform(-1, 1, a.shape))
-        Gs.append(G)
-        Ss.append(HostGF(T_s, ntau_s, N, -1))
-    df = po.DF(p.Vija)
-    t0 = time.perf_counter()
-    if ns == 2:
-        df.solve_spin(T_s, Ss, Gs)
-    else:
-        df.solve(T_s, Ss[0], Gs[0])
-    ts = time.perf_counter() - t0
-    rate_s = flops_sigma(T_s, N, A, ntau_s, ns) / ts
-    # Dyson sample
-    T_d, ntau_d = 24, 16
-    F, mu = hf_equilibrium(make_problem(N, A, args.seed), args.beta)
-    x, _ = po.colloc_nodes(ntau_d)
-    Gd = HostGF(T_d, ntau_d, N, -1)
-    les, ret, tv, mat = free_history(T_d, T_d + 1, ntau_d, x, mu, F, args.beta, args.dt)
-    Gd.les[:] = les
-    Gd.ret[:] = ret
-    Gd.tv[:] = tv
-    Gd.mat[:] = mat
-    Sd = HostGF(T_d, ntau_d, N, -1)
-    Sd.les[:] = 0.02 * les
-    Sd.ret[:] = 0.02 * ret
-    Sd.tv[:] = 0.02 * tv
-    hmf = np.repeat(F[None].astype(complex), T_d + 1, axis=0)
-    dy = po.Dyson(T_d, ntau_d, N, 5)
-    dy.mixing(Sd.tv[0], Gd.mat, args.beta, -1.0)  # builds the tau kernel outside the timing
-    t0 = time.perf_counter()
-    dy.dyson_step(T_d, Gd, Sd, hmf, mu, args.beta, args.dt)
-    td = time.perf_counter() - t0
-    rate_d = flops_dyson(T_d, N, ntau_d) / td
-    return dict(cores=cores, T_s=T_s, ntau_s=ntau_s, sigma_s=ts, rate_sigma=rate_s, T_d=T_d, ntau_d=ntau_d,
-                dyson_s=td, rate_dyson=rate_d, nspin=ns)
+# ------------------------------------------------------------------ CPU corrector iteration (oracle)
+def cpu_threads():
+    """Host threads for the oracle: every core, bounded by memory (each OpenMP thread holds one
+    nao^4 exchange intermediate, 268 MB at nao = 64)."""
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        mem = psutil.virtual_memory().available
+        cores = max(1, min(cores, int(mem * 0.5 // (1 << 29))))
+    except Exception:
+        cores = min(cores, 32)
+    return cores
 
 
-def cpu_step_seconds(smp, T, args):
-    """One step: CorrSteps x (self-energy rows of all spins + one Dyson step per spin)."""
-    ns = smp["nspin"]
-    return args.corr * (flops_sigma(T, args.nao, args.naux, args.ntau, ns) / smp["rate_sigma"] +
-                        ns * flops_dyson(T, args.nao, args.ntau) / smp["rate_dyson"])
+class CpuIteration:
+    """One complete corrector iteration of the plain unrestricted step at time T on the host
+    cores, by the CPU restatement of the reference (oracle/): the self-energy rows of both spins
+    (2 (T+1) + ntau + 1 slices, each slice both spins: reference
+    src/mol2bSolver_spin_decomp_impl.h:436-466), the unrestricted mean field and one Dyson step
+    per spin (src/dyson_step.h:329-382), on a free-propagation state of the workload's problem
+    (rows 0..T of both spins, the metric's nao, naux and ntau).
+
+    The iteration can run in parts (ranges of slices; the two Dyson steps in two of the parts),
+    so that its complete time is measured piecewise in bounded steps."""
+
+    def __init__(self, args, T):
+        from oracle import pyoracle as po
+        from nedyson_b200.greens import HostGF
+        from nedyson_b200.inputs import make_problem, uhf_equilibrium, hf_equilibrium, free_history
+        self.po = po
+        self.cores = cpu_threads()
+        po.set_threads(self.cores)
+        N, A, ntau = args.nao, args.naux, args.ntau
+        self.T, self.N, self.ntau, self.args = T, N, ntau, args
+        self.ns = 1 if args.restricted else 2
+        p = make_problem(N, A, args.seed, spin=self.ns == 2)
+        if self.ns == 2:
+            Fs, mus = uhf_equilibrium(p, args.beta)
+        else:
+            F, mu = hf_equilibrium(p, args.beta)
+            Fs, mus = (F,), (mu,)
+        self.mus, self.Fs, self.p = mus, Fs, p
+        x, _ = po.colloc_nodes(ntau)
+        self.G, self.S, self.hmf = [], [], []
+        for s in range(self.ns):
+            G = HostGF(T, ntau, N, -1)
+            les, ret, tv, mat = free_history(T, T + 1, ntau, x, mus[s], Fs[s], args.beta, args.dt)
+            G.les[:] = les
+            G.ret[:] = ret
+            G.tv[:] = tv
+            G.mat[:] = mat
+            del les, ret, tv
+            S = HostGF(T, ntau, N, -1)
+            S.les[:] = 0.02 * G.les
+            S.ret[:] = 0.02 * G.ret
+            S.tv[:] = 0.02 * G.tv
+            self.G.append(G)
+            self.S.append(S)
+            self.hmf.append(np.repeat(Fs[s][None].astype(complex), T + 1, axis=0))
+        self.df = po.DF(p.Vija)
+        self.dy = po.Dyson(T, ntau, N, 5)
+        nles = T + 1
+        # slice jobs of the row (lesser t, retarded t, mixed tau) and their relative cost
+        # (a retarded slice is two bubble and two exchange units, the others one each)
+        self.njobs = 2 * nles + ntau + 1
+        self.weight = np.array([1.0] * nles + [2.0] * nles + [1.0] * (ntau + 1))
+
+    def run_jobs(self, lo, hi):
+        if self.ns == 2:
+            self.df.solve_spin_jobs(self.T, self.S, self.G, lo, hi)
+        else:
+            self.df.solve_jobs(self.T, self.S[0], self.G[0], lo, hi)
+
+    def run_dyson(self, s):
+        a = self.args
+        self.dy.dyson_step(self.T, self.G[s], self.S[s], self.hmf[s], self.mus[s], a.beta, a.dt)
+
+    def run_mean_field(self):
+        rho = np.stack([g.get_dm(self.T) for g in self.G])
+        if self.ns == 2:
+            hu, hd = self.hmf[0][self.T].copy(), self.hmf[1][self.T].copy()
+            self.df.hf_spin(hu, hd, rho)
+        else:
+            h = self.hmf[0][self.T].copy()
+            self.df.hf(h, rho[0])
+
+    def parts(self, n):
+        """n parts of one iteration: contiguous slice ranges of equal cost; Dyson step of spin s
+        in part (s + 1) n // (ns + 1); the mean field in part 0."""
+        cw = np.concatenate([[0.0], np.cumsum(self.weight)])
+        bounds = [int(np.searchsorted(cw, cw[-1] * i / n)) for i in range(n + 1)]
+        bounds[0], bounds[-1] = 0, self.njobs
+        out = []
+        for i in range(n):
+            dys = [s for s in range(self.ns) if (s + 1) * n // (self.ns + 1) == i] if n > 1 else list(range(self.ns))
+            out.append((bounds[i], bounds[i + 1], dys, i == 0))
+        return out
+
+    def run_part(self, part):
+        lo, hi, dys, mf = part
+        t0 = time.perf_counter()
+        if mf:
+            self.run_mean_field()
+        if hi > lo:
+            self.run_jobs(lo, hi)
+        for s in dys:
+            self.run_dyson(s)
+        return time.perf_counter() - t0
+
+    def sample(self, budget_s=20.0):
+        """Bounded sample of the iteration for the engine arm: the first `cores` slices of each
+        kind (lesser, retarded, mixed) and one Dyson step, each timed; the iteration time is
+        the measured time per slice of each kind times its slice count, plus the Dyson step
+        once per spin.  Returns (iteration seconds, description)."""
+        nles, ntv = self.T + 1, self.ntau + 1
+        c = max(1, min(self.cores, nles, ntv))
+        kinds = [("lesser", 0, nles), ("retarded", nles, nles), ("mixed", 2 * nles, ntv)]
+        total, parts = 0.0, []
+        for name, lo, cnt in kinds:
+            t0 = time.perf_counter()
+            self.run_jobs(lo, lo + c)
+            dtk = time.perf_counter() - t0
+            total += dtk / c * cnt
+            parts.append(f"{c} {name} slices {dtk:.2f} s")
+        t0 = time.perf_counter()
+        self.run_dyson(0)
+        dd = time.perf_counter() - t0
+        total += dd * self.ns
+        parts.append(f"Dyson step {dd:.2f} s (x{self.ns} spins)")
+        desc = (f"oracle (C++ restatement, OpenMP over slices, OpenBLAS) on {self.cores} threads, at the bench "
+                f"state's T={self.T}, ntau={self.ntau}, nao={self.N}, naux={self.args.naux}: "
+                + ", ".join(parts) + f"; one iteration = measured time per slice x slice count "
+                f"({2 * nles + ntv} slices per spin pair) + the Dyson steps = {total:.1f} s; one step = "
+                f"{self.args.corr} iterations (the reference's CorrSteps)")
+        return total, desc
 
 
-def cpu_baseline_obj(smp, value, args):
-    return {"value": value, "unit": "timesteps/s", "cores": smp["cores"], "kind": "port",
-            "sample": (f"oracle (C++ restatement, OpenMP over slices, OpenBLAS) timed on one "
-                       f"{'unrestricted (both spins)' if smp['nspin'] == 2 else 'restricted'} GF2 self-energy row "
-                       f"at nao={args.nao}, naux={args.naux}, T={smp['T_s']}, ntau={smp['ntau_s']} "
-                       f"({smp['sigma_s']:.2f} s, {smp['rate_sigma'] / 1e9:.1f} GFLOP/s) and one Dyson step at "
-                       f"T={smp['T_d']}, ntau={smp['ntau_d']} ({smp['dyson_s']:.2f} s, "
-                       f"{smp['rate_dyson'] / 1e9:.1f} GFLOP/s), scaled by the flop model to one "
-                       f"{args.corr}-iteration step ({smp['nspin']} Dyson steps per iteration) at T={args.t0 + args.warmup}, "
-                       f"ntau={args.ntau}")}
+def cpu_baseline_obj(value, cores, sample):
+    return {"value": value, "unit": "timesteps/s", "cores": cores, "kind": "port", "sample": sample}
 
+
+# DRAM bytes of all split GEMM launches per exchange unit (one slice of one spin) at nao=64,
+# naux=256 with two pieces per operand: sum over the GEMM classes of dram__bytes_read.sum +
+# dram__bytes_write.sum from the ncu capture of the ntau=32 case, divided by its units.
+SPLIT_TRAFFIC_PER_UNIT = 3.6e8
 
 # ------------------------------------------------------------------ peaks
 def measured_peaks():
@@ -323,6 +400,8 @@ def run_engine(args, dist: Dist):
     spin = not args.restricted
     ns = 2 if spin else 1
     t_first = args.t0
+    T_warm = list(range(t_first, t_first + W))
+    T_timed = list(range(t_first + W, t_first + W + K))
     nt = t_first + W + K
     p = make_problem(N, A, rank_seed(args.seed, dist.rank), spin=spin)
     if spin:
@@ -338,8 +417,8 @@ def run_engine(args, dist: Dist):
     solver = (api.molGF2SolverSpinDecomp if spin else api.molGF2SolverDecomp)(ctx, p.Vija)
     kk = 5
     traj = args.state == "trajectory"
-    # one-body Hamiltonian of every step and spin, resident on the device.  Trajectory state:
-    # the Gaussian pulse E0 = 0.05, t0 = 2, sigma = 0.5 along D; synthetic state: 0.1 sin(2t).
+    # one-body Hamiltonian of every step and spin.  Trajectory state: the Gaussian pulse
+    # E0 = 0.05, t0 = 2, sigma = 0.5 along D; synthetic state: 0.1 sin(2t).
     dkind, dkw = ("gauss", {"E0": 0.05, "t0": 2.0, "sigma": 0.5}) if traj else ("sin", {})
 
     def h_of(t, s):
@@ -360,6 +439,16 @@ def run_engine(args, dist: Dist):
             check(lib().nedy_decomp_tstp_tol(ctx.h, t, G[0].h, S[0].h, hmf[0].h, h[0].h, mus[0], m, tol,
                                              C.byref(it), None))
         return it.value
+
+    def step_plain(t):
+        e = C.c_double()
+        if spin:
+            check(lib().nedy_decomp_spin_tstp(ctx.h, t, G[0].h, G[1].h, S[0].h, S[1].h, hmf[0].h, hmf[1].h,
+                                              hts[0][t].h, hts[1][t].h, mus[0], mus[1], args.corr, C.byref(e)))
+        else:
+            check(lib().nedy_decomp_tstp(ctx.h, t, G[0].h, S[0].h, hmf[0].h, hts[0][t].h, mus[0], args.corr,
+                                         C.byref(e)))
+        return args.corr
 
     if traj:
         # GF2 trajectory from the Hartree-Fock equilibrium: free propagation on rows 0..k as
@@ -407,58 +496,46 @@ def run_engine(args, dist: Dist):
     pred, pred_info = None, None
     if args.predictor == "learned":
         pred, pred_info = train_predictor(ctx, args)
-    # pinned host buffers for the end-to-end pass: h(t) of each spin in, new G rows out
-    row_blocks = 2 * (nt + 1) + (ntau + 1)
-    h_host = torch.empty((ns, N, N), dtype=torch.complex128).pin_memory()
-    row_host = torch.empty((ns, row_blocks, N, N), dtype=torch.complex128).pin_memory()
-    ht_e2e = [api.DeviceBuffer(ctx, N * N * 16) for _ in range(ns)]
     sp = C.c_void_p()
     check(lib().nedy_ctx_stream(ctx.h, C.byref(sp)))
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device(f"cuda:{dev}"))
-    iters = []
-
-    def step_plain(t):
-        e = C.c_double()
-        if spin:
-            check(lib().nedy_decomp_spin_tstp(ctx.h, t, G[0].h, G[1].h, S[0].h, S[1].h, hmf[0].h, hmf[1].h,
-                                              hts[0][t].h, hts[1][t].h, mus[0], mus[1], args.corr, C.byref(e)))
-        else:
-            check(lib().nedy_decomp_tstp(ctx.h, t, G[0].h, S[0].h, hmf[0].h, hts[0][t].h, mus[0], args.corr,
-                                         C.byref(e)))
-
-    def step_split(t, ht=None):
-        iters.append(step_tol(t, args.tol, ht))
 
     def window_rows(T_list):
         """Per step T and spin: the new row of each component (les column, ret row, tv row)."""
         return [[(G[s].les_col(t), G[s].ret_row(t), G[s].tv_row(t)) for s in range(ns)] for t in T_list]
 
     def energies(T_list):
-        dy = api.dyson(ctx)
-        return [[dy.energy_conv(t, S[s], G[s]) for s in range(ns)] for t in T_list]
+        d = api.dyson(ctx)
+        return [[d.energy_conv(t, S[s], G[s]) for s in range(ns)] for t in T_list]
 
-    def timed(step, T_list, split):
-        """K steps between CUDA events on the engine stream, phase times, launches, clocks."""
+    def set_form(prec, learned):
+        ctx.set_precision(prec)
+        ctx.set_predictor(pred if learned else None)
+
+    def timed(step, T_list, split, clocks_on=True):
+        """Steps between CUDA events on the engine stream (one pair per step), phase times,
+        launches, clocks."""
         check(lib().nedy_ctx_set_timing(ctx.h, 1))
-        clocks = Clocks(dev) if dist.rank == 0 else None
+        clocks = Clocks(dev) if (dist.rank == 0 and clocks_on) else None
         n0 = lib().nedy_launch_count()
         if split:
             check(lib().nedy_split_stats(1, None, None))
         dist.barrier()
         torch.cuda.synchronize(dev)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(T_list) + 1)]
+        ev[0].record(stream)
         # NVTX range around the timed steps (lets a profiler select exactly these launches)
         torch.cuda.nvtx.range_push("timed_split" if split else "timed_plain")
-        for t in T_list:
-            step(t)
+        its = []
+        for i, t in enumerate(T_list):
+            its.append(step(t))
+            ev[i + 1].record(stream)
         torch.cuda.nvtx.range_pop()
-        e1.record(stream)
         torch.cuda.synchronize(dev)
         dist.barrier()
-        secs = e0.elapsed_time(e1) / 1e3
-        out = {"secs": dist.max(secs), "launches": int(lib().nedy_launch_count() - n0)}
+        per = [ev[i].elapsed_time(ev[i + 1]) / 1e3 for i in range(len(T_list))]
+        out = {"secs": dist.max(sum(per)), "per_step_s": per, "iters": its,
+               "launches": int(lib().nedy_launch_count() - n0)}
         ms4 = (C.c_double * 4)()
         check(lib().nedy_ctx_phase_times(ctx.h, ms4))
         check(lib().nedy_ctx_set_timing(ctx.h, 0))
@@ -470,78 +547,90 @@ def run_engine(args, dist: Dist):
         out["clocks"] = clocks.stop() if clocks else None
         return out
 
-    T_timed = list(range(t_first + W, t_first + W + K))
-    # shared warm-up: W plain steps define the starting state of both forms
-    ctx.set_precision(PREC_SPLIT if args.split_only else PREC_FP64)
-    for t in range(t_first, t_first + W):
-        (step_split if args.split_only else step_plain)(t)
+    split_step = lambda t: step_tol(t, args.tol)  # noqa: E731
+    exit_plain = lambda t: step_tol(t, args.tol)  # noqa: E731
+    # warm-up: W steps of the headline form; their rows are the history every form starts from
+    set_form(PREC_SPLIT, pred is not None)
+    for t in T_warm:
+        split_step(t)
     ctx.synchronize()
-    plain, rows_plain, e_plain = None, None, None
+    Kc = min(K, args.plain_steps)  # steps compared between the forms (the plain FP64 form is slow)
+    forms = {}
+    # 1. headline: split precision + learned predictor + residual exit
+    head = timed(split_step, T_timed, True)
+    rows_head, e_head = window_rows(T_timed[:Kc]), energies(T_timed[:Kc])
+    pstats = ctx.predictor_stats() if pred is not None else None
+    forms["split_learned_exit"] = head
+    rows, ens = {}, {}
+    rows["split_learned_exit"], ens["split_learned_exit"] = rows_head, e_head
     if not args.split_only:
-        plain = timed(step_plain, T_timed, False)
-        rows_plain = window_rows(T_timed)
-        e_plain = energies(T_timed)
-    # split+predictor: warm-up on the window rows (recomputed below from the same history)
-    ctx.set_precision(PREC_SPLIT)
-    if pred is not None:
-        ctx.set_predictor(pred)
-    for t in T_timed[:W]:
-        step_split(t)
-    ctx.synchronize()
-    iters.clear()
-    split = timed(step_split, T_timed, True)
-    split_iters = list(iters)
-    rows_split = window_rows(T_timed)
-    e_split = energies(T_timed)
+        # 2. split precision + polynomial predictor + residual exit
+        set_form(PREC_SPLIT, False)
+        forms["split_poly_exit"] = timed(split_step, T_timed, True, clocks_on=False)
+        rows["split_poly_exit"], ens["split_poly_exit"] = window_rows(T_timed[:Kc]), energies(T_timed[:Kc])
+        # 3. plain FP64 + residual exit (the exit alone, same arithmetic as the reference)
+        set_form(PREC_FP64, False)
+        forms["plain_fp64_exit"] = timed(exit_plain, T_timed[:Kc], False, clocks_on=False)
+        rows["plain_fp64_exit"], ens["plain_fp64_exit"] = window_rows(T_timed[:Kc]), energies(T_timed[:Kc])
+        # 4. plain FP64, CorrSteps fixed iterations: the reference's algorithm
+        forms["plain_fp64"] = timed(step_plain, T_timed[:Kc], False)
+        rows["plain_fp64"], ens["plain_fp64"] = window_rows(T_timed[:Kc]), energies(T_timed[:Kc])
     comps = ("les", "ret", "tv")
     spins = ("up", "down") if spin else ("restricted",)
-    err = None
-    if rows_plain:
-        err = {}
-        for si, sn in enumerate(spins):
-            for ci, cn in enumerate(comps):
-                err[f"{cn}_{sn}"] = max(float(np.abs(a[si][ci] - b[si][ci]).max())
-                                        for a, b in zip(rows_plain, rows_split))
-            err[f"energy_{sn}"] = max(abs(a[si] - b[si]) for a, b in zip(e_plain, e_split))
-    max_dg = max(v for k, v in err.items() if not k.startswith("energy")) if err else None
-    max_g = max(float(np.abs(c).max()) for r in rows_split for sr in r for c in sr)
+    errs = {}
+    if "plain_fp64" in rows:
+        ref_rows, ref_e = rows["plain_fp64"], ens["plain_fp64"]
+        for name in rows:
+            if name == "plain_fp64":
+                continue
+            err = {}
+            for si, sn in enumerate(spins):
+                for ci, cn in enumerate(comps):
+                    err[f"{cn}_{sn}"] = max(float(np.abs(a[si][ci] - b[si][ci]).max())
+                                            for a, b in zip(ref_rows, rows[name]))
+                err[f"energy_{sn}"] = max(abs(a[si] - b[si]) for a, b in zip(ref_e, ens[name]))
+            err["max_abs_dG"] = max(v for k2, v in err.items() if not k2.startswith("energy"))
+            errs[name] = err
+    max_g = max(float(np.abs(c).max()) for r in rows_head for sr in r for c in sr)
 
-    # end-to-end pass through the C ABI with host buffers (split form): re-run the last timed
-    # step T_e (rows are recomputed in place), copying h(T_e) of each spin from pinned host
-    # memory in and the new G rows (les column, ret row, tv row) back out, all inside the
-    # timed region.
-    T_e = T_timed[-1]
-    for s in range(ns):
-        h_host[s].copy_(torch.from_numpy(h_of(T_e, s)))
-    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # end-to-end pass through the C ABI with host buffers (headline form): every step of the
+    # window again, each step copying h(t) of each spin from pinned host memory in and the
+    # step's new G rows (les column, ret row, tv row) back out, inside the timed region.
+    set_form(PREC_SPLIT, pred is not None)
     es = N * N * 16
+    h_host = torch.empty((K, ns, N, N), dtype=torch.complex128).pin_memory()
+    for i, t in enumerate(T_timed):
+        for s in range(ns):
+            h_host[i, s].copy_(torch.from_numpy(h_of(t, s)))
+    row_blocks = 2 * (nt + 1) + (ntau + 1)
+    row_host = torch.empty((ns, row_blocks, N, N), dtype=torch.complex128).pin_memory()
+    ht_e2e = [api.DeviceBuffer(ctx, es) for _ in range(ns)]
+    h2d = d2h = 0
     dist.barrier()
     torch.cuda.synchronize(dev)
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ee0.record(stream)
-    for s in range(ns):
-        check(lib().nedy_buf_upload(ht_e2e[s].h, 0, es, C.c_void_p(h_host.data_ptr() + s * es)))
-    step_split(T_e, ht_e2e)
-    for s in range(ns):
-        base = row_host.data_ptr() + s * row_blocks * es
-        check(lib().nedy_gf_download(G[s].h, LES, T_e * (T_e + 1) // 2, T_e + 1, C.c_void_p(base)))
-        check(lib().nedy_gf_download(G[s].h, RET, T_e * (T_e + 1) // 2, T_e + 1,
-                                     C.c_void_p(base + (T_e + 1) * es)))
-        check(lib().nedy_gf_download(G[s].h, TV, T_e * (ntau + 1), ntau + 1,
-                                     C.c_void_p(base + 2 * (T_e + 1) * es)))
+    for i, t in enumerate(T_timed):
+        for s in range(ns):
+            check(lib().nedy_buf_upload(ht_e2e[s].h, 0, es, C.c_void_p(h_host.data_ptr() + (i * ns + s) * es)))
+            h2d += es
+        step_tol(t, args.tol, ht_e2e)
+        for s in range(ns):
+            base = row_host.data_ptr() + s * row_blocks * es
+            check(lib().nedy_gf_download(G[s].h, LES, t * (t + 1) // 2, t + 1, C.c_void_p(base)))
+            check(lib().nedy_gf_download(G[s].h, RET, t * (t + 1) // 2, t + 1, C.c_void_p(base + (t + 1) * es)))
+            check(lib().nedy_gf_download(G[s].h, TV, t * (ntau + 1), ntau + 1,
+                                         C.c_void_p(base + 2 * (t + 1) * es)))
+            d2h += (2 * (t + 1) + ntau + 1) * es
     ee1.record(stream)
     torch.cuda.synchronize(dev)
     dist.barrier()
     e2e_secs = dist.max(ee0.elapsed_time(ee1) / 1e3)
-    h2d = ns * es
-    d2h = ns * (2 * (T_e + 1) + ntau + 1) * es
-    torch.cuda.synchronize(dev)
-    pstats = ctx.predictor_stats() if pred is not None else None
     rep = C.create_string_buffer(16384)
     check(lib().nedy_split_tune_report(rep, 16384))
     tune = [x for x in rep.value.decode().split(";") if x]
-    return dict(plain=plain, split=split, split_iters=split_iters, max_dg=max_dg, err=err, max_g=max_g, T=T_timed,
-                e2e_secs=e2e_secs, h2d=h2d, d2h=d2h, prep=prep, pred_info=pred_info, pred_stats=pstats, tune=tune,
-                mu=list(mus))
+    return dict(forms=forms, errs=errs, max_g=max_g, T=T_timed, Kc=Kc, e2e_secs=e2e_secs, h2d=h2d // K,
+                d2h=d2h // K, prep=prep, pred_info=pred_info, pred_stats=pstats, tune=tune, mu=list(mus))
 
 
 def train_predictor(ctx, args):
@@ -584,28 +673,40 @@ def main():
             "spin-unrestricted density-fitted GF2 time step (both spins, independent h0 per spin, same B^Q)")
     cfg = {"workload": f"{kind}, nao={args.nao} naux={args.naux} ntau={args.ntau} "
                        f"beta={args.beta} k=5 dt={args.dt}, steps T={args.t0 + W}..{args.t0 + W + K - 1} on a "
-                       f"pre-evolved {args.state} state; plain form {args.corr} corrector iterations in FP64, split form "
-                       f"split-precision self-energy with the residual exit at {args.tol:g} (at most {args.corr})",
-           "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "nspin": 1 if args.restricted else 2, "t_window": [args.t0 + W, args.t0 + W + K - 1],
-           "corr_steps": args.corr, "precision": "fp64", "predictor": "polynomial extrapolation (k=5)",
-           "l2": "inputs (G, Sigma histories) larger than L2; no flush needed",
+                       f"pre-evolved {args.state} state",
+           "nao": args.nao, "naux": args.naux, "ntau": args.ntau, "nspin": 1 if args.restricted else 2,
+           "t_window": [args.t0 + W, args.t0 + W + K - 1], "corr_steps": args.corr,
+           "l2": "inputs (G, Sigma histories, GBs) larger than L2; no flush needed",
            "parallelism": f"replicas x{dist.world}"}
+    T_ref = args.t0 + W  # the first step of the window
     if args.impl == "reference":
         if dist.rank != 0:
             dist.close()
             return
-        samples = []
-        for i in range(W + K):
-            smp = cpu_sample(args)
-            if i >= W:
-                samples.append(smp)
-        T_mid = args.t0 + W
-        step_s = float(np.mean([cpu_step_seconds(s, T_mid, args) for s in samples]))
-        value = 1.0 / step_s
+        # One complete corrector iteration of the plain step at the window's first T, measured
+        # in K parts (one part per step; the W warm-up steps run parts untimed first).  A time
+        # step is CorrSteps such iterations, so timesteps/s = 1 / (CorrSteps x iteration time).
+        it = CpuIteration(args, T_ref)
+        parts = it.parts(K)
+        for i in range(W):
+            it.run_part(parts[i % K])
+        secs = [it.run_part(pt) for pt in parts]
+        t_iter = float(sum(secs))
+        value = 1.0 / (args.corr * t_iter)
+        sample = (f"oracle (C++ restatement of the reference, OpenMP over slices, OpenBLAS) on {it.cores} threads: "
+                  f"one complete corrector iteration of the plain {'unrestricted' if it.ns == 2 else 'restricted'} "
+                  f"step at T={T_ref}, ntau={args.ntau}, nao={args.nao}, naux={args.naux} (self-energy rows of "
+                  f"{'both spins' if it.ns == 2 else 'the row'}: {it.njobs} slices, mean field, {it.ns} Dyson "
+                  f"step{'s' if it.ns == 2 else ''}) measured in {K} parts, {t_iter:.1f} s; one time step = "
+                  f"{args.corr} iterations (CorrSteps); each bench step is one part")
+        cfg["precision"] = "fp64 (the reference's arithmetic)"
+        cfg["predictor"] = f"polynomial extrapolation (k=5), {args.corr} corrector iterations"
         line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": 0, "steps": K, "warmup": W,
-                "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "complex128", "data": "synthetic (seeded)", "config": cfg, "impl": "reference",
-                "cpu_baseline": cpu_baseline_obj(samples[-1], value, args),
+                "ms_per_step": float(np.mean(secs)) * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded)", "config": cfg,
+                "impl": "reference", "full_step_ms": args.corr * t_iter * 1e3,
+                "iteration_parts_s": secs,
+                "cpu_baseline": cpu_baseline_obj(value, it.cores, sample),
                 "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         dist.close()
@@ -613,39 +714,37 @@ def main():
 
     fp64 = fp64_gemm_peak(dist.local) if dist.rank == 0 else None
     r = run_engine(args, dist)
-    sp, pl = r["split"], r["plain"]
-    value = replica_value(K, dist.world, sp["secs"])
-    plain_value = replica_value(K, dist.world, pl["secs"]) if pl else None
-    T_mid = r["T"][len(r["T"]) // 2]
+    fm = r["forms"]
+    head = fm["split_learned_exit"]
+    value = replica_value(K, dist.world, head["secs"])
     peaks, src = measured_peaks()
     cfg["precision"] = ({"bf16x2": "split self-energy, two BF16 pieces per operand, products hi*hi + hi*lo + lo*hi",
                          "bf16x3": "split self-energy, three BF16 pieces per operand, six products"}[args.split_mode] +
-                        " (tcgen05, FP32 accumulation), FP64 Dyson/HF/density; plain form FP64 throughout")
+                        " (tcgen05, FP32 accumulation), FP64 Dyson/HF/density/residual")
     cfg["predictor"] = ("learned MLP correction of the k=5 extrapolation (polynomial fallback)" if args.predictor == "learned"
-                        else "polynomial extrapolation (k=5)") + " + residual exit at max|dG| estimate <= tol"
+                        else "polynomial extrapolation (k=5)") + f" + residual exit at tol={args.tol:g} (at most {args.corr} iterations)"
     cfg["state"] = (f"GF2 trajectory from the {'restricted' if args.restricted else 'unrestricted'} HF equilibrium "
                     "(Gaussian pulse E0=0.05 t0=2 sigma=0.5)"
                     if args.state == "trajectory" else "synthetic free-propagation history, 0.1 sin(2t) drive")
     cfg["tol"] = args.tol
+    cfg["warmup"] = f"{W} steps of the headline form (T={args.t0}..{args.t0 + W - 1}); every form starts from them"
     line = {"metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": dist.world, "steps": K, "warmup": W,
-            "ms_per_step": sp["secs"] / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": head["secs"] / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "complex128 state; self-energy contractions in BF16 pieces with FP32 accumulation",
             "data": ("synthetic (seeded random h0, B^Q, dipole); state: " + cfg["state"]), "config": cfg}
     if dist.rank == 0:
         # dominant kernel of the headline form: the split GEMM (BF16 piece products on tcgen05);
         # achieved = algorithmic BF16 pipe FLOPs / its summed device time (CUDA events per launch)
         bf16_peak = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
-        ach = sp["split_flops"] / (sp["split_ms"] / 1e3) / 1e12 if sp.get("split_ms") else None
-        sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau, 1 if args.restricted else 2)
-                        for t in r["T"]) * args.corr
+        ach = head["split_flops"] / (head["split_ms"] / 1e3) / 1e12 if head.get("split_ms") else None
         peak_key = "bf16_tflops_sustained" if peaks.get("bf16_tflops_sustained") else "bf16_tflops"
+        nsp = 1 if args.restricted else 2
         # DRAM traffic of the split GEMMs per step: bytes per exchange unit (one slice of one
         # spin; dram__bytes_read.sum + dram__bytes_write.sum of every split GEMM class, ncu
-        # capture of the nao=64, naux=256, ntau=32 case with two pieces per operand, S' and Q
-        # dominating at 134 MB and 192 MB) times the units of the step (les, tv and ret slices)
-        ns = 1 if args.restricted else 2
-        units = sum(ns * (2 * (t + 1) + args.ntau + 1) * it for t, it in zip(r["T"], r["split_iters"])) / K
-        per_unit = 3.6e8 if (args.nao, args.naux, args.split_mode) == (64, 256, "bf16x2") else None
+        # capture of the nao=64, naux=256, ntau=32 case with two pieces per operand) times the
+        # units of the step (les, tv and ret slices times the iterations)
+        units = sum(nsp * (2 * (t + 1) + args.ntau + 1) * it for t, it in zip(r["T"], head["iters"])) / K
+        per_unit = SPLIT_TRAFFIC_PER_UNIT if (args.nao, args.naux, args.split_mode) == (64, 256, "bf16x2") else None
         line["roofline"] = {"bound": "tensor", "kernel": "split_gemm_kernel (BF16 piece products, tcgen05, TMEM)",
                             "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
                             "frac": (ach / bf16_peak) if ach else None,
@@ -653,33 +752,59 @@ def main():
                             "traffic_unit": "bytes per step (DRAM, all split GEMM launches of one step)",
                             "exchange_units_per_step": units,
                             "peak_source": f"{src}: {peak_key} (kernel timed inside a long step)",
-                            "algorithmic_flops_per_step": sp["split_flops"] / K,
-                            "kernel_ms_per_step": sp["split_ms"] / K}
-        line["forms"] = {
-            "split_predictor": {"timesteps_s": value, "ms_per_step": sp["secs"] / K * 1e3,
-                                "iterations_per_step": r["split_iters"],
-                                "phase_ms": dict(zip(["predictor", "mean_field", "self_energy", "dyson"], sp["phase_ms"])),
-                                "gpu_launches": sp["launches"]},
-            "plain_fp64": {"timesteps_s": plain_value, "ms_per_step": pl["secs"] / K * 1e3,
-                           "iterations_per_step": args.corr,
-                           "phase_ms": dict(zip(["predictor", "mean_field", "self_energy", "dyson"], pl["phase_ms"])),
-                           "gpu_launches": pl["launches"],
-                           "self_energy_fp64_tflops": sig_flops / (pl["phase_ms"][2] / 1e3) / 1e12,
-                           "fp64_peak_tflops": fp64} if pl else None,
-            "state_preparation": r["prep"], "predictor_training": r["pred_info"],
-            "predictor_stats": r["pred_stats"], "split_tile_autotune": r["tune"],
-            "speedup_split_vs_plain": value / plain_value if pl else None,
-            "max_abs_dG_split_vs_plain": r["max_dg"], "error_vs_fp64_per_component": r["err"],
-            "max_abs_G": r["max_g"], "mu": r["mu"]}
-        line["clocks"] = sp["clocks"]
-        line["clocks_plain"] = pl["clocks"] if pl else None
-        line["gpu_launches"] = sp["launches"]
-        line["e2e"] = {"value": dist.world / r["e2e_secs"], "unit": "timesteps/s", "h2d_bytes_per_step": r["h2d"],
-                       "d2h_bytes_per_step": r["d2h"]}
+                            "algorithmic_flops_per_step": head["split_flops"] / K,
+                            "kernel_ms_per_step": head["split_ms"] / K}
+        Kc = r["Kc"]
+
+        def form_obj(f, name):
+            n = len(f["per_step_s"])
+            o = {"timesteps_s": n / f["secs"], "ms_per_step": f["secs"] / n * 1e3, "steps": n,
+                 "iterations_per_step": f["iters"], "mean_iterations": float(np.mean(f["iters"])),
+                 "phase_ms": dict(zip(["predictor", "mean_field", "self_energy", "dyson"], f["phase_ms"])),
+                 "gpu_launches": f["launches"],
+                 # the first Kc steps: the window every form ran
+                 "timesteps_s_first_steps": Kc / sum(f["per_step_s"][:Kc])}
+            if name in r["errs"]:
+                o["error_vs_plain_fp64"] = r["errs"][name]
+            return o
+
+        forms = {name: form_obj(f, name) for name, f in fm.items()}
+        if "plain_fp64" in fm:
+            pl = fm["plain_fp64"]
+            sig_flops = sum(flops_sigma(t, args.nao, args.naux, args.ntau, nsp) for t in r["T"][:Kc]) * args.corr
+            forms["plain_fp64"]["self_energy_fp64_tflops"] = sig_flops / (pl["phase_ms"][2] / 1e3) / 1e12
+            forms["plain_fp64"]["fp64_peak_tflops"] = fp64
+            base = forms["plain_fp64"]["timesteps_s_first_steps"]
+            for name in forms:
+                forms[name]["speedup_vs_plain_fp64"] = forms[name]["timesteps_s_first_steps"] / base
+            if "plain_fp64_exit" in forms:
+                bx = forms["plain_fp64_exit"]["timesteps_s_first_steps"]
+                for name in forms:
+                    forms[name]["speedup_vs_plain_fp64_exit"] = forms[name]["timesteps_s_first_steps"] / bx
+        line["forms"] = forms
+        line["forms_note"] = (f"every form runs the window from the same state (the {W} warm-up steps); the "
+                              f"plain FP64 forms and the error comparison cover the first {Kc} steps; "
+                              "speedups compare timesteps/s over those common steps; errors are max |G_form - "
+                              "G_plain_fp64| over the new rows of those steps (per component and spin) and "
+                              "|E_corr difference| per spin")
+        line["state_preparation"] = r["prep"]
+        line["predictor_training"] = r["pred_info"]
+        line["predictor_stats"] = r["pred_stats"]
+        line["split_tile_autotune"] = r["tune"]
+        line["max_abs_G"] = r["max_g"]
+        line["mu"] = r["mu"]
+        line["clocks"] = head["clocks"]
+        if "plain_fp64" in fm:
+            line["clocks_plain"] = fm["plain_fp64"]["clocks"]
+        line["gpu_launches"] = head["launches"]
+        line["e2e"] = {"value": replica_value(K, dist.world, r["e2e_secs"]), "unit": "timesteps/s",
+                       "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                       "what": "the headline form over the whole window again through the C ABI, each step copying "
+                               "h(t) of each spin in from pinned host memory and its new G rows out"}
         if dist.world == 1 and not args.no_cpu_baseline:
-            smp = cpu_sample(args)
-            v = 1.0 / cpu_step_seconds(smp, T_mid, args)
-            line["cpu_baseline"] = cpu_baseline_obj(smp, v, args)
+            it = CpuIteration(args, T_ref)
+            t_iter, desc = it.sample()
+            line["cpu_baseline"] = cpu_baseline_obj(1.0 / (args.corr * t_iter), it.cores, desc)
         print(json.dumps(line), flush=True)
     dist.close()
 

@@ -230,7 +230,7 @@ def free_history(nt: int, t_fill: int, ntau: int, x: np.ndarray, mu: float, F: n
     les = 1j * np.conj(np.transpose(Ud[tt - ss], (0, 2, 1))) @ fval   # les block (t', t): U(t'-t) f = U(t-t')^+ f
     taus = beta / 2.0 * (np.asarray(x) + 1.0)
     core = np.stack([(V * fermi_exp(beta, tau, -ev)) @ V.conj().T for tau in taus])
-    tv = 1j * np.einsum("nij,mjk->nmik", Ud, core)
+    tv = 1j * np.matmul(Ud[:, None], core[None])  # (t, m) -> U(t) e(tau_m), batched BLAS products
     mat = np.stack([-(V * fermi_exp(beta, tau, ev)) @ V.conj().T for tau in taus])
     return (scale * les).astype(np.complex128), (scale * ret).astype(np.complex128), \
         (scale * tv).astype(np.complex128), mat.astype(np.complex128)

@@ -111,6 +111,12 @@ void orc_df_solve_loop(void *s, int tstp, const orc_gf *Sig, const orc_gf *G) {
 void orc_df_solve_spin(void *s, int tstp, const orc_gf *Sig, const orc_gf *G) {
   static_cast<DFSolver *>(s)->solve_spin(tstp, &G_(Sig), &G_(G));
 }
+void orc_df_solve_jobs(void *s, int tstp, const orc_gf *Sig, const orc_gf *G, int job_lo, int job_hi) {
+  static_cast<DFSolver *>(s)->solve_jobs(tstp, G_(Sig), G_(G), job_lo, job_hi);
+}
+void orc_df_solve_spin_jobs(void *s, int tstp, const orc_gf *Sig, const orc_gf *G, int job_lo, int job_hi) {
+  static_cast<DFSolver *>(s)->solve_spin_jobs(tstp, &G_(Sig), &G_(G), job_lo, job_hi);
+}
 void orc_df_solve_spin_loop(void *s, int tstp, const orc_gf *Sig, const orc_gf *G) {
   static_cast<DFSolver *>(s)->solve_spin_loop(tstp, &G_(Sig), &G_(G));
 }

@@ -12,8 +12,12 @@ struct DFSolver {
   std::vector<double> Vija_, Viaj_;
   std::vector<cplx> VijaC_, ViajC_;
   void solve(int tstp, const GF &Sig, const GF &G) const;
+  // slices [job_lo, job_hi) of the restricted row (lesser t, retarded t, mixed tau), not zeroed first
+  void solve_jobs(int tstp, const GF &Sig, const GF &G, int job_lo, int job_hi) const;
   void solve_loop(int tstp, const GF &Sig, const GF &G) const;
   void solve_spin(int tstp, const GF *Sig, const GF *G) const;       // Sig[2], G[2]
+  // slices [job_lo, job_hi) of the unrestricted row, Sigma not zeroed first
+  void solve_spin_jobs(int tstp, const GF *Sig, const GF *G, int job_lo, int job_hi) const;
   void solve_spin_loop(int tstp, const GF *Sig, const GF *G) const;
 };
 

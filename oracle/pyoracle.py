@@ -72,6 +72,7 @@ def lib():
         "orc_df_new": ([I, I, P, P], P), "orc_df_free": ([P], None),
         "orc_df_solve": ([P, I, P, P], None), "orc_df_solve_loop": ([P, I, P, P], None),
         "orc_df_solve_spin": ([P, I, P, P], None), "orc_df_solve_spin_loop": ([P, I, P, P], None),
+        "orc_df_solve_spin_jobs": ([P, I, P, P, I, I], None), "orc_df_solve_jobs": ([P, I, P, P, I, I], None),
         "orc_full_new": ([I, P, P], P), "orc_full_free": ([P], None),
         "orc_full_solve": ([P, I, P, P], None), "orc_full_solve_loop": ([P, I, P, P], None),
         "orc_hf_decomp": ([I, I, P, P, P], None), "orc_hf_decomp_loop": ([I, I, P, P, P], None),
@@ -229,6 +230,16 @@ class DF:
 
     def solve_spin(self, tstp, Sig2, G2):
         lib().orc_df_solve_spin(self.h, tstp, gf_pair(*Sig2), gf_pair(*G2))
+
+    def solve_jobs(self, tstp, Sig, G, job_lo, job_hi):
+        """Slices [job_lo, job_hi) of the restricted row T (lesser t, then retarded t, then mixed
+        tau); Sigma is not zeroed first."""
+        lib().orc_df_solve_jobs(self.h, tstp, C.byref(gf(Sig)), C.byref(gf(G)), int(job_lo), int(job_hi))
+
+    def solve_spin_jobs(self, tstp, Sig2, G2, job_lo, job_hi):
+        """Slices [job_lo, job_hi) of the unrestricted row T (lesser t, then retarded t, then
+        mixed tau; both spins per slice); Sigma is not zeroed first."""
+        lib().orc_df_solve_spin_jobs(self.h, tstp, gf_pair(*Sig2), gf_pair(*G2), int(job_lo), int(job_hi))
 
     def solve_spin_loop(self, tstp, Sig2, G2):
         lib().orc_df_solve_spin_loop(self.h, tstp, gf_pair(*Sig2), gf_pair(*G2))

@@ -11,6 +11,7 @@
 // Slices (t' or tau) are independent and run on OpenMP threads.
 #include "oracle_sigma.h"
 #include <omp.h>
+#include <algorithm>
 
 namespace orc {
 
@@ -147,14 +148,21 @@ static void tv_back(int n, const cplx *Gvt, int sig, cplx *out) {  // -sig conj(
 // mol2bSolver_decomp_impl.h:412-429
 void DFSolver::solve(int tstp, const GF &Sig, const GF &G) const {
   Sig.set_tstp_zero(tstp);
+  solve_jobs(tstp, Sig, G, 0, 2 * (tstp + 1) + G.ntau + 1);
+}
+
+// Slices job_lo .. job_hi-1 of the restricted row, numbered as in solve_spin_jobs.
+void DFSolver::solve_jobs(int tstp, const GF &Sig, const GF &G, int job_lo, int job_hi) const {
   int n = nao_, ntau = G.ntau, sig = G.sig;
   int nles = tstp + 1, ntv = ntau + 1;
+  job_lo = std::max(0, job_lo);
+  job_hi = std::min(2 * nles + ntv, job_hi);
 #pragma omp parallel
   {
     DFScratch w(n, naux_, 1);
     std::vector<cplx> gb((size_t)n * n);
 #pragma omp for schedule(dynamic)
-    for (int job = 0; job < 2 * nles + ntv; job++) {
+    for (int job = job_lo; job < job_hi; job++) {
       if (job < nles) {
         int t = job;
         les_back(n, G.lesptr(t, tstp), G.retptr(tstp, t), gb.data());
@@ -284,14 +292,24 @@ static void sdf_bubble_ret(const DFSolver &s, const cplx *L[2], const cplx *R[2]
 void DFSolver::solve_spin(int tstp, const GF *Sig, const GF *G) const {
   Sig[0].set_tstp_zero(tstp);
   Sig[1].set_tstp_zero(tstp);
+  solve_spin_jobs(tstp, Sig, G, 0, 2 * (tstp + 1) + G[0].ntau + 1);
+}
+
+// Slices job_lo .. job_hi-1 of the unrestricted row (both spins of one slice per job):
+// jobs [0, tstp] lesser slices t, [tstp+1, 2 tstp+1] retarded slices, then the ntau+1
+// mixed slices.  Every slice is an independent piece of the reference's row
+// (mol2bSolver_spin_decomp_impl.h:436-466), so a row can be computed -- or timed -- in parts.
+void DFSolver::solve_spin_jobs(int tstp, const GF *Sig, const GF *G, int job_lo, int job_hi) const {
   int n = nao_, ntau = G[0].ntau, sig = G[0].sig;
   int nles = tstp + 1, ntv = ntau + 1;
+  job_lo = std::max(0, job_lo);
+  job_hi = std::min(2 * nles + ntv, job_hi);
 #pragma omp parallel
   {
     DFScratch w(n, naux_, 2);
     std::vector<cplx> gb0((size_t)n * n), gb1((size_t)n * n);
 #pragma omp for schedule(dynamic)
-    for (int job = 0; job < 2 * nles + ntv; job++) {
+    for (int job = job_lo; job < job_hi; job++) {
       if (job < nles) {
         int t = job;
         const cplx *Gf[2] = {G[0].lesptr(t, tstp), G[1].lesptr(t, tstp)};

@@ -9,8 +9,10 @@ It writes, next to this script:
 
 * calccoeff.json  -- the calculus-weight tables stored by the reference in
   tests/data/calccoeff.h5 (datasets PInterp, PDiff, PInteg, BD, Start, Sigma, w),
-  read with the small HDF5 reader below (superblock v0, symbol-table groups,
-  contiguous or compact datasets of little-endian float64 -- all this file uses).
+  read with the package's HDF5 reader (nedyson_b200/h5io.py).
+* gfree_const.json -- the free propagator G0_from_h0 of the reference's free-test
+  (tests/data/Gfree_const.h5, tests/free-test.cpp:8-42): the first k+1 time steps of
+  GR, GL, GTV and the Matsubara component.
 * integrals.json  -- the known-answer values of tests/integrals-test.cpp:8-212
   (energy_conv, CTV1, Ctv_tstp, Cles2_tstp, Cles3_tstp), parsed from the test
   source, with the time step each value belongs to and its tolerance.
@@ -20,120 +22,16 @@ Nothing at test time reads the reference tree; only these JSON files.
 import json
 import os
 import re
-import struct
+import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = None  # the reference checkout, from the command line or NEDY_REFERENCE (see main)
 
 
-# ---------------------------------------------------------------- HDF5 (tiny)
-class H5:
-    def __init__(self, path):
-        self.d = open(path, "rb").read()
-        assert self.d[:8] == b"\x89HDF\r\n\x1a\n", "not an HDF5 file"
-        assert self.d[8] == 0, "only superblock version 0 is handled"
-        self.so = self.d[13]  # size of offsets
-        self.sl = self.d[14]  # size of lengths
-        # root symbol table entry follows base/freespace/eof/driver addresses
-        p = 24 + 4 * self.so
-        self.root = self._entry(p)
-
-    def _u(self, p, n):
-        return int.from_bytes(self.d[p:p + n], "little")
-
-    def _entry(self, p):
-        name_off = self._u(p, self.so)
-        hdr = self._u(p + self.so, self.so)
-        ctype = self._u(p + 2 * self.so, 4)
-        scratch = p + 2 * self.so + 8
-        btree = heap = None
-        if ctype == 1:
-            btree = self._u(scratch, self.so)
-            heap = self._u(scratch + self.so, self.so)
-        return dict(name_off=name_off, hdr=hdr, btree=btree, heap=heap)
-
-    def _heap_data(self, heap):
-        assert self.d[heap:heap + 4] == b"HEAP"
-        return self._u(heap + 8 + 2 * self.sl, self.so)
-
-    def _name(self, heap_data, off):
-        e = self.d.index(b"\x00", heap_data + off)
-        return self.d[heap_data + off:e].decode()
-
-    def _symbols(self, btree, heap):
-        hd = self._heap_data(heap)
-        out = {}
-        stack = [btree]
-        while stack:
-            node = stack.pop()
-            assert self.d[node:node + 4] == b"TREE"
-            level = self.d[node + 5]
-            used = self._u(node + 6, 2)
-            p = node + 8 + 2 * self.so
-            children = []
-            for i in range(used):
-                p += self.sl  # key
-                children.append(self._u(p, self.so))
-                p += self.so
-            if level > 0:
-                stack.extend(children)
-                continue
-            for snod in children:
-                assert self.d[snod:snod + 4] == b"SNOD"
-                nsym = self._u(snod + 6, 2)
-                q = snod + 8
-                for _ in range(nsym):
-                    ent = self._entry(q)
-                    out[self._name(hd, ent["name_off"])] = ent
-                    q += 2 * self.so + 8 + 16
-        return out
-
-    def datasets(self):
-        return {k: self.read(v["hdr"]) for k, v in self._symbols(self.root["btree"], self.root["heap"]).items()}
-
-    def read(self, hdr):
-        assert self.d[hdr] == 1, "object header v1 expected"
-        nmsg = self._u(hdr + 2, 2)
-        p = hdr + 16
-        dims, raw = None, None
-        left = nmsg
-        while left > 0:
-            mtype = self._u(p, 2)
-            msize = self._u(p + 2, 2)
-            body = p + 8
-            if mtype == 0x0001:  # dataspace
-                ver = self.d[body]
-                rank = self.d[body + 1]
-                q = body + (8 if ver == 1 else 4)
-                dims = [self._u(q + i * self.sl, self.sl) for i in range(rank)]
-            elif mtype == 0x0003:  # datatype: float64 little-endian only
-                cls = self.d[body] & 0x0F
-                size = self._u(body + 4, 4)
-                assert cls == 1 and size == 8, "float64 datasets only"
-            elif mtype == 0x0008:  # layout
-                ver = self.d[body]
-                assert ver == 3
-                lclass = self.d[body + 1]
-                if lclass == 0:
-                    n = self._u(body + 2, 2)
-                    raw = self.d[body + 4:body + 4 + n]
-                elif lclass == 1:
-                    addr = self._u(body + 2, self.so)
-                    n = self._u(body + 2 + self.so, self.sl)
-                    raw = self.d[addr:addr + n]
-                else:
-                    raise ValueError("chunked layout not handled")
-            elif mtype == 0x0010:  # continuation
-                addr = self._u(body, self.so)
-                p = addr
-                left -= 1
-                continue
-            p = body + msize
-            left -= 1
-        n = 1
-        for x in dims or [len(raw) // 8]:
-            n *= x
-        return list(struct.unpack("<%dd" % n, raw[:8 * n]))
+# ---------------------------------------------------------------- HDF5
+# the package's reader (superblock v0, symbol-table groups, contiguous / compact data)
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from nedyson_b200.h5io import H5File  # noqa: E402
 
 
 # ----------------------------------------------------------- integrals goldens
@@ -173,9 +71,9 @@ def main():
     REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NEDY_REFERENCE")
     if not REF:
         sys.exit("usage: make_golden.py <path-to-NEdyson-checkout>  (or set NEDY_REFERENCE)")
-    h5 = H5(os.path.join(REF, "tests/data/calccoeff.h5"))
-    ds = h5.datasets()
-    keep = {k: ds[k] for k in ("PInterp", "PDiff", "PInteg", "BD", "Start", "Sigma", "w") if k in ds}
+    h5 = H5File(os.path.join(REF, "tests/data/calccoeff.h5"))
+    keep = {k: [float(v) for v in h5["/" + k]] for k in ("PInterp", "PDiff", "PInteg", "BD", "Start", "Sigma", "w")
+            if "/" + k in h5}
     keep["_source"] = "reference tests/data/calccoeff.h5 (k=5), checked at tests/integration-test.cpp:5-69"
     with open(os.path.join(HERE, "calccoeff.json"), "w") as f:
         json.dump(keep, f, indent=1)
@@ -183,6 +81,22 @@ def main():
     ints["_source"] = "reference tests/integrals-test.cpp:8-212 with fixtures tests/set_up_g.h:13-242"
     with open(os.path.join(HERE, "integrals.json"), "w") as f:
         json.dump(ints, f, indent=1)
+    # free propagator of a constant h0 (reference tests/free-test.cpp:8-42): G0_from_h0 with
+    # Nt=20, Ntau=30, nao=2, beta=9, dt=0.1, mu=1, h0 = [[1, -3], [-3, 2]]; the test compares
+    # the first k+1 = 6 time steps and the Matsubara component
+    fr = H5File(os.path.join(REF, "tests/data/Gfree_const.h5"))
+    nao, ntau = 2, 30
+    es, nk = nao * nao, 6
+    tri = nk * (nk + 1) // 2
+    cut = {"GR": tri * es, "GL": tri * es, "GTV": nk * (ntau + 1) * es, "GM": (ntau + 1) * es}
+    gfree = {"_source": "reference tests/data/Gfree_const.h5, checked at tests/free-test.cpp:8-42",
+             "Nt": 20, "Ntau": ntau, "nao": nao, "beta": 9.0, "dt": 0.1, "mu": 1.0, "h0": [[1.0, -3.0], [-3.0, 2.0]],
+             "k": 5, "tol_norm": 1e-10}
+    for k, n in cut.items():
+        v = fr["/" + k][:n]
+        gfree[k] = [[float(z.real), float(z.imag)] for z in v]
+    with open(os.path.join(HERE, "gfree_const.json"), "w") as f:
+        json.dump(gfree, f, indent=0)
     print({k: len(v) for k, v in keep.items() if isinstance(v, list)},
           {k: len(v) for k, v in ints["cases"].items()})
 

@@ -157,3 +157,35 @@ def test_uhf_equilibrium_with_equal_spins_is_rhf():
     F, mu = hf_equilibrium(q, 10.0)
     assert np.abs(Fu - F).max() < 1e-10 and np.abs(Fd - F).max() < 1e-10
     assert abs(mu_u - mu) < 1e-10 and abs(mu_d - mu) < 1e-10
+
+
+def test_row_in_parts_equals_whole_row():
+    """The job-range solves (used to time the CPU iteration in bounded parts) compute exactly the
+    slices of the whole-row solve."""
+    from nedyson_b200.greens import HostGF
+    rng = np.random.default_rng(77)
+    nao, naux, nt, ntau = 4, 7, 5, 6
+    V = rng.uniform(-1, 1, (nao, nao, naux))
+    df = po.DF(V)
+    G = []
+    for _ in range(2):
+        g = HostGF(nt, ntau, nao, -1)
+        for a in (g.les, g.ret, g.tv, g.mat):
+            a[:] = rng.uniform(-1, 1, a.shape) + 1j * rng.uniform(-1, 1, a.shape)
+        G.append(g)
+    T = 4
+    njobs = 2 * (T + 1) + ntau + 1
+    whole = [HostGF(nt, ntau, nao, -1) for _ in range(2)]
+    parts = [HostGF(nt, ntau, nao, -1) for _ in range(2)]
+    df.solve_spin(T, whole, G)
+    for lo, hi in ((0, 3), (3, 11), (11, njobs)):
+        df.solve_spin_jobs(T, parts, G, lo, hi)
+    for a, b in zip(parts, whole):
+        for comp in ("les", "ret", "tv"):
+            assert np.array_equal(getattr(a, comp), getattr(b, comp)), comp
+    w1, p1 = HostGF(nt, ntau, nao, -1), HostGF(nt, ntau, nao, -1)
+    df.solve(T, w1, G[0])
+    df.solve_jobs(T, p1, G[0], 0, 5)
+    df.solve_jobs(T, p1, G[0], 5, njobs)
+    for comp in ("les", "ret", "tv"):
+        assert np.array_equal(getattr(p1, comp), getattr(w1, comp)), comp
