@@ -274,6 +274,30 @@ int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn,
                           nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
                           double mu_up, double mu_dn, int corr_steps, double *err);
 
+/* --- Batched independent simulations (many molecules or fields of uneven nao; no
+ * counterpart in the reference, which steps one DecompSimulation at a time,
+ * src/molNEsim_decomp_impl.h:85-104).  Each instance keeps its own context (stream,
+ * workspace), G, Sigma, mean-field buffer and the one-body Hamiltonians h(t) of all steps
+ * (h_all: (nt+1) x nao x nao complex; hmf the same size).  nedy_batch_tstp runs the step
+ * of every instance: a pool of native worker threads (workers <= 0: up to 16) takes the
+ * instances largest nao first and issues each step on its instance's stream, so the
+ * instances' kernels run concurrently.  tol = 0: corr_steps iterations per instance
+ * (nedy_decomp_tstp); tol > 0: the residual exit of nedy_decomp_tstp_tol with at most
+ * corr_steps.  iters (optional, n entries) receives the iterations of each instance.
+ * On an error the remaining instances are not started and the first failing instance
+ * is named in nedy_last_error. */
+typedef struct nedy_batch nedy_batch;
+typedef struct {
+  nedy_ctx *ctx;
+  nedy_gf *G, *Sigma;
+  nedy_buf *hmf;
+  const nedy_buf *h_all;
+  double mu;
+} nedy_batch_instance;
+int nedy_batch_create(const nedy_batch_instance *inst, int n, int workers, nedy_batch **out);
+int nedy_batch_destroy(nedy_batch *b);
+int nedy_batch_tstp(nedy_batch *b, int tstp, int corr_steps, double tol, int *iters);
+
 #ifdef __cplusplus
 }
 #endif

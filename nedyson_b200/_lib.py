@@ -22,6 +22,11 @@ class NedyConfig(C.Structure):
                 ("workspace_bytes", C.c_longlong)]
 
 
+class BatchInstance(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("G", C.c_void_p), ("Sigma", C.c_void_p), ("hmf", C.c_void_p),
+                ("h_all", C.c_void_p), ("mu", C.c_double)]
+
+
 class NedyError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"nedy status {status}: {msg}")
@@ -94,6 +99,9 @@ SIGNATURES = {
     "nedy_energy_conv": ([_P, _I, _P, _P, _DP], _I),
     "nedy_decomp_tstp": ([_P, _I, _P, _P, _P, _P, _D, _I, _DP], _I),
     "nedy_full_tstp": ([_P, _I, _P, _P, _P, _P, _D, _I, _DP], _I),
+    "nedy_batch_create": ([C.POINTER(BatchInstance), _I, _I, _PP], _I),
+    "nedy_batch_destroy": ([_P], _I),
+    "nedy_batch_tstp": ([_P, _I, _I, _D, C.POINTER(_I)], _I),
     "nedy_decomp_spin_tstp": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I, _DP], _I),
 }
 

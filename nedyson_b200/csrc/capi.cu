@@ -12,7 +12,7 @@ using namespace nedy;
 
 namespace nedy {
 
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 // Optional per-phase device timing of the whole-step entry points (CUDA events
 // on the engine stream): predictor, mean field, self-energy, Dyson step.
@@ -380,7 +380,7 @@ int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4) {
   });
 }
 
-unsigned long long nedy_launch_count(void) { return g_launches; }
+unsigned long long nedy_launch_count(void) { return g_launches.load(); }
 
 int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w) {
   return guard([&] {
@@ -726,12 +726,23 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
                      double mu, int corr_steps, double *err) {
   return guard([&] {
     NEDY_REQUIRE(ctx && G && S && hmf && h_t, "null argument");
+    NEDY_REQUIRE(h_t->bytes >= G->g.es * 16, "h_t buffer too small");
+    decomp_step_fixed(ctx, tstp, G, S, hmf, (const double2 *)h_t->p, mu, corr_steps, err);
+  });
+}
+
+} // extern "C"
+
+// DecompSimulation::do_tstp (src/molNEsim_decomp_impl.h:85-104) with h_t a device pointer.
+void nedy::decomp_step_fixed(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const double2 *h_t,
+                             double mu, int corr_steps, double *err) {
+  {
+    NEDY_REQUIRE(ctx && G && S && hmf && h_t, "null argument");
     NEDY_REQUIRE(corr_steps >= 1, "corr_steps must be >= 1");
     set_dev(ctx);
     Ctx &c = ctx->c;
     const int N = G->g.nao;
     const i64 es = (i64)N * N;
-    NEDY_REQUIRE(h_t->bytes >= es * 16, "h_t buffer too small");
     double2 *hT = hmf_row(hmf, ctx, tstp, N);
     hmf_row(hmf, ctx, G->g.nt, N);
     PhaseTimer pt(c);
@@ -743,7 +754,7 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
       pt.mark(1);
       double2 *rho = c.ws.alloc<double2>(es);
       get_dm(c, G->g, tstp, rho);
-      NEDY_CUDA(cudaMemcpyAsync(hT, h_t->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      NEDY_CUDA(cudaMemcpyAsync(hT, h_t, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
       double2 *h[1] = {hT};
       hf_decomp(c, 1, h, rho);
       DevGF *Ss[1] = {&S->g};
@@ -757,8 +768,10 @@ int nedy_decomp_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *
     NEDY_CUDA(cudaStreamSynchronize(c.stream));
     pt.collect();
     if (err) *err = e[0] + e[1] + e[2];
-  });
+  }
 }
+
+extern "C" {
 
 int nedy_full_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const nedy_buf *h_t, double mu,
                    int corr_steps, double *err) {
@@ -798,14 +811,15 @@ int nedy_full_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hm
 
 } // extern "C"
 
-namespace {
+namespace nedy {
 // One time step with the residual exit for one (restricted) or two (unrestricted) spins.
 // After iteration k the change d_k = max over the spins' new rows of |G_k - G_{k-1}| is
 // measured; the step stops once d_k times the corrector's contraction is <= tol.  The
 // contraction is measured (4 x the ratio of successive changes) on steps that run two or
 // more iterations: the first step of a context, and every 8th after, run at least two.
+// h_t[s]: device pointer to the nao x nao one-body Hamiltonian of spin s at tstp.
 void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *const *S, nedy_buf *const *hmf,
-              const nedy_buf *const *h_t, const double *mu, int max_corr, double tol, int *iters, double *err_hist) {
+              const double2 *const *h_t, const double *mu, int max_corr, double tol, int *iters, double *err_hist) {
   NEDY_REQUIRE(max_corr >= 1 && tol >= 0.0, "max_corr must be >= 1 and tol >= 0");
   for (int s = 0; s < nspin; s++) NEDY_REQUIRE(G[s] && S[s] && hmf[s] && h_t[s], "null argument");
   set_dev(ctx);
@@ -814,7 +828,7 @@ void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *co
   const i64 es = (i64)N * N;
   double2 *hT[2];
   for (int s = 0; s < nspin; s++) {
-    NEDY_REQUIRE(G[s]->g.nao == N && h_t[s]->bytes >= es * 16, "h_t buffer too small or nao mismatch");
+    NEDY_REQUIRE(G[s]->g.nao == N, "nao mismatch between the spins");
     hT[s] = hmf_row(hmf[s], ctx, tstp, N);
     hmf_row(hmf[s], ctx, G[s]->g.nt, N);
   }
@@ -843,7 +857,7 @@ void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *co
     double2 *rho = c.ws.alloc<double2>(nspin * es);
     for (int s = 0; s < nspin; s++) {
       get_dm(c, G[s]->g, tstp, rho + s * es);
-      NEDY_CUDA(cudaMemcpyAsync(hT[s], h_t[s]->p, sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
+      NEDY_CUDA(cudaMemcpyAsync(hT[s], h_t[s], sizeof(double2) * es, cudaMemcpyDeviceToDevice, c.stream));
     }
     hf_decomp(c, nspin, hT, rho);
     DevGF *Ss[2] = {&S[0]->g, nspin > 1 ? &S[1]->g : nullptr};
@@ -894,7 +908,7 @@ void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *co
   pt.collect();
   if (iters) *iters = it;
 }
-}  // namespace
+}  // namespace nedy
 
 extern "C" {
 
@@ -902,9 +916,10 @@ int nedy_decomp_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_b
                          double mu, int max_corr, double tol, int *iters, double *err_hist) {
   return guard([&] {
     NEDY_REQUIRE(ctx, "null argument");
+    NEDY_REQUIRE(G && h_t && h_t->bytes >= G->g.es * 16, "null argument or h_t buffer too small");
     nedy_gf *Gs[1] = {G}, *Ss[1] = {S};
     nedy_buf *hs[1] = {hmf};
-    const nedy_buf *hts[1] = {h_t};
+    const double2 *hts[1] = {(const double2 *)h_t->p};
     step_tol(ctx, tstp, 1, Gs, Ss, hs, hts, &mu, max_corr, tol, iters, err_hist);
   });
 }
@@ -914,9 +929,11 @@ int nedy_decomp_spin_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G
                               double mu_up, double mu_dn, int max_corr, double tol, int *iters, double *err_hist) {
   return guard([&] {
     NEDY_REQUIRE(ctx, "null argument");
+    NEDY_REQUIRE(G_up && G_dn && h_t_up && h_t_dn, "null argument");
+    NEDY_REQUIRE(h_t_up->bytes >= G_up->g.es * 16 && h_t_dn->bytes >= G_dn->g.es * 16, "h_t buffer too small");
     nedy_gf *Gs[2] = {G_up, G_dn}, *Ss[2] = {S_up, S_dn};
     nedy_buf *hs[2] = {hmf_up, hmf_dn};
-    const nedy_buf *hts[2] = {h_t_up, h_t_dn};
+    const double2 *hts[2] = {(const double2 *)h_t_up->p, (const double2 *)h_t_dn->p};
     const double mus[2] = {mu_up, mu_dn};
     step_tol(ctx, tstp, 2, Gs, Ss, hs, hts, mus, max_corr, tol, iters, err_hist);
   });

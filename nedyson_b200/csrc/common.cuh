@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <string>
 #include <stdexcept>
+#include <atomic>
 
 namespace nedy {
 
@@ -27,7 +28,7 @@ struct ArgError : std::runtime_error {
 
 // Every kernel launch of the engine is followed by NEDY_CHECK_LAUNCH, which also
 // counts it (nedy_launch_count in the C ABI).
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 #define NEDY_CHECK_LAUNCH()                                                                    \
   do {                                                                                         \
     ++::nedy::g_launches;                                                                      \

@@ -995,10 +995,13 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
   }
   {
     const double wnn = c.W.gregory(n, n);
-    static int attr_set = 0;
-    if (!attr_set) {
+    static std::atomic<bool> attr_set[64];  // per device (host threads may race here)
+    int dev = 0;
+    NEDY_CUDA(cudaGetDevice(&dev));
+    NEDY_REQUIRE(dev < 64, "device index out of range");
+    if (!attr_set[dev].load()) {
       NEDY_CUDA(cudaFuncSetAttribute(les_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-      attr_set = 1;
+      attr_set[dev].store(true);
     }
     NEDY_REQUIRE(2 * es * (i64)sizeof(double2) <= 200 * 1024, "dyson_step: nao too large for the diagonal kernel");
     les_diag_kernel<<<1, 256, 2 * es * sizeof(double2), c.stream>>>(N, k, n, G, S, hmf, c.d_ex, c.d_bd, wnn, mu, dt,

@@ -281,12 +281,13 @@ DView dv(const View &v) {
 template <int BM, bool AC, bool BC>
 void launch(const Params &P, cudaStream_t s) {
   using SM = Smem<BM, AC, BC>;
-  static int attr_dev = -1;
+  static std::atomic<bool> attr[64];  // per device: shared-memory attribute set (host threads may race here)
   int dev = 0;
   NEDY_CUDA(cudaGetDevice(&dev));
-  if (attr_dev != dev) {
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  if (!attr[dev].load()) {
     NEDY_CUDA(cudaFuncSetAttribute(gemm_kernel<BM, AC, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::TOTAL));
-    attr_dev = dev;
+    attr[dev].store(true);
   }
   int nb = P.nb1 * P.nb2 * P.ksplit;
   dim3 grid(cdiv(P.N, BN), cdiv(P.M, BM), (unsigned)(nb < 65535 ? nb : 65535));

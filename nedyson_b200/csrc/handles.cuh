@@ -31,4 +31,13 @@ namespace nedy {
 // Runs f, maps its exceptions to a nedy_status and records the message for
 // nedy_last_error (the same mapping every entry point uses).
 int run_guarded(const std::function<void()> &f);
+
+// Whole-step bodies shared by the entry points (h_t: device pointers to the nao x nao
+// one-body Hamiltonian at tstp).  They throw; callers map the exceptions.
+// DecompSimulation::do_tstp (src/molNEsim_decomp_impl.h:85-104): corr_steps iterations.
+void decomp_step_fixed(nedy_ctx *ctx, int tstp, nedy_gf *G, nedy_gf *S, nedy_buf *hmf, const double2 *h_t,
+                       double mu, int corr_steps, double *err);
+// The same with the residual exit, one or two spins.
+void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *const *S, nedy_buf *const *hmf,
+              const double2 *const *h_t, const double *mu, int max_corr, double tol, int *iters, double *err_hist);
 }  // namespace nedy

@@ -553,12 +553,12 @@ double Predictor::train(int iters, int B, double lr) {
 void Predictor::apply(const DevGF &g, int T, double2 *corr_out) {
   const i64 tot = row_elements(g, T);
   if (tot == 0) return;
-  static bool attr[64] = {false};
+  static std::atomic<bool> attr[64];  // per device (host threads may race here)
   const int smem = PRED_W * PRED_W * 2 + INF_E * PRED_W * 2 + INF_E * PRED_IN * 4 + INF_E * 2 * 4 + INF_E * 8;
   NEDY_REQUIRE(ctx.device < 64, "device index out of range");
-  if (!attr[ctx.device]) {
+  if (!attr[ctx.device].load()) {
     NEDY_CUDA(cudaFuncSetAttribute(infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr[ctx.device] = true;
+    attr[ctx.device].store(true);
   }
   if (!w2t) NEDY_CUDA(cudaMalloc(&w2t, sizeof(__nv_bfloat16) * PRED_W * PRED_W));
   w2t_kernel<<<64, TPB, 0, ctx.stream>>>(W + OW2, w2t);

@@ -739,16 +739,16 @@ void split_stats(bool on, double *flops, double *ms) {
 
 template <int BN, int STAGES, int BKT = BK, bool OL = false>
 void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 grid, cudaStream_t s) {
-  static bool attr[64] = {false};
+  static std::atomic<bool> attr[64];  // per device (host threads may race here)
   int dev = 0;
   NEDY_CUDA(cudaGetDevice(&dev));
   NEDY_REQUIRE(dev < 64, "device index out of range");
   const int bytes = smem_bytes(P.stage_bytes, STAGES);
   NEDY_REQUIRE(STAGES * P.stage_bytes <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
-  if (!attr[dev]) {
+  if (!attr[dev].load()) {
     NEDY_CUDA(cudaFuncSetAttribute(split_gemm_kernel<BN, STAGES, BKT, OL>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(SMEM_LIMIT / STAGES, STAGES)));
-    attr[dev] = true;
+    attr[dev].store(true);
   }
   split_gemm_kernel<BN, STAGES, BKT, OL><<<grid, THREADS, bytes, s>>>(ma, mb, P);
   NEDY_CHECK_LAUNCH();

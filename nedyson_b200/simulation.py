@@ -239,3 +239,66 @@ class DecompSpinSimulation:
         self.do_boot(boot_iter, boot_tol)
         for t in range(self.k + 1, (nt if nt is not None else self.nt) + 1):
             self.do_tstp(t)
+
+
+def batch_problems(n: int, seed: int, nao_range=(8, 48), naux_per_nao: int = 4, amp_range=(0.01, 0.2),
+                   freq_range=(0.5, 3.0)):
+    """Seeded inputs of n independent instances: nao uniform in nao_range, naux = naux_per_nao * nao,
+    each with its own h0, B^Q, dipole, and a drive E0 sin(omega t) with E0 and omega uniform in
+    the given ranges.  Returns [(Problem, drive_kw)]."""
+    from .inputs import make_problem
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nao = int(rng.integers(nao_range[0], nao_range[1] + 1))
+        p = make_problem(nao, naux_per_nao * nao, seed=int(rng.integers(1 << 30)))
+        out.append((p, {"E0": float(rng.uniform(*amp_range)), "omega": float(rng.uniform(*freq_range))}))
+    return out
+
+
+class BatchSimulation:
+    """Many independent restricted density-fitted GF2 simulations stepped together
+    (nedy_batch_tstp): each instance is a DecompSimulation with its own context; h(t) of
+    every step is resident on the device (one (nt+1) x nao x nao buffer per instance)."""
+
+    def __init__(self, problems, nt: int, ntau: int, beta: float, dt: float, k: int = 5, corr_steps: int = 5,
+                 workers: int = 0, workspace_bytes: int = 1 << 30, device: int = 0, precision: int | None = None):
+        import ctypes as C
+        from ._lib import BatchInstance, check, lib
+        self.nt, self.k, self.corr_steps = nt, k, corr_steps
+        self.sims = [DecompSimulation(p, nt, ntau, beta, dt, k, corr_steps, "sin", kw, device, workspace_bytes)
+                     for p, kw in problems]
+        self.h_all = []
+        for s in self.sims:
+            if precision is not None:
+                s.ctx.set_precision(precision)
+            h = np.stack([s.h_of_t(t) for t in range(nt + 1)])
+            self.h_all.append(api.DeviceBuffer.from_array(s.ctx, np.ascontiguousarray(h)))
+        arr = (BatchInstance * len(self.sims))()
+        for i, (s, h) in enumerate(zip(self.sims, self.h_all)):
+            arr[i] = BatchInstance(s.ctx.h.value, s.G.h.value, s.Sigma.h.value, s.hmf.h.value, h.h.value, s.mu)
+        self._arr = arr
+        hb = C.c_void_p()
+        check(lib().nedy_batch_create(arr, len(self.sims), int(workers), C.byref(hb)))
+        self.h = hb
+
+    def close(self):
+        from ._lib import lib
+        if getattr(self, "h", None):
+            lib().nedy_batch_destroy(self.h)
+            self.h = None
+        for s in self.sims:
+            s.ctx.close()
+
+    def boot(self, max_iter: int = 50, tol: float = 1e-12):
+        for s in self.sims:
+            s.free_gf()
+            s.do_boot(max_iter, tol)
+
+    def do_tstp(self, t: int, tol: float = 0.0):
+        """One step of every instance; returns the corrector iterations per instance."""
+        import ctypes as C
+        from ._lib import check, lib
+        it = (C.c_int * len(self.sims))()
+        check(lib().nedy_batch_tstp(self.h, int(t), int(self.corr_steps), float(tol), it))
+        return list(it)
