@@ -58,6 +58,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "GF2 timesteps/s, nao=64 naux=256: plain FP64 vs split+predictor at 1e-8"
+BATCH_RESULT = [None]
 
 
 def flops_sigma(T, N, A, ntau, nspin=1):
@@ -94,6 +95,9 @@ def parse():
                     help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
+    ap.add_argument("--batch", type=int, default=64,
+                    help="instances of the batched workload (0: skip it): nao uniform in [8,48], naux=4 nao")
+    ap.add_argument("--batch-steps", type=int, default=3, help="timed steps of the batched workload")
     ap.add_argument("--plain-steps", type=int, default=4,
                     help="window steps of the plain FP64 forms (and of the error comparison between the forms)")
     ap.add_argument("--workspace-gb", type=float, default=0.0,
@@ -633,6 +637,59 @@ def run_engine(args, dist: Dist):
                 d2h=d2h // K, prep=prep, pred_info=pred_info, pred_stats=pstats, tune=tune, mu=list(mus))
 
 
+def run_batch(args, dist: Dist):
+    """The batched workload: independent density-fitted GF2 instances of uneven size (nao
+    uniform in [8, 48], naux = 4 nao, own h0, B^Q and dipole each, drive E0 sin(omega t) with
+    E0 in [0.01, 0.2] and omega in [0.5, 3]; beta=10, ntau=128, k=5, dt=0.02), stepped
+    together by nedy_batch_tstp (split-precision self-energy, residual exit at args.tol).
+    After the bootstrap and a few steps, the same window runs batched (worker pool, one
+    stream per instance) and one instance at a time; time on the device (events on the
+    legacy stream, which every instance stream synchronises with)."""
+    import torch
+    from nedyson_b200._lib import PREC_SPLIT_BF16X2
+    from nedyson_b200.simulation import BatchSimulation, batch_problems
+    n, Kb, Wb = args.batch, args.batch_steps, 2
+    t_first = 6 + 2
+    nt = t_first + Wb + Kb
+    probs = batch_problems(n, seed=rank_seed(args.seed + 1000, dist.rank))
+    tp = time.time()
+    b = BatchSimulation(probs, nt, 128, 10.0, 0.02, k=5, corr_steps=5, workers=16, workspace_bytes=1 << 30,
+                        device=dist.local, precision=PREC_SPLIT_BF16X2)
+    b.boot(max_iter=20)
+    for t in range(6, t_first + Wb):
+        b.do_tstp(t, args.tol)
+    torch.cuda.synchronize()
+    prep = time.time() - tp
+    T_win = list(range(t_first + Wb, t_first + Wb + Kb))
+    out = {}
+    for mode, workers in (("batched", 16), ("one_at_a_time", 1)):
+        b.set_workers(workers)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        its = []
+        for t in T_win:
+            its.append(b.do_tstp(t, args.tol))
+        e1.record()
+        torch.cuda.synchronize()
+        dist.barrier()
+        secs = dist.max(e0.elapsed_time(e1) / 1e3)
+        out[mode] = {"timesteps_s": Kb / secs, "instance_timesteps_s": Kb * n / secs, "ms_per_step": secs / Kb * 1e3,
+                     "mean_iterations": float(np.mean(its))}
+    naos = [p.nao for p, _ in probs]
+    res = {"workload": f"{n} independent density-fitted GF2 instances, nao uniform in [8,48] (seeded: min {min(naos)}, "
+                       f"max {max(naos)}, mean {np.mean(naos):.1f}), naux=4 nao, beta=10, ntau=128, k=5, dt=0.02, "
+                       f"E0 sin(omega t) drives; steps T={T_win[0]}..{T_win[-1]} after the bootstrap; split "
+                       f"self-energy (two BF16 pieces), residual exit at tol={args.tol:g}",
+           "batched": out["batched"], "one_at_a_time": out["one_at_a_time"],
+           "speedup_batched": out["batched"]["timesteps_s"] / out["one_at_a_time"]["timesteps_s"],
+           "workers": 16, "preparation_s": prep,
+           "note": "the window is short (nt=500 of the configuration needs about 0.6 TB of Green's-function history)"}
+    b.close()
+    return res
+
+
 def train_predictor(ctx, args):
     """Train the learned predictor on short GF2 trajectories of small molecules (nao=8,
     naux=24, Gaussian pulses of different strength and width), generated by the engine
@@ -714,6 +771,10 @@ def main():
 
     fp64 = fp64_gemm_peak(dist.local) if dist.rank == 0 else None
     r = run_engine(args, dist)
+    import gc
+    gc.collect()  # release the headline state before the batched workload
+    if args.batch > 0 and not args.split_only:
+        BATCH_RESULT[0] = run_batch(args, dist)
     fm = r["forms"]
     head = fm["split_learned_exit"]
     value = replica_value(K, dist.world, head["secs"])
@@ -801,6 +862,8 @@ def main():
                        "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                        "what": "the headline form over the whole window again through the C ABI, each step copying "
                                "h(t) of each spin in from pinned host memory and its new G rows out"}
+        if args.batch > 0 and not args.split_only:
+            line["batched_workload"] = BATCH_RESULT[0]
         if dist.world == 1 and not args.no_cpu_baseline:
             it = CpuIteration(args, T_ref)
             t_iter, desc = it.sample()

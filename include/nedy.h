@@ -274,6 +274,24 @@ int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn,
                           nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
                           double mu_up, double mu_dn, int corr_steps, double *err);
 
+/* --- Equilibrium (Matsubara) GF2 state on the collocation grid: the state the reference
+ * takes from the external gfmol solver (src/molNEsim_decomp_impl.h:23-33, L_to_Tau :146-167).
+ * Restricted (nspin = 1) or unrestricted (nspin = 2, the mean field and self-energy of
+ * both spins as in molHFSolverSpinDecomp / molGF2SolverSpinDecomp) density-fitted GF2:
+ * iterates Sigma^M[G^M] (the GF2 contraction of the t = 0 mixed row, G^tv(0,tau) =
+ * -i G^M(beta - tau)), F = h0 + HF(-G^M(beta)) and the Dyson equation
+ * G = G_ref + G_ref * (F - F_ref + Sigma^M) * G (Matsubara convolutions evaluated exactly
+ * on the degree-ntau interpolants), with G <- G + mixing (G_new - G), until
+ * max |G_new - G| <= tol or max_iter iterations.
+ * On entry G[s]->mat holds G_ref, the free G^M of the Fock matrix F_ref[s] at the chemical
+ * potential of the run (which stays fixed); on return G[s]->mat holds the GF2 equilibrium,
+ * Sigma[s]->mat its self-energy and F_out[s] its mean field (nao x nao complex buffers).
+ * nedy_set_df_tensor must have been called; the context's ntau and beta are the grid.
+ * iters / diff (optional): iterations run and the last change. */
+int nedy_matsubara_gf2(nedy_ctx *ctx, int nspin, nedy_gf *const *G, nedy_gf *const *Sigma, const nedy_buf *const *h0,
+                       const nedy_buf *const *F_ref, nedy_buf *const *F_out, double mixing, int max_iter, double tol,
+                       int *iters, double *diff);
+
 /* --- Batched independent simulations (many molecules or fields of uneven nao; no
  * counterpart in the reference, which steps one DecompSimulation at a time,
  * src/molNEsim_decomp_impl.h:85-104).  Each instance keeps its own context (stream,

@@ -99,6 +99,7 @@ SIGNATURES = {
     "nedy_energy_conv": ([_P, _I, _P, _P, _DP], _I),
     "nedy_decomp_tstp": ([_P, _I, _P, _P, _P, _P, _D, _I, _DP], _I),
     "nedy_full_tstp": ([_P, _I, _P, _P, _P, _P, _D, _I, _DP], _I),
+    "nedy_matsubara_gf2": ([_P, _I, _PP, _PP, _PP, _PP, _PP, _D, _I, _D, C.POINTER(_I), _DP], _I),
     "nedy_batch_create": ([C.POINTER(BatchInstance), _I, _I, _PP], _I),
     "nedy_batch_destroy": ([_P], _I),
     "nedy_batch_tstp": ([_P, _I, _I, _D, C.POINTER(_I)], _I),

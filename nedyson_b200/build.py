@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libnedy_b200.so")
 BUILD = os.path.join(HERE, "_build")
 
-SOURCES = ["gemm_f64.cu", "split_gemm.cu", "sigma_df.cu", "sigma_full.cu", "dyson.cu", "boot.cu", "predictor.cu", "capi.cu", "batch.cu", "noalloc.cu", "host_tables.cpp"]
+SOURCES = ["gemm_f64.cu", "split_gemm.cu", "sigma_df.cu", "sigma_full.cu", "dyson.cu", "boot.cu", "predictor.cu", "capi.cu", "batch.cu", "matsubara.cu", "noalloc.cu", "host_tables.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-I" + os.path.join(ROOT, "include")]

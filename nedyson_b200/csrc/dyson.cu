@@ -663,15 +663,28 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
   std::swap(c.mixK_ver, c.mixK_alt_ver);
   std::swap(c.mixK_nao, c.mixK_alt_nao);
   if (c.mixK && c.mixK_src == G.mat && c.mixK_ver == G.mat_version && c.mixK_nao == N) return;
-  build_mixing_eval(c.col);
-  const int Q2 = 2 * c.col.Q;
   if (c.mixK && c.mixK_nao != N) { cudaFree(c.mixK); c.mixK = nullptr; }
   if (!c.mixK) NEDY_CUDA(cudaMalloc(&c.mixK, sizeof(double2) * (size_t)np * np * es));
+  build_tau_kernel(c, G.mat, N, (double)G.sig, c.mixK);
+  c.mixK_src = G.mat;
+  c.mixK_ver = G.mat_version;
+  c.mixK_nao = N;
+}
+
+// K[m][i] = int_0^beta L_i(tau') B(tau' - tau_m) dtau' for the degree-ntau interpolant B of
+// the np nodal blocks Bn (extended to negative arguments by B(x) = sig B(x + beta)), L_i the
+// Lagrange polynomial of node i: then int_0^beta f(tau') B(tau' - tau_m) dtau' = sum_i f_i K[m][i]
+// for any degree-ntau f.  The quadrature tables split the integral at tau_m (collocation.cpp).
+void build_tau_kernel(Ctx &c, const double2 *Bn, int N, double sig, double2 *K) {
+  const int np = c.ntau + 1;
+  const i64 es = (i64)N * N;
+  build_mixing_eval(c.col);
+  const int Q2 = 2 * c.col.Q;
   // sign of the antiperiodic extension folded into the first half of EB
   std::vector<double> EBs(c.col.EB);
   for (int m = 0; m < np; m++)
     for (int q = 0; q < c.col.Q; q++)
-      for (int j = 0; j < np; j++) EBs[((size_t)m * Q2 + q) * np + j] *= (double)G.sig;
+      for (int j = 0; j < np; j++) EBs[((size_t)m * Q2 + q) * np + j] *= sig;
   const int chunk = std::max(1, (int)std::min<i64>(np, (i64)(2LL << 30) / (sizeof(double2) * Q2 * es)));
   double *dEA = nullptr, *dEB = nullptr;
   double2 *BB = nullptr;
@@ -682,11 +695,11 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
   h2d_sync(dEB, EBs.data(), sizeof(double) * EBs.size(), c.stream);
   for (int m0 = 0; m0 < np; m0 += chunk) {
     int nm = std::min(chunk, np - m0);
-    {  // BB[m] = EB[m] (2Q x np) * G^M (np x N^2)
+    {  // BB[m] = EB[m] (2Q x np) * Bn (np x N^2)
       GemmArgs g;
       g.M = Q2; g.N = (int)es; g.K = np; g.nb1 = nm;
       g.A = rowmajor(dEB + (size_t)m0 * Q2 * np, np); g.A.bs1 = (i64)Q2 * np; g.a_cplx = false;
-      g.B = rowmajor(G.mat, es);
+      g.B = rowmajor(Bn, es);
       g.C = rowmajor(BB, es); g.C.bs1 = (i64)Q2 * es;
       gemm(g, c.stream);
     }
@@ -695,7 +708,7 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
       g.M = np; g.N = (int)es; g.K = Q2; g.nb1 = nm;
       g.A = rowmajor(dEA + (size_t)m0 * np * Q2, Q2); g.A.bs1 = (i64)np * Q2; g.a_cplx = false;
       g.B = rowmajor(BB, es); g.B.bs1 = (i64)Q2 * es;
-      g.C = rowmajor(c.mixK + (size_t)m0 * np * es, es); g.C.bs1 = (i64)np * es;
+      g.C = rowmajor(K + (size_t)m0 * np * es, es); g.C.bs1 = (i64)np * es;
       g.alpha = make_double2(0.5 * c.beta, 0.0);
       gemm(g, c.stream);
     }
@@ -704,9 +717,6 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G) {
   cudaFree(dEA);
   cudaFree(dEB);
   cudaFree(BB);
-  c.mixK_src = G.mat;
-  c.mixK_ver = G.mat_version;
-  c.mixK_nao = N;
 }
 
 // out[m] (+)= sum_i A_i K[m][i]   (A_i = tv blocks of one time row), out in [m][a][b] layout

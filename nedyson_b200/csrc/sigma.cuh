@@ -34,6 +34,9 @@ double dyson_start(Ctx &c, DevGF &G, const DevGF &Sig, const double2 *hmf, doubl
 double energy_conv(Ctx &c, int T, const DevGF &Sig, const DevGF &G);
 // Mixing kernel of G^M (rebuilt when G^M changes)
 void ensure_mixing_kernel(Ctx &c, const DevGF &G);
+// Kernel of the imaginary-time integral int_0^beta f(tau') B(tau' - tau_m) dtau' = sum_i f_i K[m][i]
+// for nodal blocks Bn (np x N x N) extended by B(x) = sig B(x + beta); K: np x np x N x N
+void build_tau_kernel(Ctx &c, const double2 *Bn, int N, double sig, double2 *K);
 // Cached inverse of the time-local Dyson matrix for times [t0, t1] (after their rows are final)
 void update_minv(Ctx &c, const DevGF &Sig, const double2 *hmf, double mu, int t0, int t1);
 

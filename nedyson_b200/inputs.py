@@ -234,3 +234,44 @@ def free_history(nt: int, t_fill: int, ntau: int, x: np.ndarray, mu: float, F: n
     mat = np.stack([-(V * fermi_exp(beta, tau, ev)) @ V.conj().T for tau in taus])
     return (scale * les).astype(np.complex128), (scale * ret).astype(np.complex128), \
         (scale * tv).astype(np.complex128), mat.astype(np.complex128)
+
+
+def gf2_equilibrium(ctx, p: Problem, beta: float, spin: bool = False, mixing: float = 1.0, max_iter: int = 200,
+                    tol: float = 1e-12):
+    """Equilibrium GF2 state of problem p on the collocation grid of ctx (nedy_matsubara_gf2):
+    starts from the (unrestricted) Hartree-Fock equilibrium, whose mid-gap chemical potential
+    it keeps.  Returns dict(F=[Fock per spin], mu=[mu per spin], Gmat=[G^M], Smat=[Sigma^M],
+    iters, diff) with host arrays; the Vija tensor of p is set on ctx."""
+    import ctypes as C
+    from . import api
+    from ._lib import check, lib
+    ns = 2 if spin else 1
+    if spin:
+        Fs, mus = uhf_equilibrium(p, beta)
+    else:
+        F, mu = hf_equilibrium(p, beta)
+        Fs, mus = (F,), (mu,)
+    x, _ = ctx.collocation()
+    N, ntau = p.nao, ctx.ntau
+    api.molGF2SolverDecomp(ctx, p.Vija)  # sets the density-fitted tensor
+    Gs, Ss, h0b, Frb, Fob = [], [], [], [], []
+    for s in range(ns):
+        g = HostGF(-1, ntau, N, -1)
+        g0_from_h0(g, x, mus[s], Fs[s], beta, 0.01, -1)
+        Gs.append(api.green_func(ctx, -1, ntau, N, -1))
+        Gs[-1].upload(3, 0, g.mat)
+        Ss.append(api.green_func(ctx, -1, ntau, N, -1))
+        h0b.append(api.DeviceBuffer.from_array(ctx, np.ascontiguousarray(p.h0_of(s) if spin else p.h0,
+                                                                          dtype=np.complex128)))
+        Frb.append(api.DeviceBuffer.from_array(ctx, np.ascontiguousarray(Fs[s], dtype=np.complex128)))
+        Fob.append(api.DeviceBuffer(ctx, N * N * 16))
+    arr = lambda objs: (C.c_void_p * ns)(*[o.h.value for o in objs])  # noqa: E731
+    it, d = C.c_int(), C.c_double()
+    check(lib().nedy_matsubara_gf2(ctx.h, ns, arr(Gs), arr(Ss), arr(h0b), arr(Frb), arr(Fob), float(mixing),
+                                   int(max_iter), float(tol), C.byref(it), C.byref(d)))
+    out = dict(mu=list(mus), iters=it.value, diff=d.value, Gmat=[], Smat=[], F=[])
+    for s in range(ns):
+        out["Gmat"].append(Gs[s].download(3, 0, ntau + 1))
+        out["Smat"].append(Ss[s].download(3, 0, ntau + 1))
+        out["F"].append(Fob[s].download((N, N)))
+    return out

@@ -42,9 +42,17 @@ class DecompSimulation:
         E = drive(self.drive_kind, t * self.dt, self.k, self.dt, **self.drive_kw)
         return (self.p.h0 + E * self.p.D).astype(np.complex128)
 
+    def set_equilibrium(self, F, Gmat):
+        """Start from another equilibrium state than Hartree-Fock, e.g. the GF2 one of
+        inputs.gf2_equilibrium: its Fock matrix F (mean field of the first k+1 steps) and G^M
+        on the collocation grid (the free propagation of F on [0, k] stays the bootstrap guess)."""
+        self.F, self._Gmat = np.asarray(F), np.asarray(Gmat)
+
     def initial_state(self) -> HostGF:
         g = HostGF(self.nt, self.ntau, self.p.nao, -1)
         g0_from_h0(g, self.x, self.mu, self.F, self.beta, self.dt, self.k)
+        if getattr(self, "_Gmat", None) is not None:
+            g.mat[:] = self._Gmat
         return g
 
     def free_gf(self):
@@ -263,8 +271,7 @@ class BatchSimulation:
 
     def __init__(self, problems, nt: int, ntau: int, beta: float, dt: float, k: int = 5, corr_steps: int = 5,
                  workers: int = 0, workspace_bytes: int = 1 << 30, device: int = 0, precision: int | None = None):
-        import ctypes as C
-        from ._lib import BatchInstance, check, lib
+        from ._lib import BatchInstance
         self.nt, self.k, self.corr_steps = nt, k, corr_steps
         self.sims = [DecompSimulation(p, nt, ntau, beta, dt, k, corr_steps, "sin", kw, device, workspace_bytes)
                      for p, kw in problems]
@@ -278,8 +285,17 @@ class BatchSimulation:
         for i, (s, h) in enumerate(zip(self.sims, self.h_all)):
             arr[i] = BatchInstance(s.ctx.h.value, s.G.h.value, s.Sigma.h.value, s.hmf.h.value, h.h.value, s.mu)
         self._arr = arr
+        self.h = None
+        self.set_workers(workers)
+
+    def set_workers(self, workers: int):
+        """(Re)create the batch with this many worker threads (<= 0: up to 16)."""
+        import ctypes as C
+        from ._lib import check, lib
+        if getattr(self, "h", None):
+            lib().nedy_batch_destroy(self.h)
         hb = C.c_void_p()
-        check(lib().nedy_batch_create(arr, len(self.sims), int(workers), C.byref(hb)))
+        check(lib().nedy_batch_create(self._arr, len(self.sims), int(workers), C.byref(hb)))
         self.h = hb
 
     def close(self):

@@ -29,8 +29,14 @@ class OracleDecompSim:
         E = drive(self.drive_kind, t * self.dt, self.k, self.dt, **self.drive_kw)
         return (self.p.h0 + E * self.p.D).astype(np.complex128)
 
+    def set_equilibrium(self, F, Gmat):
+        """Start from another equilibrium state (e.g. the GF2 one): Fock matrix F, G^M on the grid."""
+        self.F, self._Gmat = np.asarray(F), np.asarray(Gmat)
+
     def free_gf(self):
         g0_from_h0(self.G, self.x, self.mu, self.F, self.beta, self.dt, self.k)
+        if getattr(self, "_Gmat", None) is not None:
+            self.G.mat[:] = self._Gmat
         self.hmf[: self.k + 1] = self.F
 
     def do_boot(self, max_iter=50, tol=1e-12):
