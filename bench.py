@@ -91,6 +91,9 @@ def parse():
     ap.add_argument("--restricted", action="store_true",
                     help="restricted simulation instead of the spin-unrestricted one")
     ap.add_argument("--predictor", default="learned", choices=["learned", "poly"])
+    ap.add_argument("--equilibrium", default="gf2", choices=["gf2", "hf"],
+                    help="initial state: the GF2 equilibrium on the collocation grid (nedy_matsubara_gf2) or "
+                         "the Hartree-Fock one")
     ap.add_argument("--split-mode", default="bf16x2", choices=["bf16x3", "bf16x2"],
                     help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
@@ -413,6 +416,16 @@ def run_engine(args, dist: Dist):
     else:
         F, mu = hf_equilibrium(p, args.beta)
         Fs, mus = (F,), (mu,)
+    eq_info, Gmats = None, None
+    if args.equilibrium == "gf2" and args.state == "trajectory":
+        from nedyson_b200.inputs import gf2_equilibrium
+        te = time.time()
+        ectx = api.Context(5, ntau, N, 5, args.beta, args.dt, device=dev)
+        eq = gf2_equilibrium(ectx, p, args.beta, spin=spin, tol=1e-12)
+        ectx.close()
+        Fs, Gmats = [np.ascontiguousarray(f) for f in eq["F"]], eq["Gmat"]
+        eq_info = {"kind": "GF2 equilibrium on the collocation grid (nedy_matsubara_gf2, FP64)",
+                   "iterations": eq["iters"], "last_change": eq["diff"], "seconds": time.time() - te}
     ctx = api.Context(nt, ntau, N, 5, args.beta, args.dt, device=dev,
                       workspace_bytes=int(args.workspace_gb * (1 << 30)))
     x, _ = ctx.collocation()
@@ -463,7 +476,7 @@ def run_engine(args, dist: Dist):
             G[s].upload(LES, 0, les)
             G[s].upload(RET, 0, ret)
             G[s].upload(TV, 0, tv)
-            G[s].upload(MAT, 0, mat)
+            G[s].upload(MAT, 0, Gmats[s] if Gmats is not None else mat)
             del les, ret, tv
             hm = np.zeros((nt + 1, N, N), np.complex128)
             hm[:kk + 1] = Fs[s]
@@ -480,8 +493,8 @@ def run_engine(args, dist: Dist):
         for t in range(kk + 1, t_first):
             step_tol(t, 1e-10)
         ctx.synchronize()
-        prep = {"boot_iterations": it + 1, "boot_err": berr, "steps": t_first - kk - 1,
-                "seconds": time.time() - tp}
+        prep = {"equilibrium": eq_info or "Hartree-Fock", "boot_iterations": it + 1, "boot_err": berr,
+                "steps": t_first - kk - 1, "seconds": time.time() - tp}
     else:
         for s in range(ns):
             les, ret, tv, mat = free_history(nt, t_first, ntau, x, mus[s], Fs[s], args.beta, args.dt)
@@ -784,7 +797,8 @@ def main():
                         " (tcgen05, FP32 accumulation), FP64 Dyson/HF/density/residual")
     cfg["predictor"] = ("learned MLP correction of the k=5 extrapolation (polynomial fallback)" if args.predictor == "learned"
                         else "polynomial extrapolation (k=5)") + f" + residual exit at tol={args.tol:g} (at most {args.corr} iterations)"
-    cfg["state"] = (f"GF2 trajectory from the {'restricted' if args.restricted else 'unrestricted'} HF equilibrium "
+    eqname = "GF2" if args.equilibrium == "gf2" else "HF"
+    cfg["state"] = (f"GF2 trajectory from the {'restricted' if args.restricted else 'unrestricted'} {eqname} equilibrium "
                     "(Gaussian pulse E0=0.05 t0=2 sigma=0.5)"
                     if args.state == "trajectory" else "synthetic free-propagation history, 0.1 sin(2t) drive")
     cfg["tol"] = args.tol

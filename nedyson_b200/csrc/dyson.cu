@@ -14,6 +14,7 @@
 // M(t') = (i bd0/dt + mu) - hmf(t') - dt*w0*Sig^R(t',t'): for t' < T they no longer
 // change, so each step is a single block product instead of an LU solve.
 #include "sigma.cuh"
+#include <atomic>
 #include <cmath>
 #include <algorithm>
 
@@ -132,15 +133,19 @@ __global__ void gj_first_pivot_kernel(int n, int nrhs, double2 *A, double2 *B, i
   gj_pivot_block(n, nrhs, A, B, 0, piv, fac);
 }
 
-__global__ void gj_step_kernel(int n, int nrhs, double2 *A, double2 *B, int c, int cw, int *piv, double2 *fac,
-                               int *status) {
-  __shared__ double2 rowc[64];
+// One elimination step c on this CTA's column slab.  COOP: inside the cooperative kernel,
+// where the pivot index and column come from another CTA in the same launch, so they are
+// read through L2 (ld.global.cg) rather than a possibly stale L1 line.
+template <bool COOP>
+__device__ void gj_step_body(int n, int nrhs, double2 *A, double2 *B, int c, int cw, int *piv, double2 *fac,
+                             int *status, double2 *rowc) {
   const int j0 = blockIdx.x * cw, W = n + nrhs;
   const int jn = min(cw, W - j0);
   if (jn <= 0) return;
-  const int p = piv[c & 1];
+  const int p = COOP ? __ldcg(piv + (c & 1)) : piv[c & 1];
   const double2 *f = fac + (i64)(c & 1) * n;
-  double2 pv = f[p];
+  auto fget = [&](int r) { return COOP ? __ldcg(f + r) : f[r]; };
+  double2 pv = fget(p);
   if (pv.x == 0.0 && pv.y == 0.0) {
     if (threadIdx.x == 0) *status = 1;
     pv = make_double2(1.0, 0.0);
@@ -154,7 +159,7 @@ __global__ void gj_step_kernel(int n, int nrhs, double2 *A, double2 *B, int c, i
     const double2 rc = cmul(ap, inv);
     rowc[jj] = rc;
     aug(A, B, n, nrhs, c, j) = rc;
-    if (p != c) aug(A, B, n, nrhs, p, j) = csub(ac, cmul(f[c], rc));
+    if (p != c) aug(A, B, n, nrhs, p, j) = csub(ac, cmul(fget(c), rc));
   }
   __syncthreads();
   // phase 2: eliminate the other rows (the factors are the pivot column after the swap)
@@ -162,12 +167,69 @@ __global__ void gj_step_kernel(int n, int nrhs, double2 *A, double2 *B, int c, i
     const int r = (int)(idx / jn), jj = (int)(idx - (i64)r * jn);
     if (r == c || r == p) continue;
     double2 &x = aug(A, B, n, nrhs, r, j0 + jj);
-    x = csub(x, cmul(f[r], rowc[jj]));
+    x = csub(x, cmul(fget(r), rowc[jj]));
   }
   __syncthreads();
   // the owner of column c+1 prepares the next step
   const int c1 = c + 1;
   if (c1 < n && c1 >= j0 && c1 < j0 + jn) gj_pivot_block(n, nrhs, A, B, c1, piv, fac);
+}
+
+__global__ void gj_step_kernel(int n, int nrhs, double2 *A, double2 *B, int c, int cw, int *piv, double2 *fac,
+                               int *status) {
+  __shared__ double2 rowc[64];
+  gj_step_body<false>(n, nrhs, A, B, c, cw, piv, fac, status, rowc);
+}
+
+__device__ __forceinline__ unsigned long long gj_gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier over all CTAs of a cooperative launch (every CTA is resident).  bar[0] counts
+// arrivals, bar[1] is the generation.  The wait is bounded (2 s of %globaltimer, or an
+// error another CTA reported): on give-up it sets *status = 2 and returns false, and the
+// caller returns, so the launch always ends.
+__device__ bool gj_grid_barrier(unsigned *bar, int *status) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen;  // read the generation before arriving
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      bar[0] = 0;  // nobody arrives again before the generation moves on
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const unsigned long long t0 = gj_gtime();
+      for (unsigned it = 1; *gen == g; it++) {
+        if ((it & 1023) == 0 && (gj_gtime() - t0 > 2000000000ULL || *(volatile int *)status == 2)) {
+          atomicExch(status, 2);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// All n elimination steps of gj_step_kernel in one cooperative launch, a grid barrier
+// between steps (the pivot of step c+1 is produced by the owner of column c+1 during step c).
+__global__ void gj_coop_kernel(int n, int nrhs, double2 *A, double2 *B, int cw, int *piv, double2 *fac, int *status,
+                               unsigned *bar) {
+  __shared__ double2 rowc[64];
+  if (blockIdx.x == 0) gj_pivot_block(n, nrhs, A, B, 0, piv, fac);
+  if (!gj_grid_barrier(bar, status)) return;
+  for (int c = 0; c < n; c++) {
+    gj_step_body<true>(n, nrhs, A, B, c, cw, piv, fac, status, rowc);
+    if (!gj_grid_barrier(bar, status)) return;
+  }
 }
 
 void gj(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB) {
@@ -179,11 +241,35 @@ void gj(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB)
     const int G = (W + cw - 1) / cw;
     int *piv = c.ws.alloc<int>(2);
     double2 *fac = c.ws.alloc<double2>(2 * (i64)n);
-    gj_first_pivot_kernel<<<1, TPB, 0, c.stream>>>(n, nrhs, A, B, piv, fac);
-    NEDY_CHECK_LAUNCH();
-    for (int col = 0; col < n; col++) {
-      gj_step_kernel<<<G, TPB, 0, c.stream>>>(n, nrhs, A, B, col, cw, piv, fac, st);
+    // one cooperative launch when every CTA fits on the device at once, else one launch per step
+    static std::atomic<int> coop_ok[64];  // per device: 0 unknown, 1 yes, -1 no (host threads may race here)
+    int dev = 0;
+    NEDY_CUDA(cudaGetDevice(&dev));
+    NEDY_REQUIRE(dev < 64, "device index out of range");
+    if (coop_ok[dev].load() == 0) {
+      int coop = 0, sms = 0, per_sm = 0;
+      NEDY_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+      NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      NEDY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gj_coop_kernel, TPB, 0));
+      coop_ok[dev].store(coop && (i64)per_sm * sms >= 148 ? 1 : -1);
+    }
+    int sms = 0, per_sm = 0;
+    NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    NEDY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gj_coop_kernel, TPB, 0));
+    if (coop_ok[dev].load() > 0 && G <= per_sm * sms) {
+      unsigned *bar = c.ws.alloc<unsigned>(2);
+      NEDY_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), c.stream));
+      int nn = n, nr = nrhs, cww = cw;
+      void *args[] = {&nn, &nr, &A, &B, &cww, &piv, &fac, &st, &bar};
+      NEDY_CUDA(cudaLaunchCooperativeKernel((const void *)gj_coop_kernel, dim3(G), dim3(TPB), args, 0, c.stream));
       NEDY_CHECK_LAUNCH();
+    } else {
+      gj_first_pivot_kernel<<<1, TPB, 0, c.stream>>>(n, nrhs, A, B, piv, fac);
+      NEDY_CHECK_LAUNCH();
+      for (int col = 0; col < n; col++) {
+        gj_step_kernel<<<G, TPB, 0, c.stream>>>(n, nrhs, A, B, col, cw, piv, fac, st);
+        NEDY_CHECK_LAUNCH();
+      }
     }
   } else {
     gj_kernel<<<nb, TPB, 0, c.stream>>>(n, nrhs, A, sA, B, sB, st);
@@ -594,6 +680,7 @@ void check_status(Ctx &c) {
     for (int v : h)
       if (v) {
         c.pending_status.clear();
+        if (v == 2) throw CudaError("Dyson solve: a bounded grid barrier timed out");
         throw ArgError("singular matrix in a Dyson solve");
       }
   }
