@@ -73,7 +73,7 @@ SIGNATURES = {
     "nedy_split_stats": ([_I, _DP, _DP], _I),
     "nedy_split_autotune": ([_I], _I),
     "nedy_sigma_chunk_plan": ([_I, _I, _LL, _I, _I, _I, C.POINTER(_I), C.POINTER(_I)], _I),
-    "nedy_split_gemm_check": ([_I] * 16 + [C.c_ulonglong, C.POINTER(C.c_double)], _I),
+    "nedy_split_gemm_check": ([_I] * 17 + [C.c_ulonglong, C.POINTER(C.c_double)], _I),
     "nedy_split_tune_report": ([C.c_char_p, _I], _I),
     "nedy_predictor_create": ([_P, _LL, C.c_ulonglong, _PP], _I),
     "nedy_predictor_destroy": ([_P], _I),

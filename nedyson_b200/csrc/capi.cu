@@ -330,7 +330,7 @@ int nedy_sigma_chunk_plan(int nao, int naux, long long budget, int precision, in
 
 int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, int b_cplx, int conj_a, int conj_b,
                           int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,
-                          unsigned long long seed, double *rel_err) {
+                          int persistent, unsigned long long seed, double *rel_err) {
   return guard([&] {
     NEDY_REQUIRE(rel_err, "null argument");
     NEDY_CUDA(cudaSetDevice(device));
@@ -338,7 +338,7 @@ int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, i
     k.M = M; k.N = N; k.K = K; k.nb = nb;
     k.a_cplx = a_cplx; k.b_cplx = b_cplx; k.conjA = conj_a; k.conjB = conj_b; k.np = npieces;
     k.out_pieces = out_pieces; k.accumulate = accumulate;
-    k.bn = tile_n; k.stages = stages; k.bk = k_block; k.kdiv = kdiv;
+    k.bn = tile_n; k.stages = stages; k.bk = k_block; k.kdiv = kdiv; k.persist = persistent != 0;
     k.seed = seed;
     k.alpha = 0.75;
     cudaStream_t st = nullptr;

@@ -354,6 +354,98 @@ __device__ __forceinline__ void store_fp64_16_staged(const Params &P, i64 roff, 
   __syncwarp();
 }
 
+// Epilogue of one 128 x BN output tile: this warp's 32 TMEM lanes of both parts (columns
+// [0, BN) real, [BN, 2 BN) imaginary from tmem) to the output View.  zero: the tile had no
+// K blocks (store zeros).  wbuf: this warp's staging buffer in shared memory.
+template <int BN>
+__device__ __forceinline__ void epilogue_tile(const Params &P, int m0, int n0, int b, int warp, int lane,
+                                              uint32_t tmem, bool zero, uint8_t *wbuf) {
+    const int m = m0 + warp * 32 + lane;
+    const bool mok = m < P.M;
+    const i64 roff =
+        (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // piece outputs whose 32 rows of this warp are contiguous use the row-staged store
+    const int r0 = m0 + warp * 32;
+    bool rows_contig = P.out_pieces && P.rs_lo == 1 && r0 + 32 <= P.M;
+    if (rows_contig && P.rdiv) rows_contig = (r0 % P.rdiv) + 32 <= P.rdiv;
+    const i64 roff0 = __shfl_sync(0xffffffffu, roff, 0);
+    rows_contig = rows_contig && (roff0 & 7) == 0;
+    // every row offset a multiple of 8 elements (16-byte stores of BF16 pieces)
+    const bool rows_al8 = __all_sync(0xffffffffu, (roff & 7) == 0);
+    __nv_bfloat16 *sbuf = (__nv_bfloat16 *)wbuf;
+    const int imok = mok ? 1 : 0;
+    {
+      for (int c0 = 0; c0 < BN;) {
+        if (n0 + c0 >= P.N) break;  // uniform across the warp
+        const int nf = n0 + c0;
+        if (P.out_pieces && !rows_contig && rows_al8 && c0 + 64 <= BN && nf + 64 <= P.N && P.cs_lo == 1 &&
+            (P.cdiv == 0 || (nf % P.cdiv) + 64 <= P.cdiv)) {
+          // 64 contiguous columns of each part, staged
+          const i64 cbase = P.cdiv ? (i64)(nf / P.cdiv) * P.cs_hi + (i64)(nf % P.cdiv) : (i64)nf;
+          if ((cbase & 7) == 0) {
+            __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
+            const float al = (float)P.alpha;
+            for (int part = 0; part < 2; part++) {
+              float x[64];
+              tmem_ld64(trow + (uint32_t)(part * BN + c0), x);
+#pragma unroll
+              for (int j = 0; j < 64; j++) x[j] = zero ? 0.f : al * x[j];
+              store_pieces64_staged(P, o + (i64)part * P.out_np * P.plane, roff, imok, cbase, x, sbuf, lane);
+            }
+            c0 += 64;
+            continue;
+          }
+        }
+        float vr[16], vi[16];
+        tmem_ld16(trow + (uint32_t)c0, vr);
+        tmem_ld16(trow + (uint32_t)(BN + c0), vi);
+        if (zero) {
+#pragma unroll
+          for (int j = 0; j < 16; j++) vr[j] = vi[j] = 0.f;
+        }
+        c0 += 16;
+        i64 cbase;
+        const bool fast = chunk_base(P, nf, cbase);
+        if (!P.out_pieces && fast && P.cs_lo == 1) {  // warp-uniform
+          store_fp64_16_staged(P, roff, imok, cbase, vr, vi, (double2 *)wbuf, lane);
+          continue;
+        }
+        if (!mok) continue;
+        if (P.out_pieces) {
+          __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
+          if (rows_contig && fast && (cbase & 7) == 0 && (P.cs_lo & 7) == 0) {
+            store_pieces16_rows(P, o, roff0, cbase, nf, vr, sbuf, lane);
+            store_pieces16_rows(P, o + (i64)P.out_np * P.plane, roff0, cbase, nf, vi, sbuf, lane);
+          } else {
+            store_pieces16(P, o, roff, cbase, fast, nf, vr);
+            store_pieces16(P, o + (i64)P.out_np * P.plane, roff, cbase, fast, nf, vi);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const int n = nf + j;
+            if (n >= P.N) break;
+            const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo : col_off(P, n));
+            double2 *o = (double2 *)P.out + off;
+            const double xr = P.alpha * (double)vr[j], xi = P.alpha * (double)vi[j];
+            if (P.atomic) {
+              atomicAdd(&o->x, xr);
+              atomicAdd(&o->y, xi);
+            } else if (P.accumulate) {
+              double2 t = *o;
+              t.x += xr;
+              t.y += xi;
+              *o = t;
+            } else {
+              *o = make_double2(xr, xi);
+            }
+          }
+        }
+      }
+    }
+}
+
 // OL = false: one stage holds one piece product of one K block (the A and B tiles of that
 //   product), BKT = 64;
 // OL = true ("one load"): one stage holds every piece of one K block (BKT = 32 or 64), and
@@ -500,91 +592,7 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
     __syncwarp();
     const bool ok = __shfl_sync(0xffffffffu, okl, 0) != 0 && !skip;
     tc_fence_after();
-    const int m = m0 + warp * 32 + lane;
-    const bool mok = m < P.M;
-    const i64 roff =
-        (P.rdiv ? (i64)(m / P.rdiv) * P.rs_hi + (i64)(m % P.rdiv) * P.rs_lo : (i64)m * P.rs_lo) + (i64)b * P.bs;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    // piece outputs whose 32 rows of this warp are contiguous use the row-staged store
-    const int r0 = m0 + warp * 32;
-    bool rows_contig = P.out_pieces && P.rs_lo == 1 && r0 + 32 <= P.M;
-    if (rows_contig && P.rdiv) rows_contig = (r0 % P.rdiv) + 32 <= P.rdiv;
-    const i64 roff0 = __shfl_sync(0xffffffffu, roff, 0);
-    rows_contig = rows_contig && (roff0 & 7) == 0;
-    // every row offset a multiple of 8 elements (16-byte stores of BF16 pieces)
-    const bool rows_al8 = __all_sync(0xffffffffu, (roff & 7) == 0);
-    uint8_t *wbuf = smem + warp * STAGE_WARP_BYTES;  // stages are idle in the epilogue
-    __nv_bfloat16 *sbuf = (__nv_bfloat16 *)wbuf;
-    const int imok = mok ? 1 : 0;
-    if (ok) {
-      for (int c0 = 0; c0 < BN;) {
-        if (n0 + c0 >= P.N) break;  // uniform across the warp
-        const int nf = n0 + c0;
-        if (P.out_pieces && !rows_contig && rows_al8 && c0 + 64 <= BN && nf + 64 <= P.N && P.cs_lo == 1 &&
-            (P.cdiv == 0 || (nf % P.cdiv) + 64 <= P.cdiv)) {
-          // 64 contiguous columns of each part, staged
-          const i64 cbase = P.cdiv ? (i64)(nf / P.cdiv) * P.cs_hi + (i64)(nf % P.cdiv) : (i64)nf;
-          if ((cbase & 7) == 0) {
-            __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
-            const float al = (float)P.alpha;
-            for (int part = 0; part < 2; part++) {
-              float x[64];
-              tmem_ld64(trow + (uint32_t)(part * BN + c0), x);
-#pragma unroll
-              for (int j = 0; j < 64; j++) x[j] = iters == 0 ? 0.f : al * x[j];
-              store_pieces64_staged(P, o + (i64)part * P.out_np * P.plane, roff, imok, cbase, x, sbuf, lane);
-            }
-            c0 += 64;
-            continue;
-          }
-        }
-        float vr[16], vi[16];
-        tmem_ld16(trow + (uint32_t)c0, vr);
-        tmem_ld16(trow + (uint32_t)(BN + c0), vi);
-        if (iters == 0) {
-#pragma unroll
-          for (int j = 0; j < 16; j++) vr[j] = vi[j] = 0.f;
-        }
-        c0 += 16;
-        i64 cbase;
-        const bool fast = chunk_base(P, nf, cbase);
-        if (!P.out_pieces && fast && P.cs_lo == 1) {  // warp-uniform
-          store_fp64_16_staged(P, roff, imok, cbase, vr, vi, (double2 *)wbuf, lane);
-          continue;
-        }
-        if (!mok) continue;
-        if (P.out_pieces) {
-          __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
-          if (rows_contig && fast && (cbase & 7) == 0 && (P.cs_lo & 7) == 0) {
-            store_pieces16_rows(P, o, roff0, cbase, nf, vr, sbuf, lane);
-            store_pieces16_rows(P, o + (i64)P.out_np * P.plane, roff0, cbase, nf, vi, sbuf, lane);
-          } else {
-            store_pieces16(P, o, roff, cbase, fast, nf, vr);
-            store_pieces16(P, o + (i64)P.out_np * P.plane, roff, cbase, fast, nf, vi);
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 16; j++) {
-            const int n = nf + j;
-            if (n >= P.N) break;
-            const i64 off = roff + (fast ? cbase + (i64)j * P.cs_lo : col_off(P, n));
-            double2 *o = (double2 *)P.out + off;
-            const double xr = P.alpha * (double)vr[j], xi = P.alpha * (double)vi[j];
-            if (P.atomic) {
-              atomicAdd(&o->x, xr);
-              atomicAdd(&o->y, xi);
-            } else if (P.accumulate) {
-              double2 t = *o;
-              t.x += xr;
-              t.y += xi;
-              *o = t;
-            } else {
-              *o = make_double2(xr, xi);
-            }
-          }
-        }
-      }
-    }
+    if (ok) epilogue_tile<BN>(P, m0, n0, b, warp, lane, tmem, iters == 0, smem + warp * STAGE_WARP_BYTES);
   }
   tc_fence_before();
   __syncthreads();
@@ -592,6 +600,197 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
     __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+  }
+}
+
+// Persistent variant of the one-load kernel: one CTA per SM walks a static list of tiles
+// (tile t, t + gridDim.x, ...), and TMEM holds two accumulators, so that the epilogue warps
+// store tile i while the MMA warp accumulates tile i+1 and the TMA warp loads ahead across
+// tile boundaries.  Barriers: full / empty per stage (TMA -> MMA -> TMA), tfull per
+// accumulator (MMA -> epilogue, tcgen05.commit), tempty per accumulator (the four epilogue
+// warps -> MMA).  Every wait is bounded; on give-up the roles stop, the TMA warp waits for
+// the loads it issued and the MMA warp for the MMAs it issued before TMEM is released.
+constexpr int P_EPI_BYTES = 4 * STAGE_WARP_BYTES;  // epilogue staging, apart from the stages
+constexpr int psmem_bytes(int stage_bytes, int stages) { return stages * stage_bytes + P_EPI_BYTES + 1024 + 256; }
+
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
+template <int BN, int STAGES, int BKT>
+__global__ void __launch_bounds__(THREADS, 1)
+    split_gemm_persist_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                              const __grid_constant__ Params P, int ntn, int ntm, int ntiles) {
+  static_assert(BN <= 128, "two accumulators of 2 BN TMEM columns must fit in 512 columns");
+  constexpr int A_TILE = BM * BKT * 2;
+  constexpr int B_BYTES = BN * BKT * 2;
+  constexpr uint32_t TCOLS = 2 * BN;     // one accumulator: real [0, BN), imaginary [BN, 2 BN)
+  constexpr uint32_t TALLOC = 2 * TCOLS;
+  constexpr uint32_t IDESC = idesc_for(BN);
+  constexpr uint32_t IDESC2 = idesc_for(BN * 2);
+  extern __shared__ uint8_t sraw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)sraw + 1023) & ~(uintptr_t)1023);
+  uint8_t *epi = smem + STAGES * P.stage_bytes;
+  uint64_t *bar = (uint64_t *)(epi + P_EPI_BYTES);  // full[ST], empty[ST], tfull[2], tempty[2], done
+  uint32_t *tmem_slot = (uint32_t *)(bar + 2 * STAGES + 5);
+  __shared__ int s_skip;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t full0 = smem_u32(bar), empty0 = smem_u32(bar + STAGES), tfull0 = smem_u32(bar + 2 * STAGES),
+                 tempty0 = smem_u32(bar + 2 * STAGES + 2), done = smem_u32(bar + 2 * STAGES + 4);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(tfull0 + 8 * i, 1);
+      mbar_init(tempty0 + 8 * i, 4);  // one arrival per epilogue warp
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_skip = *(volatile int *)P.err != 0;
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TALLOC));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int first = s_skip ? ntiles : (int)blockIdx.x;
+  // tile t: column tile fastest, then row tile, then batch x K split (the grid order of the
+  // non-persistent kernel)
+  auto decode = [&](int t, int &n0, int &m0, int &b, int &kb0, int &nkb) {
+    const int nt = t % ntn, r = t / ntn, mt = r % ntm, z = r / ntm;
+    b = z / P.ksplit;
+    const int ks = z - b * P.ksplit;
+    n0 = nt * BN;
+    m0 = mt * BM;
+    kb0 = ks * P.kb_per_split;
+    nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
+  };
+
+  if (warp == 4 && lane == 0) {
+    // ---- TMA producer
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    int g = 0;
+    bool stop = false;
+    for (int t = first; t < ntiles && !stop; t += gridDim.x) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      const int ab = P.a_nb > 1 ? P.a_b0 + b : 0, bb = P.b_nb > 1 ? P.b_b0 + b : 0;
+      for (int it = 0; it < nkb; it++) {
+        const int s = g % STAGES;
+        const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+        if (g >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) {
+          stop = true;
+          break;
+        }
+        const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+        mbar_expect_tx(full0 + 8 * s, P.stage_bytes);
+        const int kb = kb0 + it;
+        const uint32_t bbase = base + P.np * P.nA * A_TILE;
+        for (int p = 0; p < P.np; p++) {
+          for (int i = 0; i < P.nA; i++)
+            tma_load_3d(base + (p * P.nA + i) * A_TILE, &tmA, full0 + 8 * s, kb * BKT, m0,
+                        (P.a_comp[i] * P.np + p) * P.a_nb + ab);
+          for (int j = 0; j < P.nB; j++)
+            tma_load_3d(bbase + (p * P.nB + j) * B_BYTES, &tmB, full0 + 8 * s, kb * BKT, n0,
+                        (P.b_comp[j] * P.np + p) * P.b_nb + bb);
+        }
+        g++;
+      }
+    }
+    // the loads of the last STAGES issued stages may still be in flight: wait for them
+    for (int j = max(0, g - STAGES); j < g; j++)
+      mbar_wait_drain(full0 + 8 * (j % STAGES), (uint32_t)(j / STAGES) & 1u, P.err, 4);
+  } else if (warp == 5 && lane == 0) {
+    // ---- MMA issuer
+    int g = 0, lt = 0;
+    bool stop = false;
+    for (int t = first; t < ntiles && !stop; t += gridDim.x, lt++) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      const int bi = lt & 1;
+      const uint32_t tacc = tmem + (uint32_t)bi * TCOLS;
+      // accumulator bi is free once the epilogue has stored tile lt - 2
+      if (lt >= 2 && !mbar_wait(tempty0 + 8 * bi, (uint32_t)((lt >> 1) - 1) & 1u, P.err, 5)) break;
+      tc_fence_after();
+      bool started0 = false, started1 = false;
+      for (int it = 0; it < nkb; it++) {
+        const int s = g % STAGES;
+        const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+        if (!mbar_wait(full0 + 8 * s, ph, P.err, 2)) {
+          stop = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+        const uint32_t bbase = base + P.np * P.nA * A_TILE;
+        for (int pr = 0; pr < P.nprod; pr++) {
+          const int sa0 = P.pa[pr] * P.nA, sb0 = P.pb[pr] * P.nB;
+          if (P.fuse) {
+            const uint64_t da = op_desc<BKT>(base + sa0 * A_TILE);
+            const uint64_t db = op_desc<BKT>(bbase + sb0 * B_BYTES);
+#pragma unroll
+            for (int k = 0; k < BKT / 16; k++)
+              mma_bf16(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), IDESC2, (started0 || k > 0) ? 1u : 0u);
+            started0 = started1 = true;
+            continue;
+          }
+          for (int q = 0; q < P.nmma; q++) {
+            const Mma mq = P.mma[q];
+            const uint64_t da = op_desc<BKT>(base + (sa0 + mq.sa) * A_TILE);
+            const uint64_t db = op_desc<BKT>(bbase + (sb0 + mq.sb) * B_BYTES);
+            const uint32_t idesc = IDESC | (mq.neg ? (1u << 13) : 0u);
+            const uint32_t ta = tacc + (uint32_t)(mq.acc * BN);
+#pragma unroll
+            for (int k = 0; k < BKT / 16; k++)
+              mma_bf16(ta, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                       ((mq.acc ? started1 : started0) || k > 0) ? 1u : 0u);
+            if (mq.acc)
+              started1 = true;
+            else
+              started0 = true;
+          }
+        }
+        mma_commit(empty0 + 8 * s);
+        g++;
+      }
+      if (stop) break;
+      mma_commit(tfull0 + 8 * bi);
+    }
+    // every MMA this thread issued has finished before TMEM is released
+    mma_commit(done);
+    mbar_wait_drain(done, 0, P.err, 3);
+  } else if (warp < 4) {
+    // ---- epilogue: tile lt from accumulator lt & 1, then hand the accumulator back
+    int lt = 0;
+    for (int t = first; t < ntiles; t += gridDim.x, lt++) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      const int bi = lt & 1;
+      int okl = 0;
+      if (lane == 0) okl = mbar_wait(tfull0 + 8 * bi, (uint32_t)(lt >> 1) & 1u, P.err, 3) ? 1 : 0;
+      __syncwarp();
+      if (!__shfl_sync(0xffffffffu, okl, 0)) break;
+      tc_fence_after();
+      epilogue_tile<BN>(P, m0, n0, b, warp, lane, tmem + (uint32_t)bi * TCOLS, nkb == 0,
+                        epi + warp * STAGE_WARP_BYTES);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty0 + 8 * bi);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TALLOC));
   }
 }
 
@@ -754,6 +953,32 @@ void launch(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 
   NEDY_CHECK_LAUNCH();
 }
 
+// persistent kernel: one CTA per SM (TMEM holds its two accumulators), at most one per tile
+template <int BN, int STAGES, int BKT>
+void launch_persist(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 grid, cudaStream_t s) {
+  static std::atomic<bool> attr[64];  // per device (host threads may race here)
+  static std::atomic<int> sms_of[64];
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  const int bytes = psmem_bytes(P.stage_bytes, STAGES);
+  NEDY_REQUIRE(STAGES * P.stage_bytes + P_EPI_BYTES <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  if (!attr[dev].load()) {
+    int sms = 0;
+    NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    sms_of[dev].store(sms);
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_persist_kernel<BN, STAGES, BKT>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT + 1024 + 256));
+    attr[dev].store(true);
+  }
+  const long long ntiles = (long long)grid.x * grid.y * grid.z;
+  NEDY_REQUIRE(ntiles < (1LL << 31), "split_gemm: too many tiles");
+  const int nct = (int)std::min<long long>(ntiles, std::max(1, sms_of[dev].load()));
+  split_gemm_persist_kernel<BN, STAGES, BKT><<<nct, THREADS, bytes, s>>>(ma, mb, P, (int)grid.x, (int)grid.y,
+                                                                         (int)ntiles);
+  NEDY_CHECK_LAUNCH();
+}
+
 // ---- autotuner: the tile shape (BN, stages) of each problem class is chosen by timing
 // the candidates on the live launches.  Every candidate computes the same result; the
 // first launches of a class cycle through the candidates with CUDA events around them,
@@ -762,6 +987,7 @@ namespace {
 struct Cand {
   int bn, stages, kdiv;  // kdiv: divide the automatic K split by this (FP64-accumulating outputs)
   int bk;                // 0: per-product kernel (64-wide K blocks); 32 / 64: one-load kernel
+  int persist = 0;       // 1: persistent one-load kernel (two TMEM accumulators)
 };
 struct TuneKey {
   int dev, np, nA, nB, out_pieces, acc, M, N, kpad;
@@ -825,6 +1051,10 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
       c.push_back({bn, 2, 1, bk});
       if (st >= 3) c.push_back({bn, std::min(st, 4), 1, bk});
       if (acc && bn == 256) c.push_back({bn, 2, 2, bk});
+      if (bn == 128) {  // persistent: the epilogue of one tile beside the MMAs of the next
+        const int pst = std::min(bk == 32 ? 3 : 2, (SMEM_LIMIT - P_EPI_BYTES) / sb);
+        if (pst >= 2) c.push_back({bn, pst, 1, bk, 1});
+      }
     }
   }
   return c;
@@ -884,7 +1114,7 @@ std::string split_tune_report() {
     for (size_t i = 0; i < e.cands.size(); i++) {
       char buf[96];
       char ol[16] = "";
-      if (e.cands[i].bk) snprintf(ol, sizeof(ol), "/ol%d", e.cands[i].bk);
+      if (e.cands[i].bk) snprintf(ol, sizeof(ol), "/ol%d%s", e.cands[i].bk, e.cands[i].persist ? "p" : "");
       snprintf(buf, sizeof(buf), " %d/%d/k%d%s=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv, ol,
                e.trials[i] ? e.best[i] * 1e3 : -1.0, (int)i == e.chosen ? "*" : "");
       r += buf;
@@ -947,6 +1177,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   int STsel = 0;  // 0: as many stages as fit
   int KDsel = 1;
   int BKsel = 0;  // per-product kernel
+  int PSsel = 0;  // persistent kernel
   if (BNsel >= 128 && 2 * stage_bytes_for(P.nA, P.nB, P.np, BNsel, 32) <= SMEM_LIMIT) {
     BKsel = 32;
     STsel = 2;
@@ -963,10 +1194,13 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 64 || g.force_stages == 4 || g.force_stages == 2,
                  "split_gemm: 64-wide tiles use 2 or 4 stages");
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
+    NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && g.force_bn == 128),
+                 "split_gemm: the persistent kernel is the one-load kernel with 128-wide tiles");
     BNsel = g.force_bn;
     STsel = g.force_stages;
     KDsel = g.force_kdiv;
     BKsel = g.force_bk;
+    PSsel = g.force_persist ? 1 : 0;
   } else {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (g_tune_on) {
@@ -996,6 +1230,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
         STsel = e.cands[c].stages;
         KDsel = e.cands[c].kdiv;
         BKsel = e.cands[c].bk;
+        PSsel = e.cands[c].persist;
       }
     }
   }
@@ -1057,7 +1292,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     }
   }
   const int stages = STsel ? STsel : BNsel == 128 ? 2 : std::min(4, SMEM_LIMIT / P.stage_bytes);
-  NEDY_REQUIRE(stages >= 2 && stages * P.stage_bytes <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  NEDY_REQUIRE(stages >= 2 && stages * P.stage_bytes + (PSsel ? P_EPI_BYTES : 0) <= SMEM_LIMIT,
+               "split_gemm: stages exceed shared memory");
   cudaEvent_t tev[2] = {nullptr, nullptr};
   if (te) {
     NEDY_CUDA(cudaEventCreate(&tev[0]));
@@ -1068,14 +1304,18 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   struct Inst {
     int bk, bn, st;
     LaunchFn fn;
+    int persist;
   };
   static const Inst insts[] = {
-      {0, 64, 4, launch<64, 4>},          {0, 64, 2, launch<64, 2>},          {0, 128, 2, launch<128, 2>},        {0, 128, 3, launch<128, 3>},
-      {0, 128, 4, launch<128, 4>},        {0, 256, 2, launch<256, 2>},        {0, 256, 3, launch<256, 3>},
-      {32, 128, 2, launch<128, 2, 32, true>}, {32, 128, 3, launch<128, 3, 32, true>},
-      {32, 128, 4, launch<128, 4, 32, true>}, {32, 256, 2, launch<256, 2, 32, true>},
-      {32, 256, 3, launch<256, 3, 32, true>}, {64, 128, 2, launch<128, 2, 64, true>},
-      {64, 128, 3, launch<128, 3, 64, true>}};
+      {0, 64, 4, launch<64, 4>, 0},       {0, 64, 2, launch<64, 2>, 0},       {0, 128, 2, launch<128, 2>, 0},
+      {0, 128, 3, launch<128, 3>, 0},     {0, 128, 4, launch<128, 4>, 0},     {0, 256, 2, launch<256, 2>, 0},
+      {0, 256, 3, launch<256, 3>, 0},
+      {32, 128, 2, launch<128, 2, 32, true>, 0}, {32, 128, 3, launch<128, 3, 32, true>, 0},
+      {32, 128, 4, launch<128, 4, 32, true>, 0}, {32, 256, 2, launch<256, 2, 32, true>, 0},
+      {32, 256, 3, launch<256, 3, 32, true>, 0}, {64, 128, 2, launch<128, 2, 64, true>, 0},
+      {64, 128, 3, launch<128, 3, 64, true>, 0},
+      {32, 128, 2, launch_persist<128, 2, 32>, 1}, {32, 128, 3, launch_persist<128, 3, 32>, 1},
+      {64, 128, 2, launch_persist<128, 2, 64>, 1}};
   int st_run = stages;
   if (BKsel == 0) {  // per-product kernel: the instance nearest to the requested stages
     st_run = BNsel == 64 ? (stages <= 2 ? 2 : 4)
@@ -1083,7 +1323,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   }
   LaunchFn fn = nullptr;
   for (const Inst &x : insts)
-    if (x.bk == BKsel && x.bn == BNsel && x.st == st_run) fn = x.fn;
+    if (x.bk == BKsel && x.bn == BNsel && x.st == st_run && x.persist == PSsel) fn = x.fn;
   NEDY_REQUIRE(fn != nullptr, "split_gemm: no kernel instance for this tile shape");
   fn(P, ma, mb, grid, s);
   if (te) {
@@ -1208,6 +1448,7 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
     g.conjA = k.conjA != 0; g.conjB = k.conjB != 0;
     g.alpha = k.alpha;
     g.force_bn = k.bn; g.force_stages = k.stages; g.force_bk = k.bk; g.force_kdiv = k.kdiv;
+    g.force_persist = k.persist;
     double2 *got = C;
     if (k.out_pieces) {
       Pieces cp;

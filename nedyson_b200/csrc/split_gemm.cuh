@@ -51,6 +51,7 @@ struct SplitGemmArgs {
   // a given kernel instance instead of the autotuner's (force_bn 0: autotuner); force_bk 0
   // is the per-product kernel, 32 / 64 the one-load kernel with that K block
   int force_bn = 0, force_stages = 0, force_bk = 0, force_kdiv = 1;
+  int force_persist = 0;  // with force_bn: the persistent one-load kernel (force_bk 32 / 64, force_bn 128)
 };
 
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
@@ -61,7 +62,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
 struct SplitCheck {
   int M = 0, N = 0, K = 0, nb = 1;
   int a_cplx = 1, b_cplx = 1, conjA = 0, conjB = 0, np = 3, out_pieces = 0, accumulate = 0;
-  int bn = 128, stages = 2, bk = 0, kdiv = 1;
+  int bn = 128, stages = 2, bk = 0, kdiv = 1, persist = 0;
   double alpha = 1.0;
   unsigned long long seed = 1;
 };

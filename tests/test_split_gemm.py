@@ -26,10 +26,14 @@ SHAPES = {
     "cxr_conjA": (256, 320, 128, 1, 1, 0, 1, 0, 0, 0),     # complex x real, ragged last tile
     "cxc_n64_acc": (64, 64, 2048, 3, 1, 1, 0, 1, 0, 1),    # one 64-wide tile per batch
 }
-# (tile_n, stages, k_block, kdiv); k_block 0: per-product kernel, 32 / 64: one-load kernel
-INSTANCES = [(64, 4, 0, 1), (64, 4, 0, 2), (64, 4, 0, 4), (64, 2, 0, 1), (64, 2, 0, 2), (128, 2, 0, 1), (128, 3, 0, 1), (128, 4, 0, 1),
-             (256, 2, 0, 1), (256, 3, 0, 1), (256, 2, 0, 2), (128, 2, 32, 1), (128, 3, 32, 1), (128, 4, 32, 1),
-             (256, 2, 32, 1), (256, 3, 32, 1), (256, 2, 32, 2), (128, 2, 64, 1), (128, 3, 64, 1)]
+# (tile_n, stages, k_block, kdiv, persistent); k_block 0: per-product kernel, 32 / 64: one-load
+# kernel; persistent: the one-load kernel with one CTA per SM over a tile list and two TMEM
+# accumulators (the epilogue of one tile beside the MMAs of the next)
+INSTANCES = [(64, 4, 0, 1, 0), (64, 4, 0, 2, 0), (64, 4, 0, 4, 0), (64, 2, 0, 1, 0), (64, 2, 0, 2, 0), (128, 2, 0, 1, 0),
+             (128, 3, 0, 1, 0), (128, 4, 0, 1, 0), (256, 2, 0, 1, 0), (256, 3, 0, 1, 0), (256, 2, 0, 2, 0),
+             (128, 2, 32, 1, 0), (128, 3, 32, 1, 0), (128, 4, 32, 1, 0), (256, 2, 32, 1, 0), (256, 3, 32, 1, 0),
+             (256, 2, 32, 2, 0), (128, 2, 64, 1, 0), (128, 3, 64, 1, 0),
+             (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1)]
 
 
 @pytest.mark.parametrize("np_", [2, 3])
@@ -38,24 +42,28 @@ def test_split_gemm_instances(shape, np_):
     lib = _lib.lib()
     M, N, K, nb, ac, bc, ca, cb, op, acc = SHAPES[shape]
     ran = []
-    for (bn, st, bk, kd) in INSTANCES:
+    for (bn, st, bk, kd, ps) in INSTANCES:
         err = C.c_double(-1.0)
-        rc = lib.nedy_split_gemm_check(0, M, N, K, nb, ac, bc, ca, cb, np_, op, acc, bn, st, bk, kd, 17,
+        rc = lib.nedy_split_gemm_check(0, M, N, K, nb, ac, bc, ca, cb, np_, op, acc, bn, st, bk, kd, ps, 17,
                                        C.byref(err))
         if rc == NEDY_ERR_ARG:  # instance absent or too large for shared memory
             continue
-        assert rc == NEDY_OK, (shape, bn, st, bk, kd, lib.nedy_last_error())
-        print(f"{shape} np={np_} {bn}/{st}/bk{bk}/k{kd}: {err.value:.3e}")
-        assert 0.0 < err.value < TOL[np_], (shape, np_, bn, st, bk, kd, err.value)
-        ran.append((bn, st, bk, kd))
+        assert rc == NEDY_OK, (shape, bn, st, bk, kd, ps, lib.nedy_last_error())
+        print(f"{shape} np={np_} {bn}/{st}/bk{bk}/k{kd}{'/persistent' if ps else ''}: {err.value:.3e}")
+        assert 0.0 < err.value < TOL[np_], (shape, np_, bn, st, bk, kd, ps, err.value)
+        ran.append((bn, st, bk, kd, ps))
     assert len(ran) >= 3, ran
     if N > 64:
-        assert any(bk for (_, _, bk, _) in ran), "no one-load instance ran"
+        assert any(bk for (_, _, bk, _, _) in ran), "no one-load instance ran"
+        assert any(ps for (*_, ps) in ran), "no persistent instance ran"
 
 
 def test_split_gemm_check_rejects_missing_instance():
     err = C.c_double()
-    rc = _lib.lib().nedy_split_gemm_check(0, 128, 128, 64, 1, 1, 1, 0, 0, 2, 0, 0, 96, 2, 0, 1, 1, C.byref(err))
+    rc = _lib.lib().nedy_split_gemm_check(0, 128, 128, 64, 1, 1, 1, 0, 0, 2, 0, 0, 96, 2, 0, 1, 0, 1, C.byref(err))
+    assert rc == NEDY_ERR_ARG
+    # the persistent kernel exists only as the one-load kernel with 128-wide tiles
+    rc = _lib.lib().nedy_split_gemm_check(0, 128, 256, 64, 1, 1, 1, 0, 0, 2, 0, 0, 256, 2, 32, 1, 1, 1, C.byref(err))
     assert rc == NEDY_ERR_ARG
 
 
