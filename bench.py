@@ -98,6 +98,10 @@ def parse():
                     help="pieces per operand of the split self-energy (bf16x2: hi*hi + hi*lo + lo*hi)")
     ap.add_argument("--split-only", action="store_true",
                     help="time the split+predictor form alone (profiling runs; no plain-form comparison)")
+    ap.add_argument("--config1", action="store_true",
+                    help="instead of the headline: the whole config-1 trajectory (restricted DF GF2, nao=32, "
+                         "naux=128, ntau=256, beta=20, dt=0.01, nt=1000, Gaussian pulse) in FP64 on the GPU")
+    ap.add_argument("--config1-nt", type=int, default=1000)
     ap.add_argument("--batch", type=int, default=64,
                     help="instances of the batched workload (0: skip it): nao uniform in [8,48], naux=4 nao")
     ap.add_argument("--batch-steps", type=int, default=3, help="timed steps of the batched workload")
@@ -703,6 +707,56 @@ def run_batch(args, dist: Dist):
     return res
 
 
+def run_config1(args):
+    """Config 1 at its stated sizes: restricted density-fitted GF2, nao=32, naux=128, ntau=256,
+    beta=20, k=5, dt=0.01, Gaussian pulse E0=0.05 t0=2 sigma=0.5 along D, FP64 throughout, from
+    the GF2 equilibrium: bootstrap, then every step to nt with the reference's 5 corrector
+    iterations (nedy_decomp_tstp).  Reports timesteps/s over the whole trajectory (device
+    time), the energies at the end and the device memory the run held."""
+    import torch
+    from nedyson_b200 import api
+    from nedyson_b200.inputs import make_problem, gf2_equilibrium
+    from nedyson_b200.simulation import DecompSimulation
+    nt, ntau, beta, dt = args.config1_nt, 256, 20.0, 0.01
+    p = make_problem(32, 128, args.seed)
+    t0 = time.time()
+    ectx = api.Context(5, ntau, 32, 5, beta, dt)
+    eq = gf2_equilibrium(ectx, p, beta)
+    ectx.close()
+    sim = DecompSimulation(p, nt, ntau, beta, dt, corr_steps=5, drive_kind="gauss",
+                           drive_kw={"E0": 0.05, "t0": 2.0, "sigma": 0.5})
+    sim.set_equilibrium(eq["F"][0], eq["Gmat"][0])
+    sim.free_gf()
+    berr = sim.do_boot(max_iter=40)
+    prep = time.time() - t0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    marks = {}
+    for t in range(6, nt + 1):
+        sim.do_tstp(t)
+        if t in (100, 250, 500, 750, 1000):
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            marks[t] = ev
+    e1.record()
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    d = api.dyson(sim.ctx)
+    e_corr = d.energy_conv(nt, sim.Sigma, sim.G)
+    rho = -1j * sim.G.download(0, nt * (nt + 1) // 2 + nt, 1)[0]  # rho = i sig G^<(nt, nt), sig = -1
+    free, total = torch.cuda.mem_get_info()
+    line = {"workload": "config 1: restricted density-fitted GF2, nao=32 naux=128 ntau=256 beta=20 k=5 dt=0.01 "
+                        f"nt={nt}, Gaussian pulse E0=0.05 t0=2 sigma=0.5, FP64, 5 corrector iterations per step, "
+                        "from the GF2 equilibrium",
+            "steps": nt - 5, "seconds": secs, "timesteps_s": (nt - 5) / secs,
+            "seconds_at": {str(t): e0.elapsed_time(ev) / 1e3 for t, ev in marks.items()},
+            "equilibrium_iterations": eq["iters"], "boot_err": berr, "preparation_s": prep,
+            "E_corr_at_nt": e_corr, "device_memory_used_gb": (total - free) / 1e9,
+            "electrons_at_nt": float(np.trace(rho).real)}
+    print(json.dumps(line), flush=True)
+
+
 def train_predictor(ctx, args):
     """Train the learned predictor on short GF2 trajectories of small molecules (nao=8,
     naux=24, Gaussian pulses of different strength and width), generated by the engine
@@ -782,6 +836,11 @@ def main():
         dist.close()
         return
 
+    if args.config1:
+        if dist.rank == 0:
+            run_config1(args)
+        dist.close()
+        return
     fp64 = fp64_gemm_peak(dist.local) if dist.rank == 0 else None
     r = run_engine(args, dist)
     import gc
