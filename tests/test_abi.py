@@ -70,3 +70,23 @@ def test_step_entry_points_reject_null_handles(libpath):
     assert L.nedy_decomp_spin_tstp(None, 6, None, None, None, None, None, None, None, None, 0.0, 0.0, 5,
                                    C.byref(e)) == 1
     assert L.nedy_ctx_set_precision(None, 2) == 1
+
+
+def test_new_entry_points_reject_bad_arguments(libpath):
+    """Full-U step, batch, Matsubara solver and the error hook check their arguments before
+    touching a device."""
+    import ctypes as C
+    from nedyson_b200 import _lib
+    L = _lib.lib()
+    e = C.c_double()
+    assert L.nedy_full_tstp(None, 6, None, None, None, None, 0.0, 5, C.byref(e)) == 1
+    out = C.c_void_p()
+    assert L.nedy_batch_create(None, 0, 0, C.byref(out)) == 1
+    inst = (_lib.BatchInstance * 1)()
+    assert L.nedy_batch_create(inst, 1, 0, C.byref(out)) == 1  # null handles inside
+    assert b"instance 0" in L.nedy_last_error()
+    assert L.nedy_batch_tstp(None, 6, 1, 0.0, None) == 1
+    assert L.nedy_batch_destroy(None) == 0
+    arr = (C.c_void_p * 1)()
+    assert L.nedy_matsubara_gf2(None, 1, arr, arr, arr, arr, arr, 1.0, 10, 1e-12, None, None) == 1
+    assert L.nedy_ctx_inject_split_error(None, 2) == 1
