@@ -55,7 +55,8 @@ def test_split_gemm_instances(shape, np_):
     assert len(ran) >= 3, ran
     if N > 64:
         assert any(bk for (_, _, bk, _, _) in ran), "no one-load instance ran"
-        assert any(ps for (*_, ps) in ran), "no persistent instance ran"
+        if not (ac and bc and np_ == 3):  # complex x complex, three pieces: two stages do not fit with it
+            assert any(ps for (*_, ps) in ran), "no persistent instance ran"
 
 
 def test_split_gemm_check_rejects_missing_instance():
