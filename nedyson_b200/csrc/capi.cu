@@ -49,18 +49,27 @@ size_t Arena::capacity() const {
   for (auto &b : blocks_) s += b.cap;
   return s;
 }
+char *Arena::alloc_block(size_t bytes) {
+  char *p = nullptr;
+  cudaError_t e = stream_ ? cudaMallocAsync((void **)&p, bytes, stream_) : cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw CudaError("workspace allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  return p;
+}
 void Arena::reset() {
   if (blocks_.size() > 1) {
-    size_t total = capacity();
-    NEDY_CUDA(cudaDeviceSynchronize());
-    for (auto &b : blocks_) cudaFree(b.p);
-    blocks_.clear();
-    char *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, total);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      throw CudaError("workspace allocation of " + std::to_string(total) + " bytes failed: " + cudaGetErrorString(e));
+    // the blocks were used by work queued on stream_ only: free and reallocate in its order
+    const size_t total = capacity() + capacity() / 2;
+    for (auto &b : blocks_) {
+      if (stream_)
+        NEDY_CUDA(cudaFreeAsync(b.p, stream_));
+      else
+        cudaFree(b.p);
     }
+    blocks_.clear();
+    char *p = alloc_block(total);
     blocks_.push_back({p, total, 0});
   }
   for (auto &b : blocks_) b.top = 0;
@@ -74,13 +83,8 @@ void *Arena::get(size_t bytes) {
     b.top += need;
     return p;
   }
-  size_t cap = std::max(need, (size_t)64 << 20);
-  char *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, cap);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    throw CudaError("workspace allocation of " + std::to_string(cap) + " bytes failed: " + cudaGetErrorString(e));
-  }
+  const size_t cap = std::max(need, (size_t)64 << 20);
+  char *p = alloc_block(cap);
   blocks_.push_back({p, cap, need});
   return p;
 }
@@ -140,10 +144,13 @@ static void save_row(Ctx &c, const DevGF &g, int T, int slot = 0) {
   RowRanges r = row_ranges(g, T);
   const i64 tot = r.n[0] + r.n[1] + r.n[2];
   if (c.rowcopy_cap < 2 * tot) {
+    // rows grow with T: size the copy for the longest row of the run, so that it is
+    // allocated once (a cudaFree per step would synchronise the whole device)
+    const i64 cap = std::max<i64>(2 * tot, 2 * row_len(g, g.nt));
     if (c.rowcopy) cudaFree(c.rowcopy);
     c.rowcopy = nullptr;
-    NEDY_CUDA(cudaMalloc(&c.rowcopy, sizeof(double2) * 2 * tot));
-    c.rowcopy_cap = 2 * tot;
+    NEDY_CUDA(cudaMalloc(&c.rowcopy, sizeof(double2) * cap));
+    c.rowcopy_cap = cap;
   }
   i64 o = slot * tot;
   for (int k = 0; k < 3; k++) {
@@ -259,6 +266,7 @@ int nedy_ctx_create(const nedy_config *cfg, nedy_ctx **out) {
     try {
       NEDY_CUDA(cudaSetDevice(c.device));
       NEDY_CUDA(cudaStreamCreate(&c.stream));
+      c.ws.set_stream(c.stream);
       c.W = make_weights(c.k);
       c.col = make_colloc(c.ntau);
     } catch (...) {
@@ -838,11 +846,12 @@ void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *co
   const i64 npred = c.pred ? Predictor::row_elements(G[0]->g, tstp) : 0;
   const bool learned = c.pred && c.pred_active && npred > 0;
   if (learned) {
-    if (c.pred_corr_cap < nspin * npred) {
+    if (c.pred_corr_cap < nspin * npred) {  // sized for the longest row of the run (allocated once)
+      const i64 cap = std::max<i64>(nspin * npred, nspin * Predictor::row_elements(G[0]->g, G[0]->g.nt));
       if (c.pred_corr) cudaFree(c.pred_corr);
       c.pred_corr = nullptr;
-      NEDY_CUDA(cudaMalloc(&c.pred_corr, sizeof(double2) * nspin * npred));
-      c.pred_corr_cap = nspin * npred;
+      NEDY_CUDA(cudaMalloc(&c.pred_corr, sizeof(double2) * cap));
+      c.pred_corr_cap = cap;
     }
     for (int s = 0; s < nspin; s++) c.pred->apply(G[s]->g, tstp, c.pred_corr + s * npred);
   }

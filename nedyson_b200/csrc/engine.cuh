@@ -24,10 +24,15 @@ struct DevGF {
 
 // Bump allocator for per-call workspace.  A request that does not fit opens a
 // further device block (live pointers stay valid); at the next reset() the blocks
-// are merged into one of the combined size, so steady-state calls allocate nothing.
+// are merged into one of 1.5 x the combined size, so steady-state calls allocate
+// nothing and a workspace that grows with the time step is rarely reallocated.
+// Blocks are allocated and freed in the order of the context's stream
+// (cudaMallocAsync / cudaFreeAsync): no device-wide synchronisation, so a context
+// that grows its workspace does not stall the streams of other contexts.
 class Arena {
  public:
   ~Arena();
+  void set_stream(cudaStream_t s) { stream_ = s; }
   void reset();
   void *get(size_t bytes);
   template <class T> T *alloc(i64 n) { return (T *)get(sizeof(T) * (size_t)n); }
@@ -36,6 +41,8 @@ class Arena {
  private:
   struct Block { char *p; size_t cap, top; };
   std::vector<Block> blocks_;
+  cudaStream_t stream_ = nullptr;
+  char *alloc_block(size_t bytes);
 };
 
 // Calculus weights (host tables) -- the restatement of Integration::Integrator
