@@ -120,6 +120,13 @@ int nedy_ctx_phase_times(const nedy_ctx *ctx, double *ms4);
  * that launched them returns NEDY_ERR_TIMEOUT; reporting clears the word, so the call
  * after that runs normally.  Lets a test drive the timeout path without a device fault. */
 int nedy_ctx_inject_split_error(nedy_ctx *ctx, int code);
+/* Dense solve X = A^-1 B of nb independent complex systems, A n x n and B n x nrhs each,
+ * row-major, interleaved (re, im) doubles in HOST memory; B is overwritten by X, A is left as
+ * it was.  The engine's replacement for the partial-pivot LU solves of the Dyson step and the
+ * bootstrap (Eigen PartialPivLU::solve at src/dyson_step.h:65, :163, :252 and
+ * src/dyson_boot.h:61, :170): Gauss-Jordan with partial pivoting on the context's stream, the
+ * same routine those steps use.  NEDY_ERR_SINGULAR on a zero pivot. */
+int nedy_dense_solve(nedy_ctx *ctx, int n, int nrhs, int nb, const double *A, double *B);
 /* Number of engine kernel launches issued by this process so far. */
 unsigned long long nedy_launch_count(void);
 /* Collocation nodes x_m in [-1,1] and weights (ntau+1 values each). */

@@ -49,6 +49,7 @@ SIGNATURES = {
     "nedy_ctx_set_timing": ([_P, _I], _I),
     "nedy_ctx_phase_times": ([_P, _DP], _I),
     "nedy_ctx_inject_split_error": ([_P, _I], _I),
+    "nedy_dense_solve": ([_P, _I, _I, _I, _P, _P], _I),
     "nedy_launch_count": ([], C.c_ulonglong),
     "nedy_gf_create": ([_P, _I, _I, _I, _I, _PP], _I),
     "nedy_gf_destroy": ([_P], _I),

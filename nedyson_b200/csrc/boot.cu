@@ -7,9 +7,6 @@
 #include <algorithm>
 
 namespace nedy {
-void gj_public(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB);
-void ensure_tables(Ctx &c);
-void check_status(Ctx &c);
 
 namespace {
 constexpr int TPB = 256;

@@ -373,6 +373,24 @@ int nedy_ctx_set_timing(nedy_ctx *ctx, int on) {
   });
 }
 
+int nedy_dense_solve(nedy_ctx *ctx, int n, int nrhs, int nb, const double *A, double *B) {
+  return guard([&] {
+    NEDY_REQUIRE(ctx && A && B, "null argument");
+    NEDY_REQUIRE(n > 0 && nrhs > 0 && nb > 0, "sizes must be positive");
+    set_dev(ctx);
+    Ctx &c = ctx->c;
+    c.ws.reset();
+    const i64 sa = (i64)n * n, sb = (i64)n * nrhs;
+    double2 *dA = c.ws.alloc<double2>(sa * nb), *dB = c.ws.alloc<double2>(sb * nb);
+    NEDY_CUDA(cudaMemcpyAsync(dA, A, sizeof(double2) * sa * nb, cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dB, B, sizeof(double2) * sb * nb, cudaMemcpyHostToDevice, c.stream));
+    gj_public(c, n, nrhs, nb, dA, sa, dB, sb);
+    check_status(c);
+    NEDY_CUDA(cudaMemcpyAsync(B, dB, sizeof(double2) * sb * nb, cudaMemcpyDeviceToHost, c.stream));
+    NEDY_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
 int nedy_ctx_inject_split_error(nedy_ctx *ctx, int code) {
   return guard([&] {
     NEDY_REQUIRE(ctx && code != 0, "null context or zero code");

@@ -14,6 +14,7 @@
 // M(t') = (i bd0/dt + mu) - hmf(t') - dt*w0*Sig^R(t',t'): for t' < T they no longer
 // change, so each step is a single block product instead of an LU solve.
 #include "sigma.cuh"
+#include <cooperative_groups.h>
 #include <atomic>
 #include <cmath>
 #include <algorithm>
@@ -232,10 +233,182 @@ __global__ void gj_coop_kernel(int n, int nrhs, double2 *A, double2 *B, int cw, 
   }
 }
 
+// ---------------------------------------------------------------------------------
+// Gauss-Jordan with partial pivoting on [A | B] held in shared memory: one thread-block
+// cluster of CL CTAs per system (system b = blockIdx.x / CL), CTA r of the cluster owns the
+// augmented columns [r cw, (r + 1) cw) of its system.  Step c: every CTA holds pivot column c
+// and the pivot row index p in its own shared memory (buffer c & 1, written there by the owner
+// of column c); it swaps rows c and p of its columns, scales the pivot row and eliminates the
+// other rows.  The owner of column c + 1 then picks the next pivot (largest |.|, first row on
+// ties) and stores column c + 1 and the pivot index into buffer (c + 1) & 1 of every CTA of
+// the cluster (distributed shared memory); the cluster barrier (release / acquire) orders
+// those stores before step c + 1, and the two buffers keep them clear of the reads of step c.
+// Columns of A at or left of the pivot are not updated any more (they are unit columns and
+// no longer read), and A in global memory is left as it was; B is overwritten by A^-1 B.
+// Every CTA runs the same n steps (a zero pivot is seen by all of them and ends all loops
+// together), so every barrier is reached by the whole cluster.
+constexpr int GJS_THREADS = 512;
+constexpr int GJS_SMEM_MAX = 225 * 1024;
+
+inline i64 gjs_smem_bytes(int n, int cw) { return ((i64)n * cw + 2 * (i64)n + cw) * 16 + 16; }
+
+__global__ void __launch_bounds__(GJS_THREADS, 1)
+    gj_smem_kernel(int n, int nrhs, const double2 *A, i64 sA, double2 *B, i64 sB, int cw, int *status) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int CL = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int sys = blockIdx.x / CL;
+  A += sys * sA;
+  B += sys * sB;
+  extern __shared__ double2 gsm[];
+  double2 *slab = gsm;                    // [n][cw]
+  double2 *facb = slab + (i64)n * cw;     // [2][n]: pivot column of the step, pre-swap
+  double2 *rowc = facb + 2 * (i64)n;      // [cw]: scaled pivot row, this CTA's columns
+  int *spiv = (int *)(rowc + cw);         // [2]: pivot row index of the step
+  __shared__ double rv[GJS_THREADS / 32];
+  __shared__ int ri[GJS_THREADS / 32];
+  const int W = n + nrhs, j0 = rank * cw, jn = max(0, min(cw, W - j0));
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (i64 idx = tid; idx < (i64)n * jn; idx += blockDim.x) {
+    const int r = (int)(idx / jn), jj = (int)(idx - (i64)r * jn), j = j0 + jj;
+    slab[(i64)r * cw + jj] = j < n ? A[(i64)r * n + j] : B[(i64)r * nrhs + (j - n)];
+  }
+  cl.sync();  // every CTA of the cluster has started before any stores into its shared memory
+  // the owner of column c picks the pivot among rows >= c and hands column c to every CTA
+  auto publish = [&](int c) {
+    const int lc = c - j0;
+    double best = -1.0;
+    int bi = n;
+    for (int r = c + tid; r < n; r += blockDim.x) {
+      const double2 v = slab[(i64)r * cw + lc];
+      const double a = v.x * v.x + v.y * v.y;
+      if (a > best) { best = a; bi = r; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_down_sync(0xffffffffu, best, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (lane == 0) { rv[wid] = best; ri[wid] = bi; }
+    __syncthreads();
+    if (wid == 0) {
+      best = lane < (int)(blockDim.x >> 5) ? rv[lane] : -1.0;
+      bi = lane < (int)(blockDim.x >> 5) ? ri[lane] : n;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) ri[0] = bi < n ? bi : c;
+    }
+    __syncthreads();
+    const int p = ri[0], buf = c & 1;
+    for (int t = 0; t < CL; t++) {
+      double2 *dst = cl.map_shared_rank(facb + (i64)buf * n, t);
+      for (int r = tid; r < n; r += blockDim.x) dst[r] = slab[(i64)r * cw + lc];
+      if (tid == 0) *cl.map_shared_rank(spiv + buf, t) = p;
+    }
+  };
+  if (j0 == 0 && jn > 0) publish(0);
+  cl.sync();
+  for (int c = 0; c < n; c++) {
+    const int buf = c & 1, p = spiv[buf];
+    const double2 *f = facb + (i64)buf * n;
+    const double2 pv = f[p];
+    if (pv.x == 0.0 && pv.y == 0.0) {  // the same in every CTA of the cluster
+      if (rank == 0 && tid == 0 && status) status[sys] = 1;
+      break;
+    }
+    const double dd = pv.x * pv.x + pv.y * pv.y;
+    const double2 inv = make_double2(pv.x / dd, -pv.y / dd);
+    const int jlo = min(jn, max(0, c + 1 - j0)), wl = jn - jlo;
+    const double2 fc = f[c];
+    for (int jj = jlo + tid; jj < jn; jj += blockDim.x) {
+      const double2 ac = slab[(i64)c * cw + jj], ap = slab[(i64)p * cw + jj];
+      const double2 rc = cmul(ap, inv);
+      rowc[jj] = rc;
+      slab[(i64)c * cw + jj] = rc;
+      if (p != c) slab[(i64)p * cw + jj] = csub(ac, cmul(fc, rc));
+    }
+    __syncthreads();
+    for (int idx = tid; idx < n * wl; idx += blockDim.x) {
+      const int r = idx / wl, jj = jlo + (idx - r * wl);
+      if (r == c || r == p) continue;
+      double2 &x = slab[(i64)r * cw + jj];
+      x = csub(x, cmul(f[r], rowc[jj]));
+    }
+    __syncthreads();
+    if (c + 1 < n && c + 1 >= j0 && c + 1 < j0 + jn) publish(c + 1);
+    cl.sync();
+  }
+  for (i64 idx = tid; idx < (i64)n * jn; idx += blockDim.x) {
+    const int r = (int)(idx / jn), jj = (int)(idx - (i64)r * jn), j = j0 + jj;
+    if (j >= n) B[(i64)r * nrhs + (j - n)] = slab[(i64)r * cw + jj];
+  }
+}
+
+// Cluster size for gj_smem_kernel (0: the system does not fit in the shared memory of
+// 16 CTAs, or no such cluster can be resident).  A single system is spread until each CTA
+// holds at most 32 columns; a batch keeps one CTA per system where it fits.
+int gjs_cluster(int n, int nrhs, int nb, int &cw) {
+  static std::atomic<int> ok[64][5];  // per device and cluster size: 0 unknown, 1 yes, -1 no
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  if (dev >= 64) return 0;
+  const int W = n + nrhs;
+  for (int li = 0; li < 5; li++) {
+    const int CL = 1 << li;
+    cw = (W + CL - 1) / CL;
+    const i64 bytes = gjs_smem_bytes(n, cw);
+    if (bytes > GJS_SMEM_MAX) continue;
+    if (nb == 1 && cw > 32 && CL < 16) continue;
+    if (ok[dev][li].load() == 0) {
+      NEDY_CUDA(cudaFuncSetAttribute(gj_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GJS_SMEM_MAX));
+      NEDY_CUDA(cudaFuncSetAttribute(gj_smem_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = CL;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(CL);
+      cfg.blockDim = dim3(GJS_THREADS);
+      cfg.dynamicSmemBytes = GJS_SMEM_MAX;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      const cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, gj_smem_kernel, &cfg);
+      if (e != cudaSuccess) (void)cudaGetLastError();
+      ok[dev][li].store(e == cudaSuccess && nclusters > 0 ? 1 : -1);
+    }
+    if (ok[dev][li].load() > 0) return CL;
+  }
+  return 0;
+}
+
 void gj(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB) {
   int *st = c.ws.alloc<int>(nb);
   NEDY_CUDA(cudaMemsetAsync(st, 0, sizeof(int) * nb, c.stream));
-  if (nb == 1 && n >= 128) {
+  int cw = 0;
+  const int CL = gjs_cluster(n, nrhs, nb, cw);
+  if (CL > 0) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(nb * CL));
+    cfg.blockDim = dim3(GJS_THREADS);
+    cfg.dynamicSmemBytes = (size_t)gjs_smem_bytes(n, cw);
+    cfg.stream = c.stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    NEDY_CUDA(cudaLaunchKernelEx(&cfg, gj_smem_kernel, n, nrhs, (const double2 *)A, sA, B, sB, cw, st));
+    NEDY_CHECK_LAUNCH();
+  } else if (nb == 1 && n >= 128) {
     const int W = n + nrhs;
     const int cw = std::min(64, std::max(2, (W + 147) / 148));
     const int G = (W + cw - 1) / cw;

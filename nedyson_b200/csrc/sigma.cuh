@@ -39,5 +39,10 @@ void ensure_mixing_kernel(Ctx &c, const DevGF &G);
 void build_tau_kernel(Ctx &c, const double2 *Bn, int N, double sig, double2 *K);
 // Cached inverse of the time-local Dyson matrix for times [t0, t1] (after their rows are final)
 void update_minv(Ctx &c, const DevGF &Sig, const double2 *hmf, double mu, int t0, int t1);
+// X = A^-1 B for nb systems (A n x n at stride sA, B n x nrhs at stride sB, row-major) by
+// Gauss-Jordan with partial pivoting; B is overwritten.  A zero pivot is reported by
+// check_status, which also waits for the device.
+void gj_public(Ctx &c, int n, int nrhs, int nb, double2 *A, i64 sA, double2 *B, i64 sB);
+void check_status(Ctx &c);
 
 } // namespace nedy

@@ -354,12 +354,13 @@ __device__ __forceinline__ void store_fp64_16_staged(const Params &P, i64 roff, 
   __syncwarp();
 }
 
-// Epilogue of one 128 x BN output tile: this warp's 32 TMEM lanes of both parts (columns
-// [0, BN) real, [BN, 2 BN) imaginary from tmem) to the output View.  zero: the tile had no
-// K blocks (store zeros).  wbuf: this warp's staging buffer in shared memory.
+// Epilogue of one 128 x BN output tile: the 32 TMEM lanes of lane quarter `warp` (rows
+// m0 + 32 warp ...) of both parts (columns [0, BN) real, [BN, 2 BN) imaginary from tmem),
+// output columns [c_lo, c_hi) of the tile, to the output View.  zero: the tile had no K
+// blocks (store zeros).  wbuf: this warp's staging buffer in shared memory.
 template <int BN>
 __device__ __forceinline__ void epilogue_tile(const Params &P, int m0, int n0, int b, int warp, int lane,
-                                              uint32_t tmem, bool zero, uint8_t *wbuf) {
+                                              uint32_t tmem, bool zero, uint8_t *wbuf, int c_lo = 0, int c_hi = BN) {
     const int m = m0 + warp * 32 + lane;
     const bool mok = m < P.M;
     const i64 roff =
@@ -376,10 +377,10 @@ __device__ __forceinline__ void epilogue_tile(const Params &P, int m0, int n0, i
     __nv_bfloat16 *sbuf = (__nv_bfloat16 *)wbuf;
     const int imok = mok ? 1 : 0;
     {
-      for (int c0 = 0; c0 < BN;) {
+      for (int c0 = c_lo; c0 < c_hi;) {
         if (n0 + c0 >= P.N) break;  // uniform across the warp
         const int nf = n0 + c0;
-        if (P.out_pieces && !rows_contig && rows_al8 && c0 + 64 <= BN && nf + 64 <= P.N && P.cs_lo == 1 &&
+        if (P.out_pieces && !rows_contig && rows_al8 && c0 + 64 <= c_hi && nf + 64 <= P.N && P.cs_lo == 1 &&
             (P.cdiv == 0 || (nf % P.cdiv) + 64 <= P.cdiv)) {
           // 64 contiguous columns of each part, staged
           const i64 cbase = P.cdiv ? (i64)(nf / P.cdiv) * P.cs_hi + (i64)(nf % P.cdiv) : (i64)nf;
@@ -606,11 +607,18 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
 // Persistent variant of the one-load kernel: one CTA per SM walks a static list of tiles
 // (tile t, t + gridDim.x, ...), and TMEM holds two accumulators, so that the epilogue warps
 // store tile i while the MMA warp accumulates tile i+1 and the TMA warp loads ahead across
-// tile boundaries.  Barriers: full / empty per stage (TMA -> MMA -> TMA), tfull per
-// accumulator (MMA -> epilogue, tcgen05.commit), tempty per accumulator (the four epilogue
-// warps -> MMA).  Every wait is bounded; on give-up the roles stop, the TMA warp waits for
+// tile boundaries.  Eight epilogue warps, two per TMEM lane quarter (warps w and w + 4 read
+// the same 32 lanes and store half of the columns each): the epilogue is a long chain of
+// dependent conversions and stores, and a second warp per SM sub-partition hides its latency.
+// Warp 8 is the TMA producer, warp 9 the MMA issuer.  Barriers: full / empty per stage
+// (TMA -> MMA -> TMA), tfull per accumulator (MMA -> epilogue, tcgen05.commit), tempty per
+// accumulator (the eight epilogue warps -> MMA).  Every wait is bounded; on give-up the roles stop, the TMA warp waits for
 // the loads it issued and the MMA warp for the MMAs it issued before TMEM is released.
-constexpr int P_EPI_BYTES = 4 * STAGE_WARP_BYTES;  // epilogue staging, apart from the stages
+constexpr int P_EPI_WARPS = 8;                      // two per TMEM lane quarter, each half the columns
+constexpr int P_THREADS = 32 * (P_EPI_WARPS + 2);   // + TMA warp + MMA warp
+constexpr int P_EPI_BYTES = P_EPI_WARPS * STAGE_WARP_BYTES;  // epilogue staging, apart from the stages
+// stages + staging; the rest of the 232448-byte opt-in limit: alignment, barriers, static shared memory
+constexpr int P_SMEM_LIMIT = 232448 - 1024 - 256 - 128;
 constexpr int psmem_bytes(int stage_bytes, int stages) { return stages * stage_bytes + P_EPI_BYTES + 1024 + 256; }
 
 __device__ __forceinline__ void mbar_arrive(uint32_t a) {
@@ -618,7 +626,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t a) {
 }
 
 template <int BN, int STAGES, int BKT>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(P_THREADS, 1)
     split_gemm_persist_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                               const __grid_constant__ Params P, int ntn, int ntm, int ntiles) {
   static_assert(BN <= 128, "two accumulators of 2 BN TMEM columns must fit in 512 columns");
@@ -644,13 +652,13 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int i = 0; i < 2; i++) {
       mbar_init(tfull0 + 8 * i, 1);
-      mbar_init(tempty0 + 8 * i, 4);  // one arrival per epilogue warp
+      mbar_init(tempty0 + 8 * i, P_EPI_WARPS);  // one arrival per epilogue warp
     }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_skip = *(volatile int *)P.err != 0;
   }
-  if (warp == 5) {
+  if (warp == P_EPI_WARPS + 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(TALLOC));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -672,7 +680,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
   };
 
-  if (warp == 4 && lane == 0) {
+  if (warp == P_EPI_WARPS && lane == 0) {
     // ---- TMA producer
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
@@ -707,7 +715,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     // the loads of the last STAGES issued stages may still be in flight: wait for them
     for (int j = max(0, g - STAGES); j < g; j++)
       mbar_wait_drain(full0 + 8 * (j % STAGES), (uint32_t)(j / STAGES) & 1u, P.err, 4);
-  } else if (warp == 5 && lane == 0) {
+  } else if (warp == P_EPI_WARPS + 1 && lane == 0) {
     // ---- MMA issuer
     int g = 0, lt = 0;
     bool stop = false;
@@ -766,8 +774,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     // every MMA this thread issued has finished before TMEM is released
     mma_commit(done);
     mbar_wait_drain(done, 0, P.err, 3);
-  } else if (warp < 4) {
-    // ---- epilogue: tile lt from accumulator lt & 1, then hand the accumulator back
+  } else if (warp < P_EPI_WARPS) {
+    // ---- epilogue: tile lt from accumulator lt & 1, then hand the accumulator back; warp w
+    // reads lane quarter w & 3 and stores columns [(w >> 2) BN / 2, (w >> 2 + 1) BN / 2)
+    const int q = warp & 3, c_lo = (warp >> 2) * (BN / 2);
     int lt = 0;
     for (int t = first; t < ntiles; t += gridDim.x, lt++) {
       int n0, m0, b, kb0, nkb;
@@ -778,8 +788,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncwarp();
       if (!__shfl_sync(0xffffffffu, okl, 0)) break;
       tc_fence_after();
-      epilogue_tile<BN>(P, m0, n0, b, warp, lane, tmem + (uint32_t)bi * TCOLS, nkb == 0,
-                        epi + warp * STAGE_WARP_BYTES);
+      epilogue_tile<BN>(P, m0, n0, b, q, lane, tmem + (uint32_t)bi * TCOLS, nkb == 0, epi + warp * STAGE_WARP_BYTES,
+                        c_lo, c_lo + BN / 2);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(tempty0 + 8 * bi);
@@ -787,7 +797,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == P_EPI_WARPS + 1) {
     __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TALLOC));
@@ -962,19 +972,19 @@ void launch_persist(const Params &P, const CUtensorMap &ma, const CUtensorMap &m
   NEDY_CUDA(cudaGetDevice(&dev));
   NEDY_REQUIRE(dev < 64, "device index out of range");
   const int bytes = psmem_bytes(P.stage_bytes, STAGES);
-  NEDY_REQUIRE(STAGES * P.stage_bytes + P_EPI_BYTES <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  NEDY_REQUIRE(STAGES * P.stage_bytes + P_EPI_BYTES <= P_SMEM_LIMIT, "split_gemm: stages exceed shared memory");
   if (!attr[dev].load()) {
     int sms = 0;
     NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     sms_of[dev].store(sms);
     NEDY_CUDA(cudaFuncSetAttribute(split_gemm_persist_kernel<BN, STAGES, BKT>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_LIMIT + 1024 + 256));
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_LIMIT + 1024 + 256));
     attr[dev].store(true);
   }
   const long long ntiles = (long long)grid.x * grid.y * grid.z;
   NEDY_REQUIRE(ntiles < (1LL << 31), "split_gemm: too many tiles");
   const int nct = (int)std::min<long long>(ntiles, std::max(1, sms_of[dev].load()));
-  split_gemm_persist_kernel<BN, STAGES, BKT><<<nct, THREADS, bytes, s>>>(ma, mb, P, (int)grid.x, (int)grid.y,
+  split_gemm_persist_kernel<BN, STAGES, BKT><<<nct, P_THREADS, bytes, s>>>(ma, mb, P, (int)grid.x, (int)grid.y,
                                                                          (int)ntiles);
   NEDY_CHECK_LAUNCH();
 }
@@ -1052,7 +1062,7 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
       if (st >= 3) c.push_back({bn, std::min(st, 4), 1, bk});
       if (acc && bn == 256) c.push_back({bn, 2, 2, bk});
       if (bn == 128) {  // persistent: the epilogue of one tile beside the MMAs of the next
-        const int pst = std::min(bk == 32 ? 3 : 2, (SMEM_LIMIT - P_EPI_BYTES) / sb);
+        const int pst = std::min(bk == 32 ? 3 : 2, (P_SMEM_LIMIT - P_EPI_BYTES) / sb);
         if (pst >= 2) c.push_back({bn, pst, 1, bk, 1});
       }
     }
@@ -1292,7 +1302,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     }
   }
   const int stages = STsel ? STsel : BNsel == 128 ? 2 : std::min(4, SMEM_LIMIT / P.stage_bytes);
-  NEDY_REQUIRE(stages >= 2 && stages * P.stage_bytes + (PSsel ? P_EPI_BYTES : 0) <= SMEM_LIMIT,
+  NEDY_REQUIRE(stages >= 2 && (PSsel ? stages * P.stage_bytes + P_EPI_BYTES <= P_SMEM_LIMIT
+                                      : stages * P.stage_bytes <= SMEM_LIMIT),
                "split_gemm: stages exceed shared memory");
   cudaEvent_t tev[2] = {nullptr, nullptr};
   if (te) {

@@ -73,8 +73,8 @@ def test_step_entry_points_reject_null_handles(libpath):
 
 
 def test_new_entry_points_reject_bad_arguments(libpath):
-    """Full-U step, batch, Matsubara solver and the error hook check their arguments before
-    touching a device."""
+    """Full-U step, batch, Matsubara solver, dense solve and the error hook check their
+    arguments before touching a device."""
     import ctypes as C
     from nedyson_b200 import _lib
     L = _lib.lib()
@@ -90,3 +90,4 @@ def test_new_entry_points_reject_bad_arguments(libpath):
     arr = (C.c_void_p * 1)()
     assert L.nedy_matsubara_gf2(None, 1, arr, arr, arr, arr, arr, 1.0, 10, 1e-12, None, None) == 1
     assert L.nedy_ctx_inject_split_error(None, 2) == 1
+    assert L.nedy_dense_solve(None, 4, 1, 1, None, None) == 1
