@@ -22,7 +22,7 @@ __global__ void boot_tv0_kernel(int N, DevGF G, double *err) {
     const double2 v = make_double2(-G.sig * g.y, G.sig * g.x);
     double2 *dst = G.tvptr(0, m) + e;
     const double2 d = csub(*dst, v);
-    atomicAdd(&err[m], d.x * d.x + d.y * d.y);
+    add_warp(&err[m], d.x * d.x + d.y * d.y);
     *dst = v;
   }
 }
@@ -70,7 +70,7 @@ __global__ void diffnorm_blocks_kernel(int N, int nb, const double2 *A, const do
   const i64 es = (i64)N * N;
   GRID_STRIDE(i, es * nb) {
     const double2 d = csub(A[i], B[i]);
-    atomicAdd(&err[i / es], d.x * d.x + d.y * d.y);
+    add_warp(&err[i / es], d.x * d.x + d.y * d.y);
   }
 }
 
@@ -90,7 +90,7 @@ __global__ void boot_ret_kernel(int N, int k, DevGF G, double *err) {
     else v = csub(cscale(G.tvptr(n, G.ntau)[e], (double)G.sig), G.tvptr(n, 0)[e]);
     double2 *dst = G.retptr(n + l, l) + e;
     const double2 d = csub(v, *dst);
-    atomicAdd(&err[n * (k + 1) + l], d.x * d.x + d.y * d.y);
+    add_warp(&err[n * (k + 1) + l], d.x * d.x + d.y * d.y);
     *dst = v;
   }
 }
@@ -110,7 +110,7 @@ __global__ void boot_les_kernel(int N, int k, DevGF G, double *err) {
     const double2 v = make_double2(-t.x, t.y);
     double2 *dst = G.lesptr(n, l) + e;
     const double2 d = csub(*dst, v);
-    atomicAdd(&err[l * (k + 1) + n], d.x * d.x + d.y * d.y);
+    add_warp(&err[l * (k + 1) + n], d.x * d.x + d.y * d.y);
     *dst = v;
   }
 }

@@ -40,6 +40,25 @@ extern std::atomic<unsigned long long> g_launches;
     if (!(cond)) throw ::nedy::ArgError(std::string(msg));                                     \
   } while (0)
 
+#ifdef __CUDACC__
+// Adds v to *dst, one atomic per warp when all 32 lanes are active and target the same address
+// (the usual case of the per-block error norms, whose blocks are whole warps), one per lane
+// otherwise.  Same-address atomics from every thread serialise in L2.
+__device__ __forceinline__ void add_warp(double *dst, double v) {
+  const unsigned mask = __activemask();
+  if (mask == 0xffffffffu) {
+    const unsigned long long a = (unsigned long long)dst;
+    if (__all_sync(mask, a == __shfl_sync(mask, a, 0))) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(dst, v);
+      return;
+    }
+  }
+  atomicAdd(dst, v);
+}
+#endif
+
 // complex helpers on double2 (x = re, y = im)
 __host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

@@ -527,7 +527,7 @@ __global__ void ret_start_store(int N, int k, int T, DevGF G, const double2 *X, 
     double2 *dst = G.retptr(T, T - l - 1) + e;
     const double2 v = X[(i64)l * es + (i64)j * N + i];
     const double2 d = csub(*dst, v);
-    atomicAdd(&err[l], d.x * d.x + d.y * d.y);
+    add_warp(&err[l], d.x * d.x + d.y * d.y);
     *dst = v;
   }
 }
@@ -556,9 +556,235 @@ __global__ void ret_step_kernel(int N, int k, int T, int n, DevGF G, const doubl
     for (int c = 0; c < N; c++) acc = cadd(acc, cmul(row[c], Mi[(i64)c * N + j]));
     double2 *dst = G.retptr(T, T - n) + (i64)i * N + j;
     const double2 d = csub(*dst, acc);
-    atomicAdd(&err[n], d.x * d.x + d.y * d.y);
+    add_warp(&err[n], d.x * d.x + d.y * d.y);
     *dst = acc;
   }
+}
+
+// ---------------------------------------------------------------------------------
+// History pushes of the sequential sweeps: C_b += s_b A_b B_b for nb blocks of nao x nao
+// (nao <= 64), b = 0..nb-1, one CTA per (block, 32-column half).  Both operands are staged
+// whole by cp.async (A 64 x 64, B 64 x 32) and multiplied on the FP64 tensor path (DMMA
+// m8n8k4), eight warps of 16 x 16 outputs; no K loop, no atomics (every block has its own C).
+//   PUSH_RET (dyson_step.h:103-106): A = G^R(T, T-a), B_b = Sig^R(T-a, T-m0-b),
+//            C_b = Q_{m0+b}, s_b = gregT[a ld + m0 + b]
+//   PUSH_LES (dyson_step.h:266-269, the sum over l pushed from l = a): A_b = Sig^R(m0+b, a),
+//            B = X_a, C_b = Q_{m0+b}, s_b = dt greg[(m0+b) ld + a]
+enum PushMode { PUSH_RET = 0, PUSH_LES = 1 };
+constexpr int PB_LDA = 68, PB_LDB = 34;  // padded strides: conflict-free quarter-warp fragment reads
+constexpr int PB_SMEM = (64 * PB_LDA + 64 * PB_LDB) * 16;
+
+__device__ __forceinline__ void pb_cp16(void *dst, const void *src, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(src), "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void pb_dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// this warp's 16 x 16 outputs of the 64 x 32 half-tile: acc = As (64 x 64) * Bs (64 x 32)
+__device__ __forceinline__ void pb_product(const double2 *As, const double2 *Bs, int N, double (&cr)[2][2][2],
+                                           double (&ci)[2][2][2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 1) * 16, wn = (warp & 1) * 16;
+  const int kmax = (N + 3) >> 2;
+  for (int kk = 0; kk < kmax; kk++) {
+    const int k = kk * 4 + (lane & 3);
+    double ar[2], ai[2], br[2], bi[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const double2 v = As[(wm + i * 8 + (lane >> 2)) * PB_LDA + k];
+      ar[i] = v.x;
+      ai[i] = v.y;
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const double2 v = Bs[k * PB_LDB + wn + j * 8 + (lane >> 2)];
+      br[j] = v.x;
+      bi[j] = v.y;
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        pb_dmma(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+        pb_dmma(cr[i][j][0], cr[i][j][1], -ai[i], bi[j]);
+        pb_dmma(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+        pb_dmma(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+      }
+  }
+}
+
+// Stages the 64 x 64 block A and the 32 columns [n0, n0 + 32) of the block B (nao x nao,
+// row-major; zero outside) by cp.async; the caller waits.
+__device__ __forceinline__ void pb_stage(double2 *dst, int ld, const double2 *src, int N, int rows, int cols,
+                                         int c0) {
+  const int sh = cols == 64 ? 6 : 5;
+  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+    const int r = i >> sh, c = i & (cols - 1);
+    const bool v = r < N && c0 + c < N;
+    pb_cp16(dst + r * ld + c, v ? src + (i64)r * N + c0 + c : src, v);
+  }
+}
+
+__global__ void __launch_bounds__(256, 2)
+    push_blocks_kernel(int mode, int N, int T, int a, int m0, DevGF G, DevGF S, const double2 *X, double2 *Q,
+                       const double *w, i64 w_stride, double alpha) {
+  extern __shared__ double2 pbs[];
+  double2 *As = pbs, *Bs = pbs + 64 * PB_LDA;
+  const int b = blockIdx.x, n0 = blockIdx.y * 32;
+  const i64 es = (i64)N * N;
+  const double2 *A, *B;
+  if (mode == PUSH_RET) {
+    A = G.retptr(T, T - a);
+    B = S.retptr(T - a, T - m0 - b);
+  } else {
+    A = S.retptr(m0 + b, a);
+    B = X + (i64)a * es;
+  }
+  double2 *C = Q + (i64)(m0 + b) * es;
+  const double s = alpha * w[(i64)b * w_stride];
+  pb_stage(As, PB_LDA, A, N, 64, 64, 0);
+  pb_stage(Bs, PB_LDB, B, N, 64, 32, n0);
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  double cr[2][2][2] = {}, ci[2][2][2] = {};
+  pb_product(As, Bs, N, cr, ci);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 1) * 16, wn = (warp & 1) * 16;
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const int r = wm + i * 8 + (lane >> 2);
+    if (r >= N) continue;
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int col = n0 + wn + j * 8 + (lane & 3) * 2 + c;
+        if (col >= N) continue;
+        double2 &o = C[(i64)r * N + col];
+        o.x += s * cr[i][j][c];
+        o.y += s * ci[i][j][c];
+      }
+  }
+}
+
+// One step of a sequential sweep as a block product on the FP64 tensor path (nao <= 64), one
+// CTA per 32-column half:
+//   STEP_RET (dyson_step.h:88-106): G^R(T, T-a) = [dt Q_a + sum_l (-i bd_l/dt) G^R(T, T-a+l)] Minv(T-a),
+//            and err[a] += |change|^2
+//   STEP_LES (dyson_step.h:271-279): X_a = Minv(a) [Q_a + sum_l (-i bd_l/dt) X_{a-l}]
+enum StepMode { STEP_RET = 0, STEP_LES = 1 };
+__global__ void __launch_bounds__(256, 1)
+    step_block_kernel(int mode, int N, int k, int T, int a, DevGF G, const double2 *Q, double2 *X,
+                      const double2 *Minv, const double *bd, double dt, double *err) {
+  extern __shared__ double2 pbs[];
+  double2 *As = pbs, *Bs = pbs + 64 * PB_LDA;
+  const int n0 = blockIdx.y * 32;
+  const i64 es = (i64)N * N;
+  if (mode == STEP_RET) {
+    pb_stage(Bs, PB_LDB, Minv + (i64)(T - a) * es, N, 64, 32, n0);
+    asm volatile("cp.async.commit_group;\n" ::);
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+      const int r = i >> 6, c = i & 63;
+      double2 v = czero();
+      if (r < N && c < N) {
+        v = cscale(Q[(i64)a * es + (i64)r * N + c], dt);
+        for (int l = 1; l <= k + 1; l++) {
+          const double2 g = G.retptr(T, T - a + l)[(i64)r * N + c];
+          const double f = bd[l] / dt;
+          v.x += f * g.y;  // (-i) f g
+          v.y -= f * g.x;
+        }
+      }
+      As[r * PB_LDA + c] = v;
+    }
+  } else {
+    pb_stage(As, PB_LDA, Minv + (i64)a * es, N, 64, 64, 0);
+    asm volatile("cp.async.commit_group;\n" ::);
+    for (int i = threadIdx.x; i < 64 * 32; i += blockDim.x) {
+      const int r = i >> 5, c = i & 31;
+      double2 v = czero();
+      if (r < N && n0 + c < N) {
+        v = Q[(i64)a * es + (i64)r * N + n0 + c];
+        for (int l = 1; l <= k + 1; l++) {
+          const double2 x = X[(i64)(a - l) * es + (i64)r * N + n0 + c];
+          const double f = bd[l] / dt;
+          v.x += f * x.y;
+          v.y -= f * x.x;
+        }
+      }
+      Bs[r * PB_LDB + c] = v;
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  double cr[2][2][2] = {}, ci[2][2][2] = {};
+  pb_product(As, Bs, N, cr, ci);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp >> 1) * 16, wn = (warp & 1) * 16;
+  double2 *C = mode == STEP_RET ? G.retptr(T, T - a) : X + (i64)a * es;
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const int r = wm + i * 8 + (lane >> 2);
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int col = n0 + wn + j * 8 + (lane & 3) * 2 + c;
+        const bool ok = r < N && col < N;
+        double d2 = 0.0;
+        if (ok) {
+          double2 &o = C[(i64)r * N + col];
+          const double2 v = make_double2(cr[i][j][c], ci[i][j][c]);
+          const double2 d = csub(o, v);
+          d2 = d.x * d.x + d.y * d.y;
+          o = v;
+        }
+        if (mode == STEP_RET) add_warp(&err[a], d2);
+      }
+  }
+}
+
+// Launches push_blocks_kernel for nb blocks (nao <= 64); false when nao is larger.
+bool push_blocks(Ctx &c, int mode, int N, int T, int a, int m0, int nb, const DevGF &G, const DevGF &S,
+                 const double2 *X, double2 *Q, const double *w, i64 w_stride, double alpha) {
+  if (N > 64) return false;
+  if (nb <= 0) return true;
+  static std::atomic<bool> attr_set[64];  // per device (host threads may race here)
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  if (!attr_set[dev].load()) {
+    NEDY_CUDA(cudaFuncSetAttribute(push_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PB_SMEM));
+    attr_set[dev].store(true);
+  }
+  NEDY_REQUIRE(nb <= 2147483647 / 2, "push_blocks: too many blocks");
+  push_blocks_kernel<<<dim3((unsigned)nb, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(mode, N, T, a, m0, G, S, X, Q,
+                                                                                     w, w_stride, alpha);
+  NEDY_CHECK_LAUNCH();
+  return true;
+}
+
+// Launches step_block_kernel (nao <= 64); false when nao is larger.
+bool step_block(Ctx &c, int mode, int N, int k, int T, int a, const DevGF &G, const double2 *Q, double2 *X,
+                double *err) {
+  if (N > 64) return false;
+  static std::atomic<bool> attr_set[64];  // per device (host threads may race here)
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  if (!attr_set[dev].load()) {
+    NEDY_CUDA(cudaFuncSetAttribute(step_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PB_SMEM));
+    attr_set[dev].store(true);
+  }
+  step_block_kernel<<<dim3(1, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(mode, N, k, T, a, G, Q, X, c.Minv, c.d_bd,
+                                                                        c.dt, err);
+  NEDY_CHECK_LAUNCH();
+  return true;
 }
 
 // ---------------------------------------------------------------------------------
@@ -582,7 +808,7 @@ __global__ void diffnorm_kernel(int N, int nb, const double2 *A, const double2 *
   GRID_STRIDE(idx, es * nb) {
     const int b = (int)(idx / es);
     const double2 d = csub(A[idx], B[idx]);
-    atomicAdd(&err[b], d.x * d.x + d.y * d.y);
+    add_warp(&err[b], d.x * d.x + d.y * d.y);
   }
 }
 
@@ -597,7 +823,7 @@ __global__ void les_init_kernel(int N, int n, DevGF G, double2 *X0, double *err)
     const double2 v = make_double2(-t.x, t.y);
     double2 *dst = G.lesptr(0, n) + e;
     const double2 d = csub(*dst, v);
-    atomicAdd(err, d.x * d.x + d.y * d.y);
+    add_warp(err, d.x * d.x + d.y * d.y);
     *dst = v;
     X0[e] = v;
   }
@@ -1088,6 +1314,8 @@ static double dyson_ret(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *
   NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * (T + 1) * es, c.stream));
   // Q_n = sum_{l<=k} w(n,l) G^R(T,T-l) Sig^R(T-l,T-n),  n = k+1..T
   for (int l = 0; l <= k; l++) {
+    if (push_blocks(c, PUSH_RET, N, T, l, k + 1, T - k, G, S, nullptr, Q, c.gregT + (i64)l * ld + (k + 1), 1, 1.0))
+      continue;
     GemmArgs g;
     g.M = N; g.N = N; g.K = N; g.nb1 = T - k;
     g.A = rowmajor(G.retptr(T, T - l), N);
@@ -1099,9 +1327,13 @@ static double dyson_ret(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *
   }
   const int smem = N * sizeof(double2);
   for (int n = k + 1; n <= T; n++) {
-    ret_step_kernel<<<N, std::min(N, 256), smem, c.stream>>>(N, k, T, n, G, Q, c.Minv, c.d_bd, dt, err);
-    NEDY_CHECK_LAUNCH();
-    if (n < T) {  // push G^R(T,T-n) into Q_m, m = n+1..T
+    if (!step_block(c, STEP_RET, N, k, T, n, G, Q, nullptr, err)) {
+      ret_step_kernel<<<N, std::min(N, 256), smem, c.stream>>>(N, k, T, n, G, Q, c.Minv, c.d_bd, dt, err);
+      NEDY_CHECK_LAUNCH();
+    }
+    if (n < T &&
+        !push_blocks(c, PUSH_RET, N, T, n, n + 1, T - n, G, S, nullptr, Q, c.gregT + (i64)n * ld + (n + 1), 1, 1.0)) {
+      // push G^R(T,T-n) into Q_m, m = n+1..T
       GemmArgs g;
       g.M = N; g.N = N; g.K = N; g.nb1 = T - n;
       g.A = rowmajor(G.retptr(T, T - n), N);
@@ -1123,13 +1355,15 @@ static double dyson_tv(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *h
   NEDY_CUDA(cudaMemcpyAsync(old, G.tvptr(T, 0), sizeof(double2) * row, cudaMemcpyDeviceToDevice, c.stream));
   // mixing: int_0^beta Sig^tv(T,tau') G^M(tau' - tau_m)
   mixing_gemm(c, N, np, S.tvptr(T, 0), c.mixK, ctv, false, czero());
-  // CTV1: sum_{j<T} dt w(T,j) Sig^R(T,j) G^tv(j, .)   (the j = T term multiplies G^tv(T,.) = 0)
+  // CTV1: sum_{j<T} dt w(T,j) Sig^R(T,j) G^tv(j, .)   (the j = T term multiplies G^tv(T,.) = 0),
+  // computed transposed, ctv^T ((m,q) x i) = G^tv^T ((m,q) x (j,c)) Sig^R^T ((j,c) x i), so that
+  // the long dimension (np N) is the GEMM's M: 128-row tiles instead of 64-wide column tiles
   if (T > 0) {
     GemmArgs g;
-    g.M = N; g.N = (int)(np * N); g.K = T * N;
-    g.A.p = S.retptr(T, 0); g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1;
-    g.B.p = G.tvptr(0, 0); g.B.rdiv = N; g.B.rs_hi = row; g.B.rs_lo = N; g.B.cdiv = N; g.B.cs_hi = es; g.B.cs_lo = 1;
-    g.C.p = ctv; g.C.rs_lo = N; g.C.cdiv = N; g.C.cs_hi = es; g.C.cs_lo = 1;
+    g.M = (int)(np * N); g.N = N; g.K = T * N;
+    g.A.p = G.tvptr(0, 0); g.A.rdiv = N; g.A.rs_hi = es; g.A.rs_lo = 1; g.A.cdiv = N; g.A.cs_hi = row; g.A.cs_lo = N;
+    g.B.p = S.retptr(T, 0); g.B.rdiv = N; g.B.rs_hi = es; g.B.rs_lo = 1; g.B.cs_lo = N;
+    g.C.p = ctv; g.C.rdiv = N; g.C.rs_hi = es; g.C.rs_lo = 1; g.C.cs_lo = N;
     g.kscale = c.greg + (i64)T * ld; g.kdiv = N;
     g.alpha = make_double2(c.dt, 0.0);
     g.beta = make_double2(1.0, 0.0);
@@ -1237,30 +1471,41 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
     gj(c, kn, N, 1, M, 0, Qs, 0);
     NEDY_CUDA(cudaMemcpyAsync(X + es, Qs, sizeof(double2) * kn * N, cudaMemcpyDeviceToDevice, c.stream));
   }
-  // sequential m = k+1 .. n-1, then the diagonal
-  // blocks per split-K chunk of the pull sums: one block per CTA, so the sequential
-  // step m runs m CTAs (each 64x64x64 at nao=64) instead of m/8 long ones
-  const int LC = 1;
-  for (int m = k + 1; m <= n; m++) {
-    // Q_m += sum_{l<m} dt w(m,l) Sig^R(m,l) X_l   (split-K over l in chunks of LC blocks, atomics)
-    for (int part = 0; part < 2; part++) {
-      const int nfull = m / LC, rem = m - nfull * LC;
-      const int nb = part == 0 ? nfull : (rem > 0 ? 1 : 0);
-      if (nb == 0) continue;
-      const int l0 = part == 0 ? 0 : nfull * LC;
-      GemmArgs g;
-      g.M = N; g.N = N; g.K = (part == 0 ? LC : rem) * N; g.nb1 = nb;
-      g.A.p = S.retptr(m, l0); g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1; g.A.bs1 = LC * es;
-      g.B = rowmajor(X + (i64)l0 * es, N); g.B.bs1 = LC * es;
-      g.C = rowmajor(Q + (i64)m * es, N);
-      g.kscale = c.greg + (i64)m * ld + l0; g.kdiv = N; g.kscale_bs1 = LC;
-      g.alpha = make_double2(dt, 0.0);
-      g.atomic = true;
-      gemm(g, c.stream);
+  // sequential m = k+1 .. n-1, then the diagonal.  Q_m += sum_{l<m} dt w(m,l) Sig^R(m,l) X_l:
+  // for nao <= 64 each X_l is pushed into Q_{l+1..n} once it is known (the start block's
+  // X_0..X_k into Q_{k+1..n} first), one block product per target and no atomics
+  if (N <= 64) {
+    for (int l = 0; l <= k; l++)
+      push_blocks(c, PUSH_LES, N, 0, l, k + 1, n - k, G, S, X, Q, c.greg + (i64)(k + 1) * ld + l, ld, dt);
+    for (int m = k + 1; m < n; m++) {
+      step_block(c, STEP_LES, N, k, 0, m, G, Q, X, nullptr);
+      push_blocks(c, PUSH_LES, N, 0, m, m + 1, n - m, G, S, X, Q, c.greg + (i64)(m + 1) * ld + m, ld, dt);
     }
-    if (m < n) {
-      les_step_kernel<<<N, std::min(N, 256), N * sizeof(double2), c.stream>>>(N, k, m, Q, X, c.Minv, c.d_bd, dt);
-      NEDY_CHECK_LAUNCH();
+  } else {
+    // blocks per split-K chunk of the pull sums: one block per CTA, so the sequential
+    // step m runs m CTAs (each 64x64x64 at nao=64) instead of m/8 long ones
+    const int LC = 1;
+    for (int m = k + 1; m <= n; m++) {
+      // Q_m += sum_{l<m} dt w(m,l) Sig^R(m,l) X_l   (split-K over l in chunks of LC blocks, atomics)
+      for (int part = 0; part < 2; part++) {
+        const int nfull = m / LC, rem = m - nfull * LC;
+        const int nb = part == 0 ? nfull : (rem > 0 ? 1 : 0);
+        if (nb == 0) continue;
+        const int l0 = part == 0 ? 0 : nfull * LC;
+        GemmArgs g;
+        g.M = N; g.N = N; g.K = (part == 0 ? LC : rem) * N; g.nb1 = nb;
+        g.A.p = S.retptr(m, l0); g.A.rs_lo = N; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = 1; g.A.bs1 = LC * es;
+        g.B = rowmajor(X + (i64)l0 * es, N); g.B.bs1 = LC * es;
+        g.C = rowmajor(Q + (i64)m * es, N);
+        g.kscale = c.greg + (i64)m * ld + l0; g.kdiv = N; g.kscale_bs1 = LC;
+        g.alpha = make_double2(dt, 0.0);
+        g.atomic = true;
+        gemm(g, c.stream);
+      }
+      if (m < n) {
+        les_step_kernel<<<N, std::min(N, 256), N * sizeof(double2), c.stream>>>(N, k, m, Q, X, c.Minv, c.d_bd, dt);
+        NEDY_CHECK_LAUNCH();
+      }
     }
   }
   {

@@ -8,6 +8,7 @@
 // Row offsets of the A tile are computed once per CTA; the two-level index split of
 // the views costs one division per element per k-tile only for the split dimension.
 #include "gemm_f64.cuh"
+#include <cmath>
 
 namespace nedy {
 namespace {
@@ -324,11 +325,21 @@ void gemm(const GemmArgs &g, cudaStream_t stream) {
   P.ksplit = 1;
   P.kchunk = g.K;
   {
+    // resident CTAs: two per SM with 64-row tiles, one with 128-row tiles (148 SMs).  The split
+    // fills the device once (at least 256 of K per split); a somewhat larger one is taken when
+    // its last wave is clearly fuller (wave quantisation).
     const int bm = g.M >= 128 ? 128 : 64;
     const i64 ctas = (i64)cdiv(g.N, BN) * cdiv(g.M, bm) * g.nb1 * g.nb2;
-    const i64 target = 2 * 148;
-    if (!g.gK && ctas < target && g.K >= 1024) {
-      int ks = (int)std::min<i64>((target + ctas - 1) / ctas, g.K / 256);
+    const i64 slots = (bm == 128 ? 1 : 2) * 148;
+    if (!g.gK && ctas < slots && g.K >= 1024) {
+      const int kmax = (int)(g.K / 256);
+      auto eff = [&](int s) {
+        const double w = (double)(ctas * s) / (double)slots;
+        return w / std::ceil(w);
+      };
+      int ks = (int)std::min<i64>((slots + ctas - 1) / ctas, kmax);
+      for (int s2 = ks + 1, s_hi = std::min(kmax, 2 * ks + 8); s2 <= s_hi; s2++)
+        if (eff(s2) > eff(ks) + 0.03) ks = s2;
       if (ks > 1) {
         int kc = (g.K + ks - 1) / ks;
         kc = ((kc + BK - 1) / BK) * BK;

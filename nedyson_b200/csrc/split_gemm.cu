@@ -290,9 +290,13 @@ __device__ __forceinline__ void store_pieces16_rows(const Params &P, __nv_bfloat
 // helpers stage the warp's 32 rows in a warp-private shared buffer and write them back
 // so that each store instruction covers whole row segments (4 x 128 B of BF16 pieces,
 // or 2 x 256 B of FP64 complex).
-constexpr int STAGE_LD64 = 72;        // BF16 elements per staged row of 64 (padded, 144 B)
+// BF16 rows of 64 are staged unpadded (128 B) with the 16-byte chunks of row r at chunk
+// position j ^ (r & 7), so that both the row-wise writes and the column-wise reads of a warp
+// touch every bank once per 128 bytes.
+constexpr int STAGE_LD64 = 64;        // BF16 elements per staged row of 64 (swizzled, 128 B)
 constexpr int STAGE_LD16 = 17;        // double2 per staged row of 16 (padded, 272 B)
-constexpr int STAGE_WARP_BYTES = 32 * STAGE_LD16 * 16;  // >= 32 * STAGE_LD64 * 2
+constexpr int STAGE_WARP_BYTES = 32 * STAGE_LD16 * 16;   // FP64 outputs; >= PIECE_WARP_BYTES
+constexpr int PIECE_WARP_BYTES = 32 * STAGE_LD64 * 2;    // BF16 piece outputs only
 
 // BF16 pieces of 64 contiguous columns (x: this lane's row, scaled; consumed)
 __device__ __forceinline__ void store_pieces64_staged(const Params &P, __nv_bfloat16 *o, i64 roff, int mok,
@@ -309,16 +313,16 @@ __device__ __forceinline__ void store_pieces64_staged(const Params &P, __nv_bflo
         x[j + 2 * t + 1] -= f.y;
         w[t] = *(const uint32_t *)&h;
       }
-      *(uint4 *)(sbuf + lane * STAGE_LD64 + j) = make_uint4(w[0], w[1], w[2], w[3]);
+      *(uint4 *)(sbuf + lane * STAGE_LD64 + (((j >> 3) ^ (lane & 7)) << 3)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     __syncwarp();
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-      const int idx = i * 32 + lane, r = idx >> 3, c8 = (idx & 7) * 8;
+      const int idx = i * 32 + lane, r = idx >> 3, c8 = (idx & 7) * 8, sw = ((idx & 7) ^ (r & 7)) * 8;
       const i64 ro = __shfl_sync(0xffffffffu, roff, r);
       const int okr = __shfl_sync(0xffffffffu, mok, r);
       if (okr)
-        *(uint4 *)(o + (i64)p * P.plane + ro + cbase + c8) = *(const uint4 *)(sbuf + r * STAGE_LD64 + c8);
+        *(uint4 *)(o + (i64)p * P.plane + ro + cbase + c8) = *(const uint4 *)(sbuf + r * STAGE_LD64 + sw);
     }
     __syncwarp();
   }
@@ -616,7 +620,7 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
 // the loads it issued and the MMA warp for the MMAs it issued before TMEM is released.
 constexpr int P_EPI_WARPS = 8;                      // two per TMEM lane quarter, each half the columns
 constexpr int P_THREADS = 32 * (P_EPI_WARPS + 2);   // + TMA warp + MMA warp
-constexpr int P_EPI_BYTES = P_EPI_WARPS * STAGE_WARP_BYTES;  // epilogue staging, apart from the stages
+constexpr int P_EPI_BYTES = P_EPI_WARPS * PIECE_WARP_BYTES;  // epilogue staging (piece outputs), apart from the stages
 // stages + staging; the rest of the 232448-byte opt-in limit: alignment, barriers, static shared memory
 constexpr int P_SMEM_LIMIT = 232448 - 1024 - 256 - 128;
 constexpr int psmem_bytes(int stage_bytes, int stages) { return stages * stage_bytes + P_EPI_BYTES + 1024 + 256; }
@@ -788,7 +792,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       __syncwarp();
       if (!__shfl_sync(0xffffffffu, okl, 0)) break;
       tc_fence_after();
-      epilogue_tile<BN>(P, m0, n0, b, q, lane, tmem + (uint32_t)bi * TCOLS, nkb == 0, epi + warp * STAGE_WARP_BYTES,
+      epilogue_tile<BN>(P, m0, n0, b, q, lane, tmem + (uint32_t)bi * TCOLS, nkb == 0, epi + warp * PIECE_WARP_BYTES,
                         c_lo, c_lo + BN / 2);
       tc_fence_before();
       __syncwarp();
@@ -973,6 +977,7 @@ void launch_persist(const Params &P, const CUtensorMap &ma, const CUtensorMap &m
   NEDY_REQUIRE(dev < 64, "device index out of range");
   const int bytes = psmem_bytes(P.stage_bytes, STAGES);
   NEDY_REQUIRE(STAGES * P.stage_bytes + P_EPI_BYTES <= P_SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  NEDY_REQUIRE(P.out_pieces, "split_gemm: the persistent kernel writes BF16 piece outputs only");
   if (!attr[dev].load()) {
     int sms = 0;
     NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1027,7 +1032,7 @@ int stage_bytes_for(int nA, int nB, int np, int bn, int bk) {
   return bk == 0 ? nA * A_BYTES + nB * bn * BK * 2 : np * (nA * BM * bk * 2 + nB * bn * bk * 2);
 }
 
-std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
+std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc, bool pieces) {
   std::vector<Cand> c;
   if (N <= 64 && acc) {  // one output tile per batch: the K split is what there is to tune
     for (int kd : {1, 2, 4, 8}) c.push_back({64, 4, kd, 0});
@@ -1061,9 +1066,10 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc) {
       c.push_back({bn, 2, 1, bk});
       if (st >= 3) c.push_back({bn, std::min(st, 4), 1, bk});
       if (acc && bn == 256) c.push_back({bn, 2, 2, bk});
-      if (bn == 128) {  // persistent: the epilogue of one tile beside the MMAs of the next
-        const int pst = std::min(bk == 32 ? 3 : 2, (P_SMEM_LIMIT - P_EPI_BYTES) / sb);
+      if (bn == 128 && pieces) {  // persistent: the epilogue of one tile beside the MMAs of the next
+        const int pst = std::min(bk == 32 ? 4 : 2, (P_SMEM_LIMIT - P_EPI_BYTES) / sb);
         if (pst >= 2) c.push_back({bn, pst, 1, bk, 1});
+        if (pst >= 4) c.push_back({bn, 3, 1, bk, 1});
       }
     }
   }
@@ -1204,8 +1210,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 64 || g.force_stages == 4 || g.force_stages == 2,
                  "split_gemm: 64-wide tiles use 2 or 4 stages");
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
-    NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && g.force_bn == 128),
-                 "split_gemm: the persistent kernel is the one-load kernel with 128-wide tiles");
+    NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && g.force_bn == 128 && g.out_pieces),
+                 "split_gemm: the persistent kernel is the one-load kernel with 128-wide tiles and piece outputs");
     BNsel = g.force_bn;
     STsel = g.force_stages;
     KDsel = g.force_kdiv;
@@ -1218,7 +1224,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       auto it = g_tune.find(key);
       if (it == g_tune.end()) {
         TuneEntry e;
-        e.cands = candidates(P.nA, P.nB, P.np, g.N, g.accumulate && g.ksplit <= 0);
+        e.cands = candidates(P.nA, P.nB, P.np, g.N, g.accumulate && g.ksplit <= 0, g.out_pieces);
         e.best.assign(e.cands.size(), 1e30);
         e.trials.assign(e.cands.size(), 0);
         e.inflight.assign(e.cands.size(), 0);
@@ -1326,7 +1332,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       {32, 256, 3, launch<256, 3, 32, true>, 0}, {64, 128, 2, launch<128, 2, 64, true>, 0},
       {64, 128, 3, launch<128, 3, 64, true>, 0},
       {32, 128, 2, launch_persist<128, 2, 32>, 1}, {32, 128, 3, launch_persist<128, 3, 32>, 1},
-      {64, 128, 2, launch_persist<128, 2, 64>, 1}};
+      {32, 128, 4, launch_persist<128, 4, 32>, 1}, {64, 128, 2, launch_persist<128, 2, 64>, 1}};
   int st_run = stages;
   if (BKsel == 0) {  // per-product kernel: the instance nearest to the requested stages
     st_run = BNsel == 64 ? (stages <= 2 ? 2 : 4)

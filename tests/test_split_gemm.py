@@ -28,12 +28,12 @@ SHAPES = {
 }
 # (tile_n, stages, k_block, kdiv, persistent); k_block 0: per-product kernel, 32 / 64: one-load
 # kernel; persistent: the one-load kernel with one CTA per SM over a tile list and two TMEM
-# accumulators (the epilogue of one tile beside the MMAs of the next)
+# accumulators (the epilogue of one tile beside the MMAs of the next), BF16 piece outputs only
 INSTANCES = [(64, 4, 0, 1, 0), (64, 4, 0, 2, 0), (64, 4, 0, 4, 0), (64, 2, 0, 1, 0), (64, 2, 0, 2, 0), (128, 2, 0, 1, 0),
              (128, 3, 0, 1, 0), (128, 4, 0, 1, 0), (256, 2, 0, 1, 0), (256, 3, 0, 1, 0), (256, 2, 0, 2, 0),
              (128, 2, 32, 1, 0), (128, 3, 32, 1, 0), (128, 4, 32, 1, 0), (256, 2, 32, 1, 0), (256, 3, 32, 1, 0),
              (256, 2, 32, 2, 0), (128, 2, 64, 1, 0), (128, 3, 64, 1, 0),
-             (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1)]
+             (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 4, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1)]
 
 
 @pytest.mark.parametrize("np_", [2, 3])
@@ -55,7 +55,7 @@ def test_split_gemm_instances(shape, np_):
     assert len(ran) >= 3, ran
     if N > 64:
         assert any(bk for (_, _, bk, _, _) in ran), "no one-load instance ran"
-        if not (ac and bc and np_ == 3):  # complex x complex, three pieces: two stages do not fit with it
+        if op:  # the persistent kernel writes piece outputs
             assert any(ps for (*_, ps) in ran), "no persistent instance ran"
 
 
@@ -65,6 +65,9 @@ def test_split_gemm_check_rejects_missing_instance():
     assert rc == NEDY_ERR_ARG
     # the persistent kernel exists only as the one-load kernel with 128-wide tiles
     rc = _lib.lib().nedy_split_gemm_check(0, 128, 256, 64, 1, 1, 1, 0, 0, 2, 0, 0, 256, 2, 32, 1, 1, 1, C.byref(err))
+    assert rc == NEDY_ERR_ARG
+    # ... and writes BF16 piece outputs only (no FP64 output staging beside four stages)
+    rc = _lib.lib().nedy_split_gemm_check(0, 128, 256, 64, 1, 0, 1, 0, 0, 2, 0, 0, 128, 2, 32, 1, 1, 1, C.byref(err))
     assert rc == NEDY_ERR_ARG
 
 
