@@ -562,14 +562,16 @@ __global__ void ret_step_kernel(int N, int k, int T, int n, DevGF G, const doubl
 }
 
 // ---------------------------------------------------------------------------------
-// History pushes of the sequential sweeps: C_b += s_b A_b B_b for nb blocks of nao x nao
-// (nao <= 64), b = 0..nb-1, one CTA per (block, 32-column half).  Both operands are staged
-// whole by cp.async (A 64 x 64, B 64 x 32) and multiplied on the FP64 tensor path (DMMA
+// History pushes of the sequential sweeps: C_b += s_b A_b B_b + g_b Y for nb blocks of
+// nao x nao (nao <= 64), b = 0..nb-1, one CTA per (block, 32-column half).  Both operands are
+// staged whole by cp.async (A 64 x 64, B 64 x 32) and multiplied on the FP64 tensor path (DMMA
 // m8n8k4), eight warps of 16 x 16 outputs; no K loop, no atomics (every block has its own C).
-//   PUSH_RET (dyson_step.h:103-106): A = G^R(T, T-a), B_b = Sig^R(T-a, T-m0-b),
-//            C_b = Q_{m0+b}, s_b = gregT[a ld + m0 + b]
-//   PUSH_LES (dyson_step.h:266-269, the sum over l pushed from l = a): A_b = Sig^R(m0+b, a),
-//            B = X_a, C_b = Q_{m0+b}, s_b = dt greg[(m0+b) ld + a]
+// Y is the pushed block and g_b = -i bd(m - a) dscale the derivative weight of target
+// m = m0 + b when 1 <= m - a <= k + 1 and m <= m_dmax, so that the step itself needs only Q_m:
+//   PUSH_RET (dyson_step.h:89-92, 103-106): A = Y = G^R(T, T-a), B_b = Sig^R(T-a, T-m0-b),
+//            C_b = Q_{m0+b}, s_b = gregT[a ld + m0 + b], dscale = 1 / dt^2
+//   PUSH_LES (dyson_step.h:266-274, the sum over l pushed from l = a): A_b = Sig^R(m0+b, a),
+//            B = Y = X_a, C_b = Q_{m0+b}, s_b = dt greg[(m0+b) ld + a], dscale = 1 / dt
 enum PushMode { PUSH_RET = 0, PUSH_LES = 1 };
 constexpr int PB_LDA = 68, PB_LDB = 34;  // padded strides: conflict-free quarter-warp fragment reads
 constexpr int PB_SMEM = (64 * PB_LDA + 64 * PB_LDB) * 16;
@@ -631,7 +633,8 @@ __device__ __forceinline__ void pb_stage(double2 *dst, int ld, const double2 *sr
 
 __global__ void __launch_bounds__(256, 2)
     push_blocks_kernel(int mode, int N, int T, int a, int m0, DevGF G, DevGF S, const double2 *X, double2 *Q,
-                       const double *w, i64 w_stride, double alpha) {
+                       const double *w, i64 w_stride, double alpha, const double *bd, double dscale, int k,
+                       int m_dmax) {
   extern __shared__ double2 pbs[];
   double2 *As = pbs, *Bs = pbs + 64 * PB_LDA;
   const int b = blockIdx.x, n0 = blockIdx.y * 32;
@@ -646,6 +649,8 @@ __global__ void __launch_bounds__(256, 2)
   }
   double2 *C = Q + (i64)(m0 + b) * es;
   const double s = alpha * w[(i64)b * w_stride];
+  const int dl = m0 + b - a;
+  const double g = (dl >= 1 && dl <= k + 1 && m0 + b <= m_dmax) ? bd[dl] * dscale : 0.0;
   pb_stage(As, PB_LDA, A, N, 64, 64, 0);
   pb_stage(Bs, PB_LDB, B, N, 64, 32, n0);
   asm volatile("cp.async.commit_group;\n" ::);
@@ -665,68 +670,38 @@ __global__ void __launch_bounds__(256, 2)
       for (int c = 0; c < 2; c++) {
         const int col = n0 + wn + j * 8 + (lane & 3) * 2 + c;
         if (col >= N) continue;
+        const double2 y = mode == PUSH_RET ? As[r * PB_LDA + col] : Bs[r * PB_LDB + col - n0];
         double2 &o = C[(i64)r * N + col];
-        o.x += s * cr[i][j][c];
-        o.y += s * ci[i][j][c];
+        o.x += s * cr[i][j][c] + g * y.y;  // -i g y
+        o.y += s * ci[i][j][c] - g * y.x;
       }
   }
 }
 
 // One step of a sequential sweep as a block product on the FP64 tensor path (nao <= 64), one
-// CTA per 32-column half:
-//   STEP_RET (dyson_step.h:88-106): G^R(T, T-a) = [dt Q_a + sum_l (-i bd_l/dt) G^R(T, T-a+l)] Minv(T-a),
-//            and err[a] += |change|^2
-//   STEP_LES (dyson_step.h:271-279): X_a = Minv(a) [Q_a + sum_l (-i bd_l/dt) X_{a-l}]
+// CTA per 32-column half; the derivative terms are already in Q (pushed with the history):
+//   STEP_RET (dyson_step.h:88-101): G^R(T, T-a) = dt Q_a Minv(T-a), and err[a] += |change|^2
+//   STEP_LES (dyson_step.h:271-279): X_a = Minv(a) Q_a
 enum StepMode { STEP_RET = 0, STEP_LES = 1 };
 __global__ void __launch_bounds__(256, 1)
-    step_block_kernel(int mode, int N, int k, int T, int a, DevGF G, const double2 *Q, double2 *X,
-                      const double2 *Minv, const double *bd, double dt, double *err) {
+    step_block_kernel(int mode, int N, int T, int a, DevGF G, const double2 *Q, double2 *X, const double2 *Minv,
+                      double dt, double *err) {
   extern __shared__ double2 pbs[];
   double2 *As = pbs, *Bs = pbs + 64 * PB_LDA;
   const int n0 = blockIdx.y * 32;
   const i64 es = (i64)N * N;
-  if (mode == STEP_RET) {
-    pb_stage(Bs, PB_LDB, Minv + (i64)(T - a) * es, N, 64, 32, n0);
-    asm volatile("cp.async.commit_group;\n" ::);
-    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
-      const int r = i >> 6, c = i & 63;
-      double2 v = czero();
-      if (r < N && c < N) {
-        v = cscale(Q[(i64)a * es + (i64)r * N + c], dt);
-        for (int l = 1; l <= k + 1; l++) {
-          const double2 g = G.retptr(T, T - a + l)[(i64)r * N + c];
-          const double f = bd[l] / dt;
-          v.x += f * g.y;  // (-i) f g
-          v.y -= f * g.x;
-        }
-      }
-      As[r * PB_LDA + c] = v;
-    }
-  } else {
-    pb_stage(As, PB_LDA, Minv + (i64)a * es, N, 64, 64, 0);
-    asm volatile("cp.async.commit_group;\n" ::);
-    for (int i = threadIdx.x; i < 64 * 32; i += blockDim.x) {
-      const int r = i >> 5, c = i & 31;
-      double2 v = czero();
-      if (r < N && n0 + c < N) {
-        v = Q[(i64)a * es + (i64)r * N + n0 + c];
-        for (int l = 1; l <= k + 1; l++) {
-          const double2 x = X[(i64)(a - l) * es + (i64)r * N + n0 + c];
-          const double f = bd[l] / dt;
-          v.x += f * x.y;
-          v.y -= f * x.x;
-        }
-      }
-      Bs[r * PB_LDB + c] = v;
-    }
-  }
+  const bool ret = mode == STEP_RET;
+  pb_stage(As, PB_LDA, ret ? Q + (i64)a * es : Minv + (i64)a * es, N, 64, 64, 0);
+  pb_stage(Bs, PB_LDB, ret ? Minv + (i64)(T - a) * es : Q + (i64)a * es, N, 64, 32, n0);
+  asm volatile("cp.async.commit_group;\n" ::);
   asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
   double cr[2][2][2] = {}, ci[2][2][2] = {};
   pb_product(As, Bs, N, cr, ci);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = (warp >> 1) * 16, wn = (warp & 1) * 16;
-  double2 *C = mode == STEP_RET ? G.retptr(T, T - a) : X + (i64)a * es;
+  double2 *C = ret ? G.retptr(T, T - a) : X + (i64)a * es;
+  const double sc = ret ? dt : 1.0;
 #pragma unroll
   for (int i = 0; i < 2; i++) {
     const int r = wm + i * 8 + (lane >> 2);
@@ -739,19 +714,20 @@ __global__ void __launch_bounds__(256, 1)
         double d2 = 0.0;
         if (ok) {
           double2 &o = C[(i64)r * N + col];
-          const double2 v = make_double2(cr[i][j][c], ci[i][j][c]);
+          const double2 v = make_double2(sc * cr[i][j][c], sc * ci[i][j][c]);
           const double2 d = csub(o, v);
           d2 = d.x * d.x + d.y * d.y;
           o = v;
         }
-        if (mode == STEP_RET) add_warp(&err[a], d2);
+        if (ret) add_warp(&err[a], d2);
       }
   }
 }
 
 // Launches push_blocks_kernel for nb blocks (nao <= 64); false when nao is larger.
 bool push_blocks(Ctx &c, int mode, int N, int T, int a, int m0, int nb, const DevGF &G, const DevGF &S,
-                 const double2 *X, double2 *Q, const double *w, i64 w_stride, double alpha) {
+                 const double2 *X, double2 *Q, const double *w, i64 w_stride, double alpha, double dscale,
+                 int m_dmax) {
   if (N > 64) return false;
   if (nb <= 0) return true;
   static std::atomic<bool> attr_set[64];  // per device (host threads may race here)
@@ -763,15 +739,14 @@ bool push_blocks(Ctx &c, int mode, int N, int T, int a, int m0, int nb, const De
     attr_set[dev].store(true);
   }
   NEDY_REQUIRE(nb <= 2147483647 / 2, "push_blocks: too many blocks");
-  push_blocks_kernel<<<dim3((unsigned)nb, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(mode, N, T, a, m0, G, S, X, Q,
-                                                                                     w, w_stride, alpha);
+  push_blocks_kernel<<<dim3((unsigned)nb, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(
+      mode, N, T, a, m0, G, S, X, Q, w, w_stride, alpha, c.d_bd, dscale, c.k, m_dmax);
   NEDY_CHECK_LAUNCH();
   return true;
 }
 
 // Launches step_block_kernel (nao <= 64); false when nao is larger.
-bool step_block(Ctx &c, int mode, int N, int k, int T, int a, const DevGF &G, const double2 *Q, double2 *X,
-                double *err) {
+bool step_block(Ctx &c, int mode, int N, int T, int a, const DevGF &G, const double2 *Q, double2 *X, double *err) {
   if (N > 64) return false;
   static std::atomic<bool> attr_set[64];  // per device (host threads may race here)
   int dev = 0;
@@ -781,8 +756,8 @@ bool step_block(Ctx &c, int mode, int N, int k, int T, int a, const DevGF &G, co
     NEDY_CUDA(cudaFuncSetAttribute(step_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PB_SMEM));
     attr_set[dev].store(true);
   }
-  step_block_kernel<<<dim3(1, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(mode, N, k, T, a, G, Q, X, c.Minv, c.d_bd,
-                                                                        c.dt, err);
+  step_block_kernel<<<dim3(1, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(mode, N, T, a, G, Q, X, c.Minv, c.dt,
+                                                                        err);
   NEDY_CHECK_LAUNCH();
   return true;
 }
@@ -1312,10 +1287,16 @@ static double dyson_ret(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *
   if (T <= k) return sum_dev(c, err, T + 1, true);
   double2 *Q = c.ws.alloc<double2>((i64)(T + 1) * es);
   NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * (T + 1) * es, c.stream));
-  // Q_n = sum_{l<=k} w(n,l) G^R(T,T-l) Sig^R(T-l,T-n),  n = k+1..T
+  // Q_n = sum_{l<=k} w(n,l) G^R(T,T-l) Sig^R(T-l,T-n),  n = k+1..T.  For nao <= 64 the block
+  // kernels also push the derivative terms -i bd(n-l)/dt^2 G^R(T,T-l) into Q_n, and the step is
+  // the single product dt Q_n Minv(T-n).
+  const bool fused = N <= 64;
   for (int l = 0; l <= k; l++) {
-    if (push_blocks(c, PUSH_RET, N, T, l, k + 1, T - k, G, S, nullptr, Q, c.gregT + (i64)l * ld + (k + 1), 1, 1.0))
+    if (fused) {
+      push_blocks(c, PUSH_RET, N, T, l, k + 1, T - k, G, S, nullptr, Q, c.gregT + (i64)l * ld + (k + 1), 1, 1.0,
+                  1.0 / (dt * dt), T);
       continue;
+    }
     GemmArgs g;
     g.M = N; g.N = N; g.K = N; g.nb1 = T - k;
     g.A = rowmajor(G.retptr(T, T - l), N);
@@ -1327,13 +1308,16 @@ static double dyson_ret(Ctx &c, int T, DevGF &G, const DevGF &S, const double2 *
   }
   const int smem = N * sizeof(double2);
   for (int n = k + 1; n <= T; n++) {
-    if (!step_block(c, STEP_RET, N, k, T, n, G, Q, nullptr, err)) {
-      ret_step_kernel<<<N, std::min(N, 256), smem, c.stream>>>(N, k, T, n, G, Q, c.Minv, c.d_bd, dt, err);
-      NEDY_CHECK_LAUNCH();
+    if (fused) {
+      step_block(c, STEP_RET, N, T, n, G, Q, nullptr, err);
+      if (n < T)
+        push_blocks(c, PUSH_RET, N, T, n, n + 1, T - n, G, S, nullptr, Q, c.gregT + (i64)n * ld + (n + 1), 1, 1.0,
+                    1.0 / (dt * dt), T);
+      continue;
     }
-    if (n < T &&
-        !push_blocks(c, PUSH_RET, N, T, n, n + 1, T - n, G, S, nullptr, Q, c.gregT + (i64)n * ld + (n + 1), 1, 1.0)) {
-      // push G^R(T,T-n) into Q_m, m = n+1..T
+    ret_step_kernel<<<N, std::min(N, 256), smem, c.stream>>>(N, k, T, n, G, Q, c.Minv, c.d_bd, dt, err);
+    NEDY_CHECK_LAUNCH();
+    if (n < T) {  // push G^R(T,T-n) into Q_m, m = n+1..T
       GemmArgs g;
       g.M = N; g.N = N; g.K = N; g.nb1 = T - n;
       g.A = rowmajor(G.retptr(T, T - n), N);
@@ -1431,23 +1415,40 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
       Mv[p] = (p + 1) * N;
       Kv[p] = p * N;
     }
-    i64 *dOffA = c.ws.alloc<i64>(n + 1), *dOffB = c.ws.alloc<i64>(n + 1), *dOffC = c.ws.alloc<i64>(n + 1);
-    int *dM = c.ws.alloc<int>(n + 1), *dK = c.ws.alloc<int>(n + 1);
+    // part 1 in groups (p, chunk of at most PC blocks j): the groups' K no longer grows with p,
+    // so the longest CTA does PC blocks instead of n (the chunks of one p accumulate atomically)
+    constexpr int PC = 8;
+    std::vector<i64> cA, cB, cC;
+    std::vector<int> cK;
+    for (int p = 1; p <= n; p++)
+      for (int j0 = 0; j0 < p; j0 += PC) {
+        cA.push_back(offA[p] + (i64)j0 * es);
+        cB.push_back((i64)j0 * es);
+        cC.push_back((i64)p * es);
+        cK.push_back(std::min(PC, p - j0) * N);
+      }
+    const int ng = (int)cK.size();
+    i64 *dOffA = c.ws.alloc<i64>(n + 1), *dOffB = c.ws.alloc<i64>(n + 1);
+    int *dM = c.ws.alloc<int>(n + 1);
+    i64 *dcA = c.ws.alloc<i64>(ng), *dcB = c.ws.alloc<i64>(ng), *dcC = c.ws.alloc<i64>(ng);
+    int *dcK = c.ws.alloc<int>(ng);
     NEDY_CUDA(cudaMemcpyAsync(dOffA, offA.data(), sizeof(i64) * (n + 1), cudaMemcpyHostToDevice, c.stream));
     NEDY_CUDA(cudaMemcpyAsync(dOffB, offB.data(), sizeof(i64) * (n + 1), cudaMemcpyHostToDevice, c.stream));
-    NEDY_CUDA(cudaMemcpyAsync(dOffC, offC.data(), sizeof(i64) * (n + 1), cudaMemcpyHostToDevice, c.stream));
     NEDY_CUDA(cudaMemcpyAsync(dM, Mv.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream));
-    NEDY_CUDA(cudaMemcpyAsync(dK, Kv.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c.stream));
-    {  // part 1: Q_p -= sum_{j<p} Sig^<(j,p)^+ X_j     (group p: K = p N)
+    NEDY_CUDA(cudaMemcpyAsync(dcA, cA.data(), sizeof(i64) * ng, cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dcB, cB.data(), sizeof(i64) * ng, cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dcC, cC.data(), sizeof(i64) * ng, cudaMemcpyHostToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dcK, cK.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, c.stream));
+    if (ng > 0) {  // part 1: Q_p -= sum_{j<p} Sig^<(j,p)^+ X_j
       GemmArgs g;
-      g.M = N; g.N = N; g.K = n * N; g.nb1 = n + 1;
+      g.M = N; g.N = N; g.K = PC * N; g.nb1 = ng;
       g.A.p = S.les; g.A.rs_lo = 1; g.A.cdiv = N; g.A.cs_hi = es; g.A.cs_lo = N;
       g.conjA = true;
       g.B = rowmajor(Xc, N);
       g.C = rowmajor(Q, N);
-      g.goffA = dOffA; g.goffC = dOffC; g.gK = dK;
+      g.goffA = dcA; g.goffB = dcB; g.goffC = dcC; g.gK = dcK;
       g.alpha = make_double2(-1.0, 0.0);
-      g.beta = make_double2(1.0, 0.0);
+      g.atomic = true;
       gemm(g, c.stream);
     }
     {  // part 2: Q_p += sum_{j>=p} Sig^<(p,j) X_j        (group j: rows (p,a), p <= j)
@@ -1475,11 +1476,15 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
   // for nao <= 64 each X_l is pushed into Q_{l+1..n} once it is known (the start block's
   // X_0..X_k into Q_{k+1..n} first), one block product per target and no atomics
   if (N <= 64) {
+    // the derivative terms -i bd(m-l)/dt X_l go into Q_m with the pushes (targets m < n: the
+    // diagonal takes its own, dyson_step.h:303-306), and the step is the product Minv(m) Q_m
     for (int l = 0; l <= k; l++)
-      push_blocks(c, PUSH_LES, N, 0, l, k + 1, n - k, G, S, X, Q, c.greg + (i64)(k + 1) * ld + l, ld, dt);
+      push_blocks(c, PUSH_LES, N, 0, l, k + 1, n - k, G, S, X, Q, c.greg + (i64)(k + 1) * ld + l, ld, dt, 1.0 / dt,
+                  n - 1);
     for (int m = k + 1; m < n; m++) {
-      step_block(c, STEP_LES, N, k, 0, m, G, Q, X, nullptr);
-      push_blocks(c, PUSH_LES, N, 0, m, m + 1, n - m, G, S, X, Q, c.greg + (i64)(m + 1) * ld + m, ld, dt);
+      step_block(c, STEP_LES, N, 0, m, G, Q, X, nullptr);
+      push_blocks(c, PUSH_LES, N, 0, m, m + 1, n - m, G, S, X, Q, c.greg + (i64)(m + 1) * ld + m, ld, dt, 1.0 / dt,
+                  n - 1);
     }
   } else {
     // blocks per split-K chunk of the pull sums: one block per CTA, so the sequential
