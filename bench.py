@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--t0", type=int, default=100)
     ap.add_argument("--corr", type=int, default=5)
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--tight-tol", type=float, default=1e-10,
+                    help="tolerance of the predictor ablation forms (0: skip them)")
     ap.add_argument("--state", default="trajectory", choices=["trajectory", "synthetic"])
     ap.add_argument("--restricted", action="store_true",
                     help="restricted simulation instead of the spin-unrestricted one")
@@ -494,8 +496,14 @@ def run_engine(args, dist: Dist):
             if berr < 1e-12:
                 break
         ctx.set_precision(PREC_SPLIT_BF16X3)  # the same state for either split mode
+        # the learned predictor is trained on this trajectory's own converged rows (the steps
+        # before the window; the window itself is held out)
+        hist_pred = api.Predictor(ctx, 1 << 22, seed=5) if args.predictor == "learned" else None
         for t in range(kk + 1, t_first):
             step_tol(t, 1e-10)
+            if hist_pred is not None and t >= 9:
+                for s in range(ns):
+                    hist_pred.collect(G[s], t, 64)
         ctx.synchronize()
         prep = {"equilibrium": eq_info or "Hartree-Fock", "boot_iterations": it + 1, "boot_err": berr,
                 "steps": t_first - kk - 1, "seconds": time.time() - tp}
@@ -515,7 +523,15 @@ def run_engine(args, dist: Dist):
             hmf.append(api.hmf_buffer(ctx, N, hm))
     # learned predictor: trained on small trajectories the engine generates (outside the timing)
     pred, pred_info = None, None
-    if args.predictor == "learned":
+    if args.predictor == "learned" and traj:
+        tt = time.time()
+        nsamp = hist_pred.samples()
+        loss = hist_pred.train(3000, 2048, 1e-3)
+        pred = hist_pred
+        pred_info = {"data": f"rows T=9..{t_first - 1} of this trajectory (both spins, every 64th element), "
+                             f"the window T>={t_first} held out", "samples": nsamp, "final_loss": loss,
+                     "seconds": time.time() - tt}
+    elif args.predictor == "learned":
         pred, pred_info = train_predictor(ctx, args)
     sp = C.c_void_p()
     check(lib().nedy_ctx_stream(ctx.h, C.byref(sp)))
@@ -589,6 +605,18 @@ def run_engine(args, dist: Dist):
         set_form(PREC_SPLIT, False)
         forms["split_poly_exit"] = timed(split_step, T_timed, True, clocks_on=False)
         rows["split_poly_exit"], ens["split_poly_exit"] = window_rows(T_timed[:Kc]), energies(T_timed[:Kc])
+        if pred is not None and args.tight_tol > 0:
+            # predictor ablation at a tolerance where the prediction error decides the
+            # iteration count: learned and polynomial prediction, same steps, same exit
+            Tt = T_timed[:max(Kc, min(K, 10))]
+            tight_step = lambda t: step_tol(t, args.tight_tol)  # noqa: E731
+            for name, learned in (("split_learned_exit_tight", True), ("split_poly_exit_tight", False)):
+                set_form(PREC_SPLIT, learned)
+                forms[name] = timed(tight_step, Tt, True, clocks_on=False)
+                forms[name]["tol"] = args.tight_tol
+                if learned:
+                    forms[name]["predictor_stats"] = ctx.predictor_stats()
+                rows[name], ens[name] = window_rows(T_timed[:Kc]), energies(T_timed[:Kc])
         # 3. plain FP64 + residual exit (the exit alone, same arithmetic as the reference)
         set_form(PREC_FP64, False)
         forms["plain_fp64_exit"] = timed(exit_plain, T_timed[:Kc], False, clocks_on=False)
@@ -900,6 +928,9 @@ def main():
                  "timesteps_s_first_steps": Kc / sum(f["per_step_s"][:Kc])}
             if name in r["errs"]:
                 o["error_vs_plain_fp64"] = r["errs"][name]
+            for key in ("tol", "predictor_stats"):
+                if key in f:
+                    o[key] = f[key]
             return o
 
         forms = {name: form_obj(f, name) for name, f in fm.items()}
