@@ -17,6 +17,8 @@
 // a^2/(b s6)] -> 256 tanh -> 256 tanh -> 2, BF16 operands with FP32 accumulation in the
 // forward and the backward pass, FP32 master weights updated by Adam.  Training data are
 // the rows the engine itself converged (collect); training runs on the GPU in these kernels.
+// Inference corrects the elements whose sixth-difference scale is within a factor
+// PRED_SELECT of the row's largest (the others keep the polynomial prediction).
 #include "predictor.cuh"
 #include <random>
 
@@ -151,8 +153,10 @@ __global__ void w2t_kernel(const float *W2, __nv_bfloat16 *w2t) {
   }
 }
 
-__global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, i64 total, const double *exw, const float *W,
+__global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, const i64 *sel,
+                                                    const unsigned long long *nsel, const double *exw, const float *W,
                                                     const __nv_bfloat16 *w2t_g, double2 *corr_out) {
+  const i64 total = (i64)nsel[1];
   extern __shared__ __align__(16) unsigned char smem[];
   __nv_bfloat16 *w2t = (__nv_bfloat16 *)smem;  // [256 in][256 out]
   __nv_bfloat16 *h1 = w2t + PRED_W * PRED_W;    // [64][256]
@@ -176,12 +180,12 @@ __global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, i64 total, c
   for (i64 base = (i64)blockIdx.x * INF_E; base < total; base += (i64)gridDim.x * INF_E) {
     __syncthreads();
     if (threadIdx.x < INF_E) {
-      const i64 idx = base + threadIdx.x;
+      const i64 idx = base + threadIdx.x < total ? sel[base + threadIdx.x] : -1;
       float x[PRED_IN] = {};
       double s6 = 0.0;
       Series s;
       double2 p;
-      if (!(idx < total && series_of(G, T, idx, s) && features(s, exw, x, p, s6))) s6 = 0.0;
+      if (!(idx >= 0 && series_of(G, T, idx, s) && features(s, exw, x, p, s6))) s6 = 0.0;
       for (int i = 0; i < PRED_IN; i++) xs[threadIdx.x * PRED_IN + i] = bfr(x[i]);
       sc[threadIdx.x] = s6;
       ys[threadIdx.x * 2] = 0.f;
@@ -239,8 +243,8 @@ __global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, i64 total, c
     }
     __syncthreads();
     if (threadIdx.x < INF_E) {
-      const i64 idx = base + threadIdx.x;
-      if (idx < total) {
+      const i64 idx = base + threadIdx.x < total ? sel[base + threadIdx.x] : -1;
+      if (idx >= 0) {
         const double s6 = sc[threadIdx.x];
         double2 cr = make_double2(0, 0);
         if (s6 > 0.0) {
@@ -255,6 +259,39 @@ __global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, i64 total, c
         }
         if (corr_out) corr_out[idx] = cr;
       }
+    }
+  }
+}
+
+// Selection of the elements the network corrects: the scale s6 of every element of row T
+// (0 where no correction applies) and the row maximum; then the elements with
+// s6 >= max / PRED_SELECT go into a list and every other element's correction is zero.
+// An element left out keeps the polynomial prediction, whose error there is of order s6,
+// i.e. far below the row's largest error, which is what the corrector's residual sees.
+constexpr double PRED_SELECT = 32.0;
+__global__ void s6_kernel(DevGF G, int T, i64 total, const double *exw, double *s6buf, unsigned long long *mx) {
+  double m = 0.0;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < total; idx += (i64)gridDim.x * blockDim.x) {
+    Series s;
+    float x[PRED_IN];
+    double2 p;
+    double s6 = 0.0;
+    if (!(series_of(G, T, idx, s) && features(s, exw, x, p, s6))) s6 = 0.0;
+    s6buf[idx] = s6;
+    m = fmax(m, s6);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(mx, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void select_kernel(i64 total, const double *s6buf, unsigned long long *w, i64 *sel, double2 *corr_out) {
+  const double lim = __longlong_as_double((long long)w[0]) / PRED_SELECT;
+  for (i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x; idx < total; idx += (i64)gridDim.x * blockDim.x) {
+    const double s6 = s6buf[idx];
+    if (s6 > 0.0 && s6 >= lim) {
+      sel[atomicAdd(w + 1, 1ULL)] = idx;
+    } else if (corr_out) {
+      corr_out[idx] = make_double2(0.0, 0.0);
     }
   }
 }
@@ -412,6 +449,9 @@ Predictor::Predictor(Ctx &c, i64 capacity, unsigned long long seed_) : ctx(c), c
 
 Predictor::~Predictor() {
   if (w2t) cudaFree(w2t);
+  if (s6buf) cudaFree(s6buf);
+  if (sel) cudaFree(sel);
+  if (selw) cudaFree(selw);
   cudaFree(W);
   cudaFree(X);
   cudaFree(count);
@@ -561,10 +601,30 @@ void Predictor::apply(const DevGF &g, int T, double2 *corr_out) {
     attr[ctx.device].store(true);
   }
   if (!w2t) NEDY_CUDA(cudaMalloc(&w2t, sizeof(__nv_bfloat16) * PRED_W * PRED_W));
+  if (!selw) NEDY_CUDA(cudaMalloc(&selw, 2 * sizeof(unsigned long long)));
+  if (sel_cap < tot) {  // grown geometrically, so that a run reallocates a few times at most
+    const i64 cap2 = std::max<i64>(tot, sel_cap + sel_cap / 2);
+    NEDY_CUDA(cudaStreamSynchronize(ctx.stream));
+    cudaFree(s6buf);
+    cudaFree(sel);
+    s6buf = nullptr;
+    sel = nullptr;
+    sel_cap = 0;
+    NEDY_CUDA(cudaMalloc(&s6buf, sizeof(double) * cap2));
+    NEDY_CUDA(cudaMalloc(&sel, sizeof(i64) * cap2));
+    sel_cap = cap2;
+  }
   w2t_kernel<<<64, TPB, 0, ctx.stream>>>(W + OW2, w2t);
   NEDY_CHECK_LAUNCH();
+  NEDY_CUDA(cudaMemsetAsync(selw, 0, 2 * sizeof(unsigned long long), ctx.stream));
+  const unsigned gb = (unsigned)std::min<i64>((tot + TPB - 1) / TPB, 148LL * 8);
+  s6_kernel<<<gb, TPB, 0, ctx.stream>>>(g, T, tot, ctx.d_ex, s6buf, selw);
+  NEDY_CHECK_LAUNCH();
+  select_kernel<<<gb, TPB, 0, ctx.stream>>>(tot, s6buf, selw, sel, corr_out);
+  NEDY_CHECK_LAUNCH();
+  // the selected count is read by the kernel; the grid covers every element in the worst case
   const unsigned blocks = (unsigned)std::min<i64>((tot + INF_E - 1) / INF_E, 148LL);
-  infer_kernel<<<blocks, TPB, smem, ctx.stream>>>(g, T, tot, ctx.d_ex, W, w2t, corr_out);
+  infer_kernel<<<blocks, TPB, smem, ctx.stream>>>(g, T, sel, selw, ctx.d_ex, W, w2t, corr_out);
   NEDY_CHECK_LAUNCH();
 }
 

@@ -48,6 +48,11 @@ class Predictor {
   unsigned long long ncollect = 0;
   long long adam_t = 0;
   __nv_bfloat16 *w2t = nullptr;
+  // selection of the elements the network corrects (grown once for the longest row)
+  double *s6buf = nullptr;
+  i64 *sel = nullptr;
+  unsigned long long *selw = nullptr;  // [0] row max of s6 (as bits), [1] selected count
+  i64 sel_cap = 0;
 };
 
 }  // namespace nedy
