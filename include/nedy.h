@@ -258,6 +258,9 @@ int nedy_predictor_params(nedy_predictor *p, float *host, int get);
 /* forward pass on n host feature rows (n x 12) -> y (n x 2); loss 0.5 sum|y-t|^2 / n and
  * its gradient (nparams floats) on host rows, for checks against a CPU restatement */
 int nedy_predictor_forward(nedy_predictor *p, const float *x, int n, float *y);
+/* the same network through the inference kernel the steps use (tcgen05 tensor cores,
+ * 128 rows per CTA, W1/W2 resident in shared memory), on n host rows -> y (n x 2) */
+int nedy_predictor_infer(nedy_predictor *p, const float *x, int n, float *y);
 int nedy_predictor_loss_grad(nedy_predictor *p, const float *x, const float *t, int n, double *loss, float *grad);
 /* the prediction of row tstp alone: dyson::Extrapolate, plus the learned correction of
  * the context's predictor when learned != 0 */

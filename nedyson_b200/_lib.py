@@ -85,6 +85,7 @@ SIGNATURES = {
     "nedy_predictor_nparams": ([], _LL),
     "nedy_predictor_params": ([_P, _P, _I], _I),
     "nedy_predictor_forward": ([_P, _P, _I, _P], _I),
+    "nedy_predictor_infer": ([_P, _P, _I, _P], _I),
     "nedy_predictor_loss_grad": ([_P, _P, _P, _I, _DP, _P], _I),
     "nedy_predict": ([_P, _I, _P, _I], _I),
     "nedy_ctx_set_predictor": ([_P, _P], _I),

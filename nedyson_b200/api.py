@@ -309,6 +309,13 @@ class Predictor:
         assert w.size == self.nparams
         check(lib().nedy_predictor_params(self.h, _ptr(w), 0))
 
+    def infer(self, x: np.ndarray) -> np.ndarray:
+        """The network through the tensor-core inference kernel (what the steps run)."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty((x.shape[0], 2), np.float32)
+        check(lib().nedy_predictor_infer(self.h, _ptr(x), x.shape[0], _ptr(y)))
+        return y
+
     def forward(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float32)
         y = np.empty((x.shape[0], 2), np.float32)

@@ -1043,6 +1043,30 @@ int nedy_predictor_params(nedy_predictor *p, float *host, int get) {
   });
 }
 
+int nedy_predictor_infer(nedy_predictor *p, const float *x, int n, float *y) {
+  return guard([&] {
+    NEDY_REQUIRE(p && x && y && n > 0, "bad argument");
+    set_dev(p->ctx);
+    Ctx &c = p->ctx->c;
+    float *d = nullptr;
+    NEDY_CUDA(cudaMalloc(&d, sizeof(float) * (size_t)n * (PRED_IN + 2)));
+    float *yd = d + (i64)n * PRED_IN;
+    cudaError_t e = cudaMemcpyAsync(d, x, sizeof(float) * n * PRED_IN, cudaMemcpyHostToDevice, c.stream);
+    if (e == cudaSuccess) {
+      try {
+        p->p->infer(n, d, yd);
+      } catch (...) {
+        cudaFree(d);
+        throw;
+      }
+      e = cudaMemcpyAsync(y, yd, sizeof(float) * n * 2, cudaMemcpyDeviceToHost, c.stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    cudaFree(d);
+    NEDY_CUDA(e);
+  });
+}
+
 int nedy_predictor_forward(nedy_predictor *p, const float *x, int n, float *y) {
   return guard([&] {
     NEDY_REQUIRE(p && x && y && n > 0, "bad argument");

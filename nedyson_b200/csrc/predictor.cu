@@ -20,6 +20,7 @@
 // Inference corrects the elements whose sixth-difference scale is within a factor
 // PRED_SELECT of the row's largest (the others keep the polynomial prediction).
 #include "predictor.cuh"
+#include "tcgen05.cuh"
 #include <random>
 
 namespace nedy {
@@ -141,118 +142,168 @@ __global__ void collect_kernel(DevGF G, int T, i64 total, const double *exw, int
   }
 }
 
-// Learned correction of the new row (after the polynomial extrapolation wrote p into it).
-// One CTA: 64 elements per pass; W2 (BF16, transposed: [in][out]) and h1 (BF16) in
-// shared memory.  Layer 2 is register-blocked: thread t owns units 4*(t%64)..+3 for
-// elements 16*(t/64)..+15.
-constexpr int INF_E = 64;
-__global__ void w2t_kernel(const float *W2, __nv_bfloat16 *w2t) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < PRED_W * PRED_W; i += gridDim.x * blockDim.x) {
-    const int k = i / PRED_W, u = i - k * PRED_W;
-    w2t[i] = __float2bfloat16_rn(W2[u * PRED_W + k]);
-  }
-}
+// Learned correction of the new row (after the polynomial extrapolation wrote p into it),
+// on the 5th-generation tensor cores: one CTA of 128 threads per 128-element tile, thread t
+// owns element t (TMEM lane t).  Layer 1 (K = 16: the 12 inputs, zero-padded) and layer 2
+// (K = 256) are tcgen05.mma M128 N256 with BF16 operands K-major in shared memory (64-wide
+// K blocks, 128-byte swizzle) and the FP32 accumulator in TMEM (256 columns, reused by
+// both layers); W1 and W2 (BF16) stay in shared memory for all tiles of the CTA, h1 is
+// written back into the A tile by the layer-1 epilogue.  The output layer (2 x 256) runs in
+// registers in the layer-2 epilogue.  Operand rounding is that of the training forward
+// (BF16 inputs, weights and hidden activations, FP32 accumulation).
+// xin != nullptr: the network on given inputs (n rows of PRED_IN), raw outputs (with b3)
+// to yout; else the elements sel[0 .. nsel[1]) of row T of G.
+constexpr int MLP_T = 128;
+constexpr int MLP_W2 = 4 * PRED_W * 128;     // 4 K blocks x 256 rows x 128 B
+constexpr int MLP_W1 = PRED_W * 128;         // 1 K block x 256 rows
+constexpr int MLP_H = 4 * MLP_T * 128;       // 4 K blocks x 128 rows (X in block 0 first)
+constexpr int MLP_SMEM = MLP_W2 + MLP_W1 + MLP_H + 64 + 1024;
 
-__global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, const i64 *sel,
-                                                    const unsigned long long *nsel, const double *exw, const float *W,
-                                                    const __nv_bfloat16 *w2t_g, double2 *corr_out) {
-  const i64 total = (i64)nsel[1];
-  extern __shared__ __align__(16) unsigned char smem[];
-  __nv_bfloat16 *w2t = (__nv_bfloat16 *)smem;  // [256 in][256 out]
-  __nv_bfloat16 *h1 = w2t + PRED_W * PRED_W;    // [64][256]
-  float *xs = (float *)(h1 + INF_E * PRED_W);   // [64][PRED_IN]
-  float *ys = xs + INF_E * PRED_IN;             // [64][2]
-  double *sc = (double *)(ys + INF_E * 2);      // [64] s6 (0: no correction)
+__global__ void __launch_bounds__(MLP_T, 1)
+    mlp_tc_kernel(DevGF G, int T, const i64 *sel, const unsigned long long *nsel, const double *exw, const float *W,
+                  double2 *corr_out, const float *xin, int nin, float *yout, int *err) {
+  using namespace tc;
+  extern __shared__ uint8_t mraw[];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)mraw + 1023) & ~(uintptr_t)1023);
+  uint8_t *w2s = sm, *w1s = sm + MLP_W2, *hs = w1s + MLP_W1;
+  uint64_t *bar = (uint64_t *)(hs + MLP_H);
+  uint32_t *tslot = (uint32_t *)(bar + 1);
   const float *W1 = W, *b1 = W1 + PRED_W * PRED_IN, *W2 = b1 + PRED_W, *b2 = W2 + PRED_W * PRED_W;
   const float *W3 = b2 + PRED_W, *b3 = W3 + 2 * PRED_W;
-  {
-    const uint4 *src = (const uint4 *)w2t_g;
-    uint4 *dst = (uint4 *)w2t;
-    for (int i = threadIdx.x; i < PRED_W * PRED_W * 2 / 16; i += TPB) dst[i] = src[i];
-  }
-  const int ug = threadIdx.x & 63, eg = threadIdx.x >> 6;  // 4 units, 16 elements
-  float b2r[4], w3r[2][4];
-  for (int j = 0; j < 4; j++) {
-    b2r[j] = b2[ug * 4 + j];
-    w3r[0][j] = bfr(W3[ug * 4 + j]);
-    w3r[1][j] = bfr(W3[PRED_W + ug * 4 + j]);
-  }
-  for (i64 base = (i64)blockIdx.x * INF_E; base < total; base += (i64)gridDim.x * INF_E) {
-    __syncthreads();
-    if (threadIdx.x < INF_E) {
-      const i64 idx = base + threadIdx.x < total ? sel[base + threadIdx.x] : -1;
-      float x[PRED_IN] = {};
-      double s6 = 0.0;
-      Series s;
-      double2 p;
-      if (!(idx >= 0 && series_of(G, T, idx, s) && features(s, exw, x, p, s6))) s6 = 0.0;
-      for (int i = 0; i < PRED_IN; i++) xs[threadIdx.x * PRED_IN + i] = bfr(x[i]);
-      sc[threadIdx.x] = s6;
-      ys[threadIdx.x * 2] = 0.f;
-      ys[threadIdx.x * 2 + 1] = 0.f;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const i64 total = xin ? (i64)nin : (i64)nsel[1];
+  // weights into the K-major swizzled tiles: W2 row = output unit, K = input unit
+  for (int q = tid; q < PRED_W * PRED_W / 8; q += MLP_T) {
+    const int n = q / (PRED_W / 8), k0 = (q % (PRED_W / 8)) * 8;
+    uint32_t w[4];
+    for (int j = 0; j < 4; j++) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(W2[n * PRED_W + k0 + 2 * j], W2[n * PRED_W + k0 + 2 * j + 1]);
+      w[j] = *(const uint32_t *)&h;
     }
-    __syncthreads();
-    {  // layer 1: thread u computes unit u for the 64 elements
-      const int u = threadIdx.x;
-      float w[PRED_IN];
-      for (int i = 0; i < PRED_IN; i++) w[i] = bfr(W1[u * PRED_IN + i]);
-      const float bb = b1[u];
-      for (int e = 0; e < INF_E; e++) {
-        float acc = bb;
-        for (int i = 0; i < PRED_IN; i++) acc = fmaf(xs[e * PRED_IN + i], w[i], acc);
-        h1[e * PRED_W + u] = __float2bfloat16_rn(tanhf(acc));
+    *(uint4 *)(w2s + sw128_offset(PRED_W, n, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  for (int q = tid; q < PRED_W * 2; q += MLP_T) {  // W1: K 0..15 (inputs 12..15 are zero)
+    const int n = q >> 1, k0 = (q & 1) * 8;
+    uint32_t w[4];
+    for (int j = 0; j < 4; j++) {
+      const int k = k0 + 2 * j;
+      const float a = k < PRED_IN ? W1[n * PRED_IN + k] : 0.f, b = k + 1 < PRED_IN ? W1[n * PRED_IN + k + 1] : 0.f;
+      const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+      w[j] = *(const uint32_t *)&h;
+    }
+    *(uint4 *)(w1s + sw128_offset(PRED_W, n, k0)) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(PRED_W));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot, trow = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t IDESC = idesc_bf16(MLP_T, PRED_W), mb = smem_u32(bar);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (i64 base = (i64)blockIdx.x * MLP_T; base < total && ok; base += (i64)gridDim.x * MLP_T) {
+    // inputs of this thread's element into the A tile (K block 0, chunks 0 and 1)
+    const i64 slot = base + tid;
+    float x[PRED_IN] = {};
+    double s6 = 0.0;
+    i64 idx = -1;
+    Series s;
+    if (slot < total) {
+      if (xin) {
+        for (int i = 0; i < PRED_IN; i++) x[i] = xin[slot * PRED_IN + i];
+        s6 = 1.0;
+      } else {
+        idx = sel[slot];
+        double2 p;
+        if (!(series_of(G, T, idx, s) && features(s, exw, x, p, s6))) s6 = 0.0;
       }
     }
-    __syncthreads();
-    {  // layer 2 and the output layer
-      float acc[16][4];
-      for (int e = 0; e < 16; e++)
-        for (int j = 0; j < 4; j++) acc[e][j] = b2r[j];
-      const __nv_bfloat16 *hb = h1 + (eg * 16) * PRED_W;
-#pragma unroll 2
-      for (int k = 0; k < PRED_W; k++) {
-        const uint2 wv = *(const uint2 *)(w2t + k * PRED_W + ug * 4);
-        const float2 w01 = __bfloat1622float2(*(const __nv_bfloat162 *)&wv.x);
-        const float2 w23 = __bfloat1622float2(*(const __nv_bfloat162 *)&wv.y);
-#pragma unroll
-        for (int e = 0; e < 16; e++) {
-          const float h = __bfloat162float(hb[e * PRED_W + k]);
-          acc[e][0] = fmaf(h, w01.x, acc[e][0]);
-          acc[e][1] = fmaf(h, w01.y, acc[e][1]);
-          acc[e][2] = fmaf(h, w23.x, acc[e][2]);
-          acc[e][3] = fmaf(h, w23.y, acc[e][3]);
-        }
+    for (int c = 0; c < 2; c++) {
+      uint32_t w[4];
+      for (int j = 0; j < 4; j++) {
+        const int k = c * 8 + 2 * j;
+        const __nv_bfloat162 h = __floats2bfloat162_rn(k < PRED_IN ? x[k] : 0.f, k + 1 < PRED_IN ? x[k + 1] : 0.f);
+        w[j] = *(const uint32_t *)&h;
       }
+      *(uint4 *)(hs + sw128_offset(MLP_T, tid, c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {  // layer 1: one K = 16 step
+      mma_bf16(tmem, sw128_desc(smem_u32(hs)), sw128_desc(smem_u32(w1s)), IDESC, 0u);
+      mma_commit(mb);
+    }
+    ok = mbar_wait_drain(mb, phase, err, 6);
+    phase ^= 1u;
+    if (!ok) break;
+    tc_fence_after();
+    // layer-1 epilogue: h1 = bf(tanh(acc + b1)) into the A tile, K = hidden unit
+    for (int c0 = 0; c0 < PRED_W; c0 += 64) {
+      float v[64];
+      tmem_ld64(trow + (uint32_t)c0, v);
 #pragma unroll
-      for (int e = 0; e < 16; e++) {
-        float y0 = 0.f, y1 = 0.f;
+      for (int c = 0; c < 8; c++) {
+        uint32_t w[4];
+#pragma unroll
         for (int j = 0; j < 4; j++) {
-          const float h2 = bfr(tanhf(acc[e][j]));
-          y0 = fmaf(h2, w3r[0][j], y0);
-          y1 = fmaf(h2, w3r[1][j], y1);
+          const int u = c0 + c * 8 + 2 * j;
+          const __nv_bfloat162 h = __floats2bfloat162_rn(tanhf(v[c * 8 + 2 * j] + b1[u]),
+                                                         tanhf(v[c * 8 + 2 * j + 1] + b1[u + 1]));
+          w[j] = *(const uint32_t *)&h;
         }
-        for (int o = 16; o > 0; o >>= 1) {
-          y0 += __shfl_xor_sync(0xffffffffu, y0, o);
-          y1 += __shfl_xor_sync(0xffffffffu, y1, o);
-        }
-        if ((threadIdx.x & 31) == 0) {
-          atomicAdd(&ys[(eg * 16 + e) * 2], y0);
-          atomicAdd(&ys[(eg * 16 + e) * 2 + 1], y1);
-        }
+        *(uint4 *)(hs + sw128_offset(MLP_T, tid, c0 + c * 8)) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
     __syncthreads();
-    if (threadIdx.x < INF_E) {
-      const i64 idx = base + threadIdx.x < total ? sel[base + threadIdx.x] : -1;
-      if (idx >= 0) {
-        const double s6 = sc[threadIdx.x];
+    tc_fence_after();
+    if (tid == 0) {  // layer 2: 4 K blocks x 4 K = 16 steps
+      for (int kb = 0; kb < 4; kb++)
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+          mma_bf16(tmem, sw128_desc(smem_u32(hs + kb * MLP_T * 128 + kk * 32)),
+                   sw128_desc(smem_u32(w2s + kb * PRED_W * 128 + kk * 32)), IDESC, (kb | kk) ? 1u : 0u);
+      mma_commit(mb);
+    }
+    ok = mbar_wait_drain(mb, phase, err, 7);
+    phase ^= 1u;
+    if (!ok) break;
+    tc_fence_after();
+    // layer-2 epilogue and the output layer
+    float y0 = 0.f, y1 = 0.f;
+    for (int c0 = 0; c0 < PRED_W; c0 += 64) {
+      float v[64];
+      tmem_ld64(trow + (uint32_t)c0, v);
+#pragma unroll
+      for (int j = 0; j < 64; j++) {
+        const int u = c0 + j;
+        const float h2 = bfr(tanhf(v[j] + b2[u]));
+        y0 = fmaf(h2, bfr(W3[u]), y0);
+        y1 = fmaf(h2, bfr(W3[PRED_W + u]), y1);
+      }
+    }
+    if (slot < total) {
+      if (xin) {
+        yout[slot * 2] = y0 + b3[0];
+        yout[slot * 2 + 1] = y1 + b3[1];
+      } else {
         double2 cr = make_double2(0, 0);
         if (s6 > 0.0) {
-          const double yr = fmin(CLIP, fmax(-CLIP, (double)(ys[threadIdx.x * 2] + b3[0])));
-          const double yi = fmin(CLIP, fmax(-CLIP, (double)(ys[threadIdx.x * 2 + 1] + b3[1])));
+          const double yr = fmin(CLIP, fmax(-CLIP, (double)(y0 + b3[0])));
+          const double yi = fmin(CLIP, fmax(-CLIP, (double)(y1 + b3[1])));
           cr = make_double2(s6 * yr, s6 * yi);
-          Series s;
-          series_of(G, T, idx, s);
           double2 *dst = (double2 *)s.z[0];
           dst->x += cr.x;
           dst->y += cr.y;
@@ -260,6 +311,16 @@ __global__ void __launch_bounds__(TPB) infer_kernel(DevGF G, int T, const i64 *s
         if (corr_out) corr_out[idx] = cr;
       }
     }
+    // the next tile's inputs overwrite the A tile only after every thread read its TMEM lanes
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(PRED_W));
   }
 }
 
@@ -448,7 +509,6 @@ Predictor::Predictor(Ctx &c, i64 capacity, unsigned long long seed_) : ctx(c), c
 }
 
 Predictor::~Predictor() {
-  if (w2t) cudaFree(w2t);
   if (s6buf) cudaFree(s6buf);
   if (sel) cudaFree(sel);
   if (selw) cudaFree(selw);
@@ -590,18 +650,35 @@ double Predictor::train(int iters, int B, double lr) {
   return l;
 }
 
+void Predictor::ensure_mlp() {
+  static std::atomic<bool> attr[64];  // per device (host threads may race here)
+  NEDY_REQUIRE(ctx.device < 64, "device index out of range");
+  if (!attr[ctx.device].load()) {
+    NEDY_CUDA(cudaFuncSetAttribute(mlp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_SMEM));
+    attr[ctx.device].store(true);
+  }
+  if (!selw) {
+    NEDY_CUDA(cudaMalloc(&selw, 2 * sizeof(unsigned long long) + sizeof(int)));
+    NEDY_CUDA(cudaMemsetAsync(selw, 0, 2 * sizeof(unsigned long long) + sizeof(int), ctx.stream));
+  }
+}
+
+int *Predictor::err_word() const { return (int *)(selw + 2); }
+
+void Predictor::check_err() {
+  int e = 0;
+  NEDY_CUDA(cudaMemcpyAsync(&e, err_word(), sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  NEDY_CUDA(cudaStreamSynchronize(ctx.stream));
+  if (e) {
+    NEDY_CUDA(cudaMemsetAsync(err_word(), 0, sizeof(int), ctx.stream));
+    throw CudaError("learned predictor: a bounded tensor-core wait timed out");
+  }
+}
+
 void Predictor::apply(const DevGF &g, int T, double2 *corr_out) {
   const i64 tot = row_elements(g, T);
   if (tot == 0) return;
-  static std::atomic<bool> attr[64];  // per device (host threads may race here)
-  const int smem = PRED_W * PRED_W * 2 + INF_E * PRED_W * 2 + INF_E * PRED_IN * 4 + INF_E * 2 * 4 + INF_E * 8;
-  NEDY_REQUIRE(ctx.device < 64, "device index out of range");
-  if (!attr[ctx.device].load()) {
-    NEDY_CUDA(cudaFuncSetAttribute(infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr[ctx.device].store(true);
-  }
-  if (!w2t) NEDY_CUDA(cudaMalloc(&w2t, sizeof(__nv_bfloat16) * PRED_W * PRED_W));
-  if (!selw) NEDY_CUDA(cudaMalloc(&selw, 2 * sizeof(unsigned long long)));
+  ensure_mlp();
   if (sel_cap < tot) {  // grown geometrically, so that a run reallocates a few times at most
     const i64 cap2 = std::max<i64>(tot, sel_cap + sel_cap / 2);
     NEDY_CUDA(cudaStreamSynchronize(ctx.stream));
@@ -614,8 +691,6 @@ void Predictor::apply(const DevGF &g, int T, double2 *corr_out) {
     NEDY_CUDA(cudaMalloc(&sel, sizeof(i64) * cap2));
     sel_cap = cap2;
   }
-  w2t_kernel<<<64, TPB, 0, ctx.stream>>>(W + OW2, w2t);
-  NEDY_CHECK_LAUNCH();
   NEDY_CUDA(cudaMemsetAsync(selw, 0, 2 * sizeof(unsigned long long), ctx.stream));
   const unsigned gb = (unsigned)std::min<i64>((tot + TPB - 1) / TPB, 148LL * 8);
   s6_kernel<<<gb, TPB, 0, ctx.stream>>>(g, T, tot, ctx.d_ex, s6buf, selw);
@@ -623,9 +698,19 @@ void Predictor::apply(const DevGF &g, int T, double2 *corr_out) {
   select_kernel<<<gb, TPB, 0, ctx.stream>>>(tot, s6buf, selw, sel, corr_out);
   NEDY_CHECK_LAUNCH();
   // the selected count is read by the kernel; the grid covers every element in the worst case
-  const unsigned blocks = (unsigned)std::min<i64>((tot + INF_E - 1) / INF_E, 148LL);
-  infer_kernel<<<blocks, TPB, smem, ctx.stream>>>(g, T, sel, selw, ctx.d_ex, W, w2t, corr_out);
+  const unsigned blocks = (unsigned)std::min<i64>((tot + MLP_T - 1) / MLP_T, 148LL);
+  mlp_tc_kernel<<<blocks, MLP_T, MLP_SMEM, ctx.stream>>>(g, T, sel, selw, ctx.d_ex, W, corr_out, nullptr, 0, nullptr,
+                                                         err_word());
   NEDY_CHECK_LAUNCH();
+}
+
+void Predictor::infer(int n, const float *x, float *y) {
+  ensure_mlp();
+  const unsigned blocks = (unsigned)std::min<i64>((n + MLP_T - 1) / MLP_T, 148LL);
+  mlp_tc_kernel<<<blocks, MLP_T, MLP_SMEM, ctx.stream>>>(DevGF{}, 0, nullptr, nullptr, nullptr, W, nullptr, x, n, y,
+                                                         err_word());
+  NEDY_CHECK_LAUNCH();
+  check_err();
 }
 
 void Predictor::judge(const DevGF &g, int T, const double2 *saved, const double2 *corr, double &d_learned,
@@ -642,6 +727,7 @@ void Predictor::judge(const DevGF &g, int T, const double2 *saved, const double2
   NEDY_CUDA(cudaStreamSynchronize(ctx.stream));
   d_learned = __builtin_bit_cast(double, h[0]);
   d_plain = __builtin_bit_cast(double, h[1]);
+  if (selw) check_err();
 }
 
 }  // namespace nedy

@@ -24,6 +24,8 @@ class Predictor {
   // adds the learned correction to row T (which holds the polynomial extrapolation);
   // corr_out (optional, row_elements values) receives the corrections
   void apply(const DevGF &g, int T, double2 *corr_out);
+  // the network on the tensor cores for n given input rows (device x: n x PRED_IN, y: n x 2)
+  void infer(int n, const float *x, float *y);
   static i64 row_elements(const DevGF &g, int T);
   // after the first corrector iteration: max change from the learned and from the plain
   // prediction over the corrected elements (saved: the row before the iteration)
@@ -47,12 +49,14 @@ class Predictor {
   i64 work_cap = 0;
   unsigned long long ncollect = 0;
   long long adam_t = 0;
-  __nv_bfloat16 *w2t = nullptr;
   // selection of the elements the network corrects (grown once for the longest row)
   double *s6buf = nullptr;
   i64 *sel = nullptr;
-  unsigned long long *selw = nullptr;  // [0] row max of s6 (as bits), [1] selected count
+  unsigned long long *selw = nullptr;  // [0] row max of s6 (as bits), [1] selected count, then the error word
   i64 sel_cap = 0;
+  void ensure_mlp();
+  int *err_word() const;
+  void check_err();
 };
 
 }  // namespace nedy

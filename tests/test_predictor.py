@@ -50,6 +50,28 @@ def test_predictor_forward_and_gradient_match_cpu():
     ctx.close()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 128, 300, 5000])
+def test_tensor_core_inference_matches_cpu(n):
+    """The inference kernel of the steps (tcgen05, 128 rows per CTA, ragged last tile, more
+    tiles than CTAs) against the CPU restatement with the same BF16 operand rounding."""
+    from nedyson_b200 import api
+    ctx = api.Context(12, 8, 4, 5, 1.0, 0.02)
+    pr = api.Predictor(ctx, 1 << 10, seed=7)
+    rng = np.random.default_rng(n)
+    w = pr.params()
+    w += rng.normal(0, 0.05, w.size).astype(np.float32)  # biases and all weights nonzero
+    pr.set_params(w)
+    x = rng.uniform(-1, 1, (n, mlp.IN)).astype(np.float32)
+    y = pr.infer(x)
+    yc, _ = mlp.forward(w, x)
+    err = np.abs(y - yc).max() / np.abs(yc).max()
+    print(f"tensor-core inference n={n}: {err:.2e} of the largest output")
+    assert err <= 2e-3
+    pr.close()
+    ctx.close()
+
+
 def _sim(seed, kw, nt=50, nao=6):
     from nedyson_b200.inputs import make_problem
     from nedyson_b200.simulation import DecompSimulation
@@ -111,3 +133,37 @@ def test_predictor_trains_on_engine_trajectories_and_beats_extrapolation():
     assert np.all(gain > 1.0)
     P.close()
     s.ctx.close()
+
+
+@pytest.mark.gpu
+def test_learned_predictor_needs_fewer_iterations_at_tight_tolerance():
+    """Trained on the first 50 steps of a trajectory (nao=16), the learned prediction beats
+    the polynomial one on the judged steps of the next 40 and, at tol 1e-9 where the
+    prediction error decides the corrector's iteration count, needs fewer iterations:
+    two identical simulations step from the same state, one per predictor."""
+    from nedyson_b200 import api
+    kw = {"E0": 0.08, "t0": 0.6, "sigma": 0.2}
+    sims = [_sim(21, kw, nt=90, nao=16) for _ in range(2)]
+    for s in sims:
+        s.free_gf()
+        s.do_boot()
+    P = api.Predictor(sims[0].ctx, 1 << 21, seed=5)
+    for t in range(6, 51):
+        for s in sims:
+            s.do_tstp_tol(t, 1e-13, 8)
+        if t >= 9:
+            P.collect(sims[0].G, t, 1)
+    P.train(2000, 1024, 1e-3)
+    sims[0].ctx.set_predictor(P)
+    its = [0, 0]
+    for t in range(51, 91):
+        for i, s in enumerate(sims):
+            its[i] += s.do_tstp_tol(t, 1e-9, 6)[0]
+    st = sims[0].ctx.predictor_stats()
+    print(f"iterations over 40 steps: learned {its[0]}, polynomial {its[1]}; judged {st}")
+    assert st["judged"] >= 30 and st["learned_better"] >= 0.8 * st["judged"]
+    assert its[0] < its[1]
+    P.close()
+    for s in sims:
+        s.ctx.close()
+
