@@ -207,6 +207,61 @@ __device__ __forceinline__ void store_pieces64_staged(const Params &P, __nv_bflo
   }
 }
 
+// BF16 pieces of 64 columns of any alignment (the columns may cross index segments of the
+// output View, e.g. (l, n) with n < nao for nao not a multiple of 16): one piece at a time
+// staged through the warp's buffer (values re-read from TMEM 16 columns at a time, so that
+// few registers stay live), then written a row at a time, lane i storing columns i and
+// i + 32 of the row, so that each store instruction covers consecutive columns of one row
+// instead of one scattered element in each of 32 rows.
+__device__ __noinline__ void store_pieces64_generic(const Params &P, __nv_bfloat16 *o, i64 roff, int mok, int nf,
+                                                    uint32_t taddr, bool zero, __nv_bfloat16 *sbuf, int lane) {
+  i64 coff[2];
+  bool cok[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int c = nf + lane + 32 * h;
+    cok[h] = c < P.N;
+    coff[h] = cok[h] ? col_off(P, c) : 0;
+  }
+  const float al = (float)P.alpha;
+  for (int p = 0; p < P.out_np; p++) {
+    for (int q = 0; q < 4; q++) {
+      float x[16];
+      tmem_ld16(taddr + (uint32_t)(16 * q), x);
+#pragma unroll
+      for (int j = 0; j < 16; j++) x[j] = zero ? 0.f : al * x[j];
+      for (int pp = 0; pp < p; pp++)  // the residual after the earlier pieces
+#pragma unroll
+        for (int j = 0; j < 16; j++) x[j] -= __bfloat162float(__float2bfloat16_rn(x[j]));
+#pragma unroll
+      for (int j = 0; j < 16; j += 8) {
+        uint32_t w[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x[j + 2 * t], x[j + 2 * t + 1]);
+          w[t] = *(const uint32_t *)&h;
+        }
+        const int ch = (16 * q + j) >> 3;
+        *(uint4 *)(sbuf + lane * STAGE_LD64 + ((ch ^ (lane & 7)) << 3)) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
+    }
+    __syncwarp();
+    __nv_bfloat16 *op = o + (i64)p * P.plane;
+    for (int r = 0; r < 32; r++) {
+      const i64 ro = __shfl_sync(0xffffffffu, roff, r);
+      const int okr = __shfl_sync(0xffffffffu, mok, r);
+      if (!okr) continue;  // uniform across the warp
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = lane + 32 * h;
+        const __nv_bfloat16 v = sbuf[r * STAGE_LD64 + ((((c >> 3) ^ (r & 7)) << 3) | (c & 7))];
+        if (cok[h]) op[ro + coff[h]] = v;
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // FP64 complex outputs of 16 contiguous columns (store, accumulate or atomic add)
 __device__ __forceinline__ void store_fp64_16_staged(const Params &P, i64 roff, int mok, i64 cbase,
                                                      const float (&vr)[16], const float (&vi)[16], double2 *sb,
@@ -280,6 +335,16 @@ __device__ __forceinline__ void epilogue_tile(const Params &P, int m0, int n0, i
             c0 += 64;
             continue;
           }
+        }
+        if (P.out_pieces && !rows_contig && c0 + 64 <= c_hi && P.cs_lo == 1 && nf + 16 < P.N &&
+            (!rows_al8 || (P.cdiv != 0 && ((nf % P.cdiv) + 16 > P.cdiv || (P.cdiv & 15) != 0)))) {
+          // 64 columns that the aligned paths would store element by element
+          __nv_bfloat16 *o = (__nv_bfloat16 *)P.out;
+          for (int part = 0; part < 2; part++)
+            store_pieces64_generic(P, o + (i64)part * P.out_np * P.plane, roff, imok, nf,
+                                   trow + (uint32_t)(part * BN + c0), zero, sbuf, lane);
+          c0 += 64;
+          continue;
         }
         float vr[16], vi[16];
         tmem_ld16(trow + (uint32_t)c0, vr);

@@ -271,7 +271,8 @@ SPLIT_TOL = {"bf16x3": 5e-5, "bf16x2": 5e-4}
 
 
 @pytest.mark.parametrize("mode", ["bf16x3", "bf16x2"])
-@pytest.mark.parametrize("nao,naux,sym,nspin", [(16, 48, True, 1), (16, 40, False, 1), (12, 36, True, 2)])
+@pytest.mark.parametrize("nao,naux,sym,nspin", [(16, 48, True, 1), (16, 40, False, 1), (12, 36, True, 2),
+                                                (23, 70, False, 1), (13, 40, True, 2)])
 def test_sigma_split(nao, naux, sym, nspin, mode):
     from nedyson_b200 import _lib
     prec = {"bf16x3": _lib.PREC_SPLIT_BF16X3, "bf16x2": _lib.PREC_SPLIT_BF16X2}[mode]
