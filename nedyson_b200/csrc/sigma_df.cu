@@ -366,7 +366,9 @@ struct DF {
       View w = rowmajor(vzt, es); w.bs1 = N2A;
       split_pieces(w, true, false, (int)es, Zp, s);
     }
-    if (kpN != es) NEDY_CUDA(cudaMemsetAsync(Sp.p, 0, Sp.elems() * 2, s));
+    if (kpN != es)  // only the K padding of every S' row must be zero (the GEMM writes the rest)
+      NEDY_CUDA(cudaMemset2DAsync(Sp.p + es, (size_t)kpN * 2, 0, (size_t)(kpN - es) * 2,
+                                  (size_t)(Sp.elems() / kpN), s));
     {  // computed as S^T (rows (q,j), columns (l,n)) so that each thread stores runs of n
       SplitGemmArgs g;
       g.M = (int)es; g.N = (int)es; g.K = A; g.nb = nu;
