@@ -631,51 +631,70 @@ __device__ __forceinline__ void pb_stage(double2 *dst, int ld, const double2 *sr
   }
 }
 
-__global__ void __launch_bounds__(256, 2)
-    push_blocks_kernel(int mode, int N, int T, int a, int m0, DevGF G, DevGF S, const double2 *X, double2 *Q,
-                       const double *w, i64 w_stride, double alpha, const double *bd, double dscale, int k,
-                       int m_dmax) {
+// Shared memory of push_blocks_kernel: the operand shared by all blocks once, the varying
+// one double-buffered (PUSH_RET: A shared, B_b varies; PUSH_LES: B shared, A_b varies).
+constexpr int PB_ABYTES = 64 * PB_LDA * 16, PB_BBYTES = 64 * PB_LDB * 16;
+inline int push_smem(int mode) { return mode == PUSH_RET ? PB_ABYTES + 2 * PB_BBYTES : PB_BBYTES + 2 * PB_ABYTES; }
+
+__global__ void __launch_bounds__(256, 1)
+    push_blocks_kernel(int mode, int N, int T, int a, int m0, int nb, DevGF G, DevGF S, const double2 *X,
+                       double2 *Q, const double *w, i64 w_stride, double alpha, const double *bd, double dscale,
+                       int k, int m_dmax) {
   extern __shared__ double2 pbs[];
-  double2 *As = pbs, *Bs = pbs + 64 * PB_LDA;
-  const int b = blockIdx.x, n0 = blockIdx.y * 32;
+  const bool ret = mode == PUSH_RET;
+  const int n0 = blockIdx.y * 32;
   const i64 es = (i64)N * N;
-  const double2 *A, *B;
-  if (mode == PUSH_RET) {
-    A = G.retptr(T, T - a);
-    B = S.retptr(T - a, T - m0 - b);
-  } else {
-    A = S.retptr(m0 + b, a);
-    B = X + (i64)a * es;
-  }
-  double2 *C = Q + (i64)(m0 + b) * es;
-  const double s = alpha * w[(i64)b * w_stride];
-  const int dl = m0 + b - a;
-  const double g = (dl >= 1 && dl <= k + 1 && m0 + b <= m_dmax) ? bd[dl] * dscale : 0.0;
-  pb_stage(As, PB_LDA, A, N, 64, 64, 0);
-  pb_stage(Bs, PB_LDB, B, N, 64, 32, n0);
+  // shared operand, then the two buffers of the varying one
+  double2 *sh = pbs, *v0 = pbs + (ret ? 64 * PB_LDA : 64 * PB_LDB);
+  const int vstride = ret ? 64 * PB_LDB : 64 * PB_LDA;
+  auto stage_var = [&](int b, double2 *dst) {
+    if (ret)
+      pb_stage(dst, PB_LDB, S.retptr(T - a, T - m0 - b), N, 64, 32, n0);
+    else
+      pb_stage(dst, PB_LDA, S.retptr(m0 + b, a), N, 64, 64, 0);
+  };
+  if (ret)
+    pb_stage(sh, PB_LDA, G.retptr(T, T - a), N, 64, 64, 0);
+  else
+    pb_stage(sh, PB_LDB, X + (i64)a * es, N, 64, 32, n0);
+  if ((int)blockIdx.x < nb) stage_var(blockIdx.x, v0);
   asm volatile("cp.async.commit_group;\n" ::);
-  asm volatile("cp.async.wait_group 0;\n" ::);
-  __syncthreads();
-  double cr[2][2][2] = {}, ci[2][2][2] = {};
-  pb_product(As, Bs, N, cr, ci);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = (warp >> 1) * 16, wn = (warp & 1) * 16;
+  int it = 0;
+  for (int b = blockIdx.x; b < nb; b += gridDim.x, it++) {
+    double2 *cur = v0 + (it & 1) * vstride, *nxt = v0 + ((it + 1) & 1) * vstride;
+    if (b + (int)gridDim.x < nb) stage_var(b + gridDim.x, nxt);  // overlaps this block's product
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 1;\n" ::);
+    __syncthreads();
+    const double2 *As = ret ? sh : cur, *Bs = ret ? cur : sh;
+    double cr[2][2][2] = {}, ci[2][2][2] = {};
+    pb_product(As, Bs, N, cr, ci);
+    double2 *C = Q + (i64)(m0 + b) * es;
+    const double s = alpha * w[(i64)b * w_stride];
+    const int dl = m0 + b - a;
+    const double g = (dl >= 1 && dl <= k + 1 && m0 + b <= m_dmax) ? bd[dl] * dscale : 0.0;
 #pragma unroll
-  for (int i = 0; i < 2; i++) {
-    const int r = wm + i * 8 + (lane >> 2);
-    if (r >= N) continue;
+    for (int i = 0; i < 2; i++) {
+      const int r = wm + i * 8 + (lane >> 2);
+      if (r >= N) continue;
 #pragma unroll
-    for (int j = 0; j < 2; j++)
+      for (int j = 0; j < 2; j++)
 #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        const int col = n0 + wn + j * 8 + (lane & 3) * 2 + c;
-        if (col >= N) continue;
-        const double2 y = mode == PUSH_RET ? As[r * PB_LDA + col] : Bs[r * PB_LDB + col - n0];
-        double2 &o = C[(i64)r * N + col];
-        o.x += s * cr[i][j][c] + g * y.y;  // -i g y
-        o.y += s * ci[i][j][c] - g * y.x;
-      }
+        for (int c = 0; c < 2; c++) {
+          const int col = n0 + wn + j * 8 + (lane & 3) * 2 + c;
+          if (col >= N) continue;
+          // the pushed block Y (derivative term) is the shared operand
+          const double2 y = ret ? sh[r * PB_LDA + col] : sh[r * PB_LDB + col - n0];
+          double2 &o = C[(i64)r * N + col];
+          o.x += s * cr[i][j][c] + g * y.y;  // -i g y
+          o.y += s * ci[i][j][c] - g * y.x;
+        }
+    }
+    __syncthreads();  // every thread is done with `cur` before the next prefetch reuses it
   }
+  asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
 // One step of a sequential sweep as a block product on the FP64 tensor path (nao <= 64), one
@@ -724,23 +743,30 @@ __global__ void __launch_bounds__(256, 1)
   }
 }
 
-// Launches push_blocks_kernel for nb blocks (nao <= 64); false when nao is larger.
+// Launches push_blocks_kernel for nb blocks (nao <= 64); false when nao is larger.  One CTA
+// per SM and column half, each looping over its blocks.
 bool push_blocks(Ctx &c, int mode, int N, int T, int a, int m0, int nb, const DevGF &G, const DevGF &S,
                  const double2 *X, double2 *Q, const double *w, i64 w_stride, double alpha, double dscale,
                  int m_dmax) {
   if (N > 64) return false;
   if (nb <= 0) return true;
   static std::atomic<bool> attr_set[64];  // per device (host threads may race here)
+  static std::atomic<int> sms_of[64];
   int dev = 0;
   NEDY_CUDA(cudaGetDevice(&dev));
   NEDY_REQUIRE(dev < 64, "device index out of range");
   if (!attr_set[dev].load()) {
-    NEDY_CUDA(cudaFuncSetAttribute(push_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PB_SMEM));
+    NEDY_CUDA(cudaFuncSetAttribute(push_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   std::max(push_smem(PUSH_RET), push_smem(PUSH_LES))));
+    int sms = 0;
+    NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    sms_of[dev].store(sms);
     attr_set[dev].store(true);
   }
-  NEDY_REQUIRE(nb <= 2147483647 / 2, "push_blocks: too many blocks");
-  push_blocks_kernel<<<dim3((unsigned)nb, N > 32 ? 2 : 1), 256, PB_SMEM, c.stream>>>(
-      mode, N, T, a, m0, G, S, X, Q, w, w_stride, alpha, c.d_bd, dscale, c.k, m_dmax);
+  const int halves = N > 32 ? 2 : 1;
+  const int gx = std::max(1, std::min(nb, sms_of[dev].load() / halves));
+  push_blocks_kernel<<<dim3((unsigned)gx, halves), 256, push_smem(mode), c.stream>>>(
+      mode, N, T, a, m0, nb, G, S, X, Q, w, w_stride, alpha, c.d_bd, dscale, c.k, m_dmax);
   NEDY_CHECK_LAUNCH();
   return true;
 }
