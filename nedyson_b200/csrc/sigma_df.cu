@@ -254,7 +254,9 @@ struct DF {
   // C (pieces, zero-padded K) = A * B^T
   void to_pieces(const Pieces &a, const Pieces &b, int M, int Nn, int K, Pieces &out, const View &ov, int nb,
                  int out_K) {
-    if (out.kpad != out_K) NEDY_CUDA(cudaMemsetAsync(out.p, 0, out.elems() * 2, s));
+    if (out.kpad != out_K)  // the GEMM writes columns [0, out_K) of every row; zero the K padding only
+      NEDY_CUDA(cudaMemset2DAsync(out.p + out_K, (size_t)out.kpad * 2, 0, (size_t)(out.kpad - out_K) * 2,
+                                  (size_t)(out.elems() / out.kpad), s));
     SplitGemmArgs g;
     g.M = M; g.N = Nn; g.K = K; g.nb = nb;
     g.A = a; g.B = b;
