@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(MLP_T, 1)
       mma_bf16(tmem, sw128_desc(smem_u32(hs)), sw128_desc(smem_u32(w1s)), IDESC, 0u);
       mma_commit(mb);
     }
-    ok = mbar_wait_drain(mb, phase, err, 6);
+    ok = __syncthreads_and(mbar_wait_drain(mb, phase, err, 6)) != 0;  // one decision for the whole CTA
     phase ^= 1u;
     if (!ok) break;
     tc_fence_after();
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(MLP_T, 1)
                    sw128_desc(smem_u32(w2s + kb * PRED_W * 128 + kk * 32)), IDESC, (kb | kk) ? 1u : 0u);
       mma_commit(mb);
     }
-    ok = mbar_wait_drain(mb, phase, err, 7);
+    ok = __syncthreads_and(mbar_wait_drain(mb, phase, err, 7)) != 0;
     phase ^= 1u;
     if (!ok) break;
     tc_fence_after();
