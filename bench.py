@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--ntau", type=int, default=256)
     ap.add_argument("--t0", type=int, default=100)
     ap.add_argument("--corr", type=int, default=5)
+    ap.add_argument("--window", type=int, default=0,
+                    help="keep only the last W time steps of G^R and G^< on the device (Sigma whole); "
+                         "with --state synthetic the history is built on the device")
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--tight-tol", type=float, default=1e-10,
                     help="tolerance of the predictor ablation forms (0: skip them)")
@@ -397,6 +400,62 @@ def fp64_gemm_peak(device: int) -> float:
     return 2 * n**3 / best / 1e12
 
 
+def _dev_view(ptr: int, shape, torch):
+    """A complex128 torch view of engine device memory (CUDA array interface)."""
+    class _A:
+        __cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<c16", "data": (int(ptr), False),
+                                    "version": 3}
+    return torch.as_tensor(_A(), device="cuda")
+
+
+def fill_synthetic_windowed(G, S, t_first, ntau, x, mu, F, beta, dt, window):
+    """Free propagation of F on rows 0..t_first-1 (the closed forms of inputs.free_history:
+    G^R(t,t') = -i U(t-t'), G^<(t',t) = i U(t-t')^+ f, G^tv(t,tau) = i U(t) e(tau)), written
+    on the device: Sigma = 0.02 G on its full triangles and tv rows, G on its window of rows
+    and its tv rows."""
+    import ctypes as C
+    import torch
+    from nedyson_b200._lib import LES, RET, TV, MAT, check, lib
+    from nedyson_b200.inputs import fermi, fermi_exp
+    N = F.shape[0]
+    es = N * N
+    ev, V = np.linalg.eigh(mu * np.eye(N) - F)
+    Vt = torch.from_numpy(V.astype(np.complex128)).cuda()
+    evt = torch.from_numpy(ev).cuda()
+    d = torch.arange(t_first, device="cuda", dtype=torch.float64)
+    U = (Vt[None] * torch.exp(1j * dt * d[:, None] * evt[None, :])[:, None, :]) @ Vt.conj().T[None]  # U(d)
+    fval = torch.from_numpy((V * fermi(beta, -ev)) @ V.conj().T).cuda()
+    Eret = -1j * U
+    Eles = 1j * U.conj().transpose(1, 2) @ fval
+    taus = beta / 2.0 * (np.asarray(x) + 1.0)
+    core = torch.from_numpy(np.stack([(V * fermi_exp(beta, tau, -ev)) @ V.conj().T for tau in taus])).cuda()
+    mat = np.stack([-(V * fermi_exp(beta, tau, ev)) @ V.conj().T for tau in taus])
+    ntri = t_first * (t_first + 1) // 2
+    ptr = C.c_void_p()
+    views = {}
+    for comp in (LES, RET, TV):
+        check(lib().nedy_gf_device_pointer(S.h, comp, C.byref(ptr)))
+        views[comp] = ptr.value
+    Sret = _dev_view(views[RET], (ntri, N, N), torch)
+    Sles = _dev_view(views[LES], (ntri, N, N), torch)
+    for t in range(t_first):
+        o = t * (t + 1) // 2
+        Sret[o:o + t + 1] = 0.02 * Eret[:t + 1].flip(0)
+        Sles[o:o + t + 1] = 0.02 * Eles[:t + 1].flip(0)
+    check(lib().nedy_gf_device_pointer(G.h, TV, C.byref(ptr)))
+    Gtv = _dev_view(ptr.value, (t_first, ntau + 1, N, N), torch)
+    Stv = _dev_view(views[TV], (t_first, ntau + 1, N, N), torch)
+    for t0 in range(0, t_first, 32):
+        rows = 1j * (U[t0:t0 + 32, None] @ core[None])
+        Gtv[t0:t0 + rows.shape[0]] = rows
+        Stv[t0:t0 + rows.shape[0]] = 0.02 * rows
+    for t in range(max(0, t_first - window + 1), t_first):
+        G.upload(RET, t * (t + 1) // 2, Eret[:t + 1].flip(0).cpu().numpy())
+        G.upload(LES, t * (t + 1) // 2, Eles[:t + 1].flip(0).cpu().numpy())
+    G.upload(MAT, 0, mat)
+    torch.cuda.synchronize()
+
+
 # ------------------------------------------------------------------ engine arm
 def run_engine(args, dist: Dist):
     import torch
@@ -410,6 +469,8 @@ def run_engine(args, dist: Dist):
     if args.no_autotune:
         check(lib().nedy_split_autotune(0))
     N, A, ntau, K, W = args.nao, args.naux, args.ntau, args.steps, args.warmup
+    if args.window and args.state != "synthetic":
+        raise SystemExit("--window builds its state on the device: use it with --state synthetic")
     spin = not args.restricted
     ns = 2 if spin else 1
     t_first = args.t0
@@ -435,7 +496,7 @@ def run_engine(args, dist: Dist):
     ctx = api.Context(nt, ntau, N, 5, args.beta, args.dt, device=dev,
                       workspace_bytes=int(args.workspace_gb * (1 << 30)))
     x, _ = ctx.collocation()
-    G = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]
+    G = [api.green_func(ctx, nt, ntau, N, -1, window=args.window) for _ in range(ns)]
     S = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]
     solver = (api.molGF2SolverSpinDecomp if spin else api.molGF2SolverDecomp)(ctx, p.Vija)
     kk = 5
@@ -507,6 +568,18 @@ def run_engine(args, dist: Dist):
         ctx.synchronize()
         prep = {"equilibrium": eq_info or "Hartree-Fock", "boot_iterations": it + 1, "boot_err": berr,
                 "steps": t_first - kk - 1, "seconds": time.time() - tp}
+    elif args.window:
+        # the free-propagation history built on the device (the host would need the whole
+        # triangles): Sigma's full triangles and both tv histories through device views, G's
+        # window of rows through the row API
+        for s in range(ns):
+            fill_synthetic_windowed(G[s], S[s], t_first, ntau, x, mus[s], Fs[s], args.beta, args.dt, args.window)
+            hm = np.zeros((nt + 1, N, N), np.complex128)
+            hm[:t_first] = Fs[s]
+            hmf.append(api.hmf_buffer(ctx, N, hm))
+        torch.cuda.synchronize(dev)
+        prep = {"state": "synthetic free propagation built on the device", "window": args.window,
+                "device_memory_used_gb": (lambda fr: (fr[1] - fr[0]) / 1e9)(torch.cuda.mem_get_info(dev))}
     else:
         for s in range(ns):
             les, ret, tv, mat = free_history(nt, t_first, ntau, x, mus[s], Fs[s], args.beta, args.dt)

@@ -134,6 +134,17 @@ int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w);
 
 /* --- Green's functions: green_func(nt, ntau, size1, sig) (src/greens.cpp:34-55) --- */
 int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out);
+/* The same with only the last `window` time steps of G^R (rows) and G^< (columns) on the
+ * device (no reference counterpart: the reference holds every triangle, src/greens.cpp:44-45).
+ * A time step of G reads nothing older (its own row, the k+1 rows of the extrapolation,
+ * the learned predictor's history), while Sigma must keep its whole triangles for the Dyson
+ * integrals; so a windowed G and a full Sigma halve the history the device holds, and the
+ * caller streams every finished row out (nedy_gf_download of one row or column, while it is
+ * within the window).  window >= NEDY_GF_MIN_WINDOW; G^tv and G^M stay whole.  Block ranges
+ * of the lesser / retarded components must then lie in one row (column). */
+#define NEDY_GF_MIN_WINDOW 12
+int nedy_gf_create_windowed(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int window, nedy_gf **out);
+int nedy_gf_window(const nedy_gf *g, int *window);
 /* Waits for the device; may be called before or after nedy_ctx_destroy of its context
  * (every other call on the handle needs a live context). */
 int nedy_gf_destroy(nedy_gf *g);

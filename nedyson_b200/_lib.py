@@ -52,6 +52,8 @@ SIGNATURES = {
     "nedy_dense_solve": ([_P, _I, _I, _I, _P, _P], _I),
     "nedy_launch_count": ([], C.c_ulonglong),
     "nedy_gf_create": ([_P, _I, _I, _I, _I, _PP], _I),
+    "nedy_gf_create_windowed": ([_P, _I, _I, _I, _I, _I, _PP], _I),
+    "nedy_gf_window": ([_P, C.POINTER(C.c_int)], _I),
     "nedy_gf_destroy": ([_P], _I),
     "nedy_gf_upload": ([_P, _I, _LL, _LL, _P], _I),
     "nedy_gf_download": ([_P, _I, _LL, _LL, _P], _I),

@@ -80,12 +80,21 @@ class Context:
 class green_func:
     """Device-resident contour Green's function (green_func, reference src/greens.h:17-112)."""
 
-    def __init__(self, ctx: Context, nt, ntau, nao, sig=-1):
+    def __init__(self, ctx: Context, nt, ntau, nao, sig=-1, window: int = 0):
+        """window > 0: only the last `window` time steps of G^R and G^< on the device
+        (nedy_gf_create_windowed); rows are then read and written one time step at a time."""
         self.ctx = ctx
         self.nt, self.ntau, self.nao, self.sig = int(nt), int(ntau), int(nao), int(sig)
         h = C.c_void_p()
-        check(lib().nedy_gf_create(ctx.h, self.nt, self.ntau, self.nao, self.sig, C.byref(h)))
+        if window:
+            check(lib().nedy_gf_create_windowed(ctx.h, self.nt, self.ntau, self.nao, self.sig, int(window),
+                                                C.byref(h)))
+        else:
+            check(lib().nedy_gf_create(ctx.h, self.nt, self.ntau, self.nao, self.sig, C.byref(h)))
         self.h = h
+        w = C.c_int()
+        check(lib().nedy_gf_window(h, C.byref(w)))
+        self.window = w.value
 
     def close(self):
         if getattr(self, "h", None):

@@ -213,6 +213,8 @@ namespace {
 
 double2 *comp_ptr(const nedy_gf *g, int comp, i64 &nblocks) {
   const DevGF &d = g->g;
+  NEDY_REQUIRE(!d.win || (comp != NEDY_LES && comp != NEDY_RET),
+               "windowed green_func: lesser and retarded blocks are addressed a time step at a time");
   switch (comp) {
     case NEDY_LES: nblocks = d.nt >= 0 ? d.ntri() : 0; return d.les;
     case NEDY_RET: nblocks = d.nt >= 0 ? d.ntri() : 0; return d.ret;
@@ -416,16 +418,19 @@ int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w) {
   });
 }
 
-int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out) {
+static int gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int window, nedy_gf **out) {
   return guard([&] {
     NEDY_REQUIRE(ctx && out, "null argument");
     NEDY_REQUIRE(nao > 0 && nt >= -1 && ntau >= 0 && sig * sig == 1, "green_func: bad sizes (greens.cpp:35)");
+    NEDY_REQUIRE(window == 0 || (window >= NEDY_GF_MIN_WINDOW && nt >= 0),
+                 "green_func: a window holds at least NEDY_GF_MIN_WINDOW time steps");
     set_dev(ctx);
     auto *g = new nedy_gf;
     g->ctx = ctx;
     g->device = ctx->c.device;
     DevGF &d = g->g;
     d.nt = nt; d.ntau = ntau; d.nao = nao; d.sig = sig; d.es = (i64)nao * nao;
+    d.win = window > nt ? 0 : window;  // a window as long as the run is the full triangle
     auto alloc = [&](double2 *&p, i64 nblk) {
       if (nblk <= 0) { p = nullptr; return; }
       cudaError_t e = cudaMalloc(&p, sizeof(double2) * nblk * d.es);
@@ -439,8 +444,8 @@ int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **
     try {
       alloc(d.mat, ntau + 1);
       if (nt >= 0) {
-        alloc(d.les, d.ntri());
-        alloc(d.ret, d.ntri());
+        alloc(d.les, d.nstore());
+        alloc(d.ret, d.nstore());
         alloc(d.tv, (i64)(nt + 1) * (ntau + 1));
       }
     } catch (...) {
@@ -452,6 +457,21 @@ int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **
       throw;
     }
     *out = g;
+  });
+}
+
+int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out) {
+  return gf_create(ctx, nt, ntau, nao, sig, 0, out);
+}
+
+int nedy_gf_create_windowed(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int window, nedy_gf **out) {
+  return gf_create(ctx, nt, ntau, nao, sig, window, out);
+}
+
+int nedy_gf_window(const nedy_gf *g, int *window) {
+  return guard([&] {
+    NEDY_REQUIRE(g && window, "null argument");
+    *window = g->g.win;
   });
 }
 
@@ -468,15 +488,34 @@ int nedy_gf_destroy(nedy_gf *g) {
   });
 }
 
+// Windowed lesser / retarded storage: the block range [first, first + nb) of the packed
+// triangle must lie in one retarded row / lesser column t, which must be in the window.
+double2 *window_range(const nedy_gf *g, int comp, i64 first, i64 nb) {
+  const DevGF &d = g->g;
+  i64 t = (i64)((std::sqrt(8.0 * (double)first + 1.0) - 1.0) / 2.0);
+  while (t * (t + 1) / 2 > first) t--;
+  while ((t + 1) * (t + 2) / 2 <= first) t++;
+  const i64 j = first - t * (t + 1) / 2;
+  NEDY_REQUIRE(t <= d.nt && j + nb <= t + 1,
+               "windowed green_func: the block range must lie in one time step's row (column)");
+  return comp == NEDY_RET ? d.retptr(t, j) : d.lesptr(j, t);
+}
+
+double2 *range_ptr(const nedy_gf *g, int comp, i64 first, i64 nb) {
+  if (g->g.win && (comp == NEDY_LES || comp == NEDY_RET)) return window_range(g, comp, first, nb);
+  i64 tot;
+  double2 *p = comp_ptr(g, comp, tot);
+  NEDY_REQUIRE(first >= 0 && nb >= 0 && first + nb <= tot, "block range out of bounds");
+  return p + first * g->g.es;
+}
+
 int nedy_gf_upload(nedy_gf *g, int comp, long long first, long long nb, const void *host) {
   return guard([&] {
     NEDY_REQUIRE(g && host, "null argument");
     set_dev(g->ctx);
-    i64 tot;
-    double2 *p = comp_ptr(g, comp, tot);
-    NEDY_REQUIRE(first >= 0 && nb >= 0 && first + nb <= tot, "block range out of bounds");
-    NEDY_CUDA(cudaMemcpyAsync(p + first * g->g.es, host, sizeof(double2) * nb * g->g.es, cudaMemcpyHostToDevice,
-                              g->ctx->c.stream));
+    NEDY_REQUIRE(first >= 0 && nb >= 0, "block range out of bounds");
+    double2 *dst = range_ptr(g, comp, first, nb);
+    NEDY_CUDA(cudaMemcpyAsync(dst, host, sizeof(double2) * nb * g->g.es, cudaMemcpyHostToDevice, g->ctx->c.stream));
     NEDY_CUDA(cudaStreamSynchronize(g->ctx->c.stream));
     if (comp == NEDY_MAT) g->g.mat_version++;
   });
@@ -486,10 +525,9 @@ int nedy_gf_download(const nedy_gf *g, int comp, long long first, long long nb, 
   return guard([&] {
     NEDY_REQUIRE(g && host, "null argument");
     set_dev(g->ctx);
-    i64 tot;
-    double2 *p = comp_ptr(g, comp, tot);
-    NEDY_REQUIRE(first >= 0 && nb >= 0 && first + nb <= tot, "block range out of bounds");
-    NEDY_CUDA(cudaMemcpyAsync(host, p + first * g->g.es, sizeof(double2) * nb * g->g.es, cudaMemcpyDeviceToHost,
+    NEDY_REQUIRE(first >= 0 && nb >= 0, "block range out of bounds");
+    const double2 *src = range_ptr(g, comp, first, nb);
+    NEDY_CUDA(cudaMemcpyAsync(host, src, sizeof(double2) * nb * g->g.es, cudaMemcpyDeviceToHost,
                               g->ctx->c.stream));
     NEDY_CUDA(cudaStreamSynchronize(g->ctx->c.stream));
   });

@@ -1565,6 +1565,7 @@ void dyson_step(Ctx &c, int n, DevGF &G, const DevGF &Sig, const double2 *hmf, d
   NEDY_REQUIRE(G.nao == Sig.nao && G.ntau == Sig.ntau && G.nt == Sig.nt && G.sig == Sig.sig,
                "dyson_step: G and Sigma shapes differ");
   NEDY_REQUIRE(G.nt == c.nt && G.ntau == c.ntau, "dyson_step: G does not match the context sizes");
+  NEDY_REQUIRE(Sig.win == 0, "dyson_step: Sigma must hold its whole history (the integrals read every time)");
   ensure_tables(c);
   ensure_mixing_kernel(c, G);
   ensure_minv(c, G.nao);

@@ -10,14 +10,26 @@ namespace nedy {
 
 // Contour Green's function resident in HBM, same packing as the reference
 // (greens.cpp:34-195): les column T, ret row T and tv row T are contiguous.
+// win > 0 (windowed): the retarded rows and lesser columns live in a ring of win slots of
+// nt + 1 blocks (row / column t in slot t mod win), i.e. only the last win time steps of the
+// two triangles are on the device.  That is all a time step of G reads (its own row, the
+// k + 1 rows of the extrapolation, the history of the learned predictor, the diagonal of the
+// lesser step); Sigma keeps its full triangles (win = 0), which the Dyson integrals read.
 struct DevGF {
   int nt = 0, ntau = 0, nao = 0, sig = -1;
+  int win = 0;
   i64 es = 0;
   double2 *les = nullptr, *ret = nullptr, *tv = nullptr, *mat = nullptr;
   unsigned long long mat_version = 0;  // bumped whenever G^M is written
   i64 ntri() const { return (i64)(nt + 1) * (nt + 2) / 2; }
-  __host__ __device__ double2 *lesptr(i64 i, i64 j) const { return les + les_idx(i, j) * es; }
-  __host__ __device__ double2 *retptr(i64 i, i64 j) const { return ret + ret_idx(i, j) * es; }
+  // blocks held per triangle on the device
+  i64 nstore() const { return win ? (i64)win * (nt + 1) : ntri(); }
+  __host__ __device__ double2 *lesptr(i64 i, i64 j) const {
+    return les + (win ? (j % win) * (i64)(nt + 1) + i : les_idx(i, j)) * es;
+  }
+  __host__ __device__ double2 *retptr(i64 i, i64 j) const {
+    return ret + (win ? (i % win) * (i64)(nt + 1) + j : ret_idx(i, j)) * es;
+  }
   __host__ __device__ double2 *tvptr(i64 i, i64 m) const { return tv + (i * (ntau + 1) + m) * es; }
   __host__ __device__ double2 *matptr(i64 m) const { return mat + m * es; }
 };

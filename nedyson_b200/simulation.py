@@ -15,6 +15,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import api
+from ._lib import LES, MAT, RET, TV
 from .greens import HostGF
 from .inputs import Problem, drive, g0_from_h0, hf_equilibrium, uhf_equilibrium
 
@@ -22,14 +23,17 @@ from .inputs import Problem, drive, g0_from_h0, hf_equilibrium, uhf_equilibrium
 class DecompSimulation:
     def __init__(self, p: Problem, nt: int, ntau: int, beta: float, dt: float, k: int = 5,
                  corr_steps: int = 5, drive_kind: str = "none", drive_kw: dict | None = None, device: int = 0,
-                 workspace_bytes: int = 0):
+                 workspace_bytes: int = 0, g_window: int = 0):
+        """g_window > 0: G keeps only the last g_window time steps of G^R and G^< on the
+        device (Sigma keeps its whole history); read each finished row with G.ret_row(t) /
+        G.les_col(t) while it is in the window."""
         self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k
         self.corr_steps = corr_steps
         self.drive_kind, self.drive_kw = drive_kind, dict(drive_kw or {})
         self.ctx = api.Context(nt, ntau, p.nao, k, beta, dt, device, workspace_bytes)
         self.x, self.w = self.ctx.collocation()
         N = p.nao
-        self.G = api.green_func(self.ctx, nt, ntau, N, -1)
+        self.G = api.green_func(self.ctx, nt, ntau, N, -1, window=g_window)
         self.Sigma = api.green_func(self.ctx, nt, ntau, N, -1)
         self.solver = api.molGF2SolverDecomp(self.ctx, p.Vija)
         self.dyson = api.dyson(self.ctx)
@@ -56,7 +60,19 @@ class DecompSimulation:
         return g
 
     def free_gf(self):
-        self.G.from_host(self.initial_state())
+        if self.G.window:
+            # the initial rows 0..k only, a time step at a time
+            g = HostGF(self.k, self.ntau, self.p.nao, -1)
+            g0_from_h0(g, self.x, self.mu, self.F, self.beta, self.dt, self.k)
+            if getattr(self, "_Gmat", None) is not None:
+                g.mat[:] = self._Gmat
+            for t in range(self.k + 1):
+                self.G.upload(RET, t * (t + 1) // 2, g.ret_row(t))
+                self.G.upload(LES, t * (t + 1) // 2, g.les_col(t))
+            self.G.upload(TV, 0, g.tv)
+            self.G.upload(MAT, 0, g.mat)
+        else:
+            self.G.from_host(self.initial_state())
         hm = np.zeros((self.nt + 1, self.p.nao, self.p.nao), np.complex128)
         hm[: self.k + 1] = self.F
         self.hmf.upload(hm)
