@@ -424,11 +424,12 @@ def fill_synthetic_windowed(G, S, t_first, ntau, x, mu, F, beta, dt, window):
     evt = torch.from_numpy(ev).cuda()
     d = torch.arange(t_first, device="cuda", dtype=torch.float64)
     U = (Vt[None] * torch.exp(1j * dt * d[:, None] * evt[None, :])[:, None, :]) @ Vt.conj().T[None]  # U(d)
-    fval = torch.from_numpy((V * fermi(beta, -ev)) @ V.conj().T).cuda()
+    fval = torch.from_numpy(((V * fermi(beta, -ev)) @ V.conj().T).astype(np.complex128)).cuda()
     Eret = -1j * U
     Eles = 1j * U.conj().transpose(1, 2) @ fval
     taus = beta / 2.0 * (np.asarray(x) + 1.0)
-    core = torch.from_numpy(np.stack([(V * fermi_exp(beta, tau, -ev)) @ V.conj().T for tau in taus])).cuda()
+    core = torch.from_numpy(np.stack([(V * fermi_exp(beta, tau, -ev)) @ V.conj().T
+                                      for tau in taus]).astype(np.complex128)).cuda()
     mat = np.stack([-(V * fermi_exp(beta, tau, ev)) @ V.conj().T for tau in taus])
     ntri = t_first * (t_first + 1) // 2
     ptr = C.c_void_p()
