@@ -103,12 +103,14 @@ int nedy_split_tune_report(char *buf, int len);
 int nedy_sigma_chunk_plan(int nao, int naux, long long budget, int precision, int real_symmetric, int sms, int *chunk,
                           int *sub);
 /* Check of one split GEMM kernel instance (test hook, no reference counterpart):
- * C (nb x M x N) = 0.75 * op(A) op(B)^T (+ C when accumulate) on seeded uniform operands
+ * C (nb x M x N) = 0.75 * op(A) op(B)^T (+ C when accumulate is 1; accumulate 2: the product
+ * replaces a C filled with values that must not be read) on seeded uniform operands
  * (complex when *_cplx, conjugated when conj_*), split into npieces BF16 pieces, with the
  * given instance: tile_n 64/128/256 output columns per CTA, stages, k_block 0 for the
  * per-product kernel or 32/64 for the one-load kernel, kdiv the K-split divisor, persistent
- * != 0 the persistent one-load kernel (one CTA per SM over a tile list, two TMEM
- * accumulators; tile_n 128, out_pieces only).  *rel_err = max |C - C_fp64| / max |C_fp64|; NEDY_ERR_ARG for
+ * 1 the persistent one-load kernel (one CTA per SM over a tile list, two TMEM
+ * accumulators; tile_n 128, out_pieces only), persistent 2 the CTA-pair one-load kernel
+ * (clusters of two CTAs, 256-row tiles by tcgen05.mma.cta_group::2; complex x complex).  *rel_err = max |C - C_fp64| / max |C_fp64|; NEDY_ERR_ARG for
  * an instance that does not exist or does not fit in shared memory. */
 int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, int b_cplx, int conj_a, int conj_b,
                           int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,

@@ -348,7 +348,7 @@ int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, i
     k.M = M; k.N = N; k.K = K; k.nb = nb;
     k.a_cplx = a_cplx; k.b_cplx = b_cplx; k.conjA = conj_a; k.conjB = conj_b; k.np = npieces;
     k.out_pieces = out_pieces; k.accumulate = accumulate;
-    k.bn = tile_n; k.stages = stages; k.bk = k_block; k.kdiv = kdiv; k.persist = persistent != 0;
+    k.bn = tile_n; k.stages = stages; k.bk = k_block; k.kdiv = kdiv; k.persist = persistent;
     k.seed = seed;
     k.alpha = 0.75;
     cudaStream_t st = nullptr;

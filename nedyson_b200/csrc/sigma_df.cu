@@ -196,13 +196,14 @@ struct DF {
     View vb; vb.p = vyt; vb.rs_lo = N; vb.cdiv = N; vb.cs_hi = NA; vb.cs_lo = 1; vb.bs1 = N2A;
     split_pieces(va, true, false, (int)es, a, s);
     split_pieces(vb, true, false, (int)es, b, s);
-    if (!acc) NEDY_CUDA(cudaMemsetAsync(Pm, 0, sizeof(double2) * nsl * A * A, s));
     SplitGemmArgs g;
     g.M = A; g.N = A; g.K = (int)es; g.nb = nsl;
     g.A = a; g.B = b;
     g.C = rowmajor(Pm, A); g.C.bs1 = (i64)A * A;
     g.alpha = sign;
-    g.accumulate = true;
+    g.accumulate = acc;  // else P is replaced
+    g.overwrite = !acc;
+    g.zero_elems = (i64)nsl * A * A;
     split_gemm(g, s);
   }
   //   W[s] = P[s] (A x A) * Vaij (A x N^2): B operand = pieces of Vija (rows (k,j), K = a)
@@ -263,12 +264,17 @@ struct DF {
     g.out_pieces = true; g.Cp = out; g.C = ov;
     split_gemm(g, s);
   }
-  // C (FP64, accumulated) += alpha * A * B^T
-  void to_fp64(const Pieces &a, const Pieces &b, int M, int Nn, int K, const View &cv, int nb, double alpha) {
+  // C (FP64) += alpha * A * B^T, or, with zero_elems > 0, C = alpha * A * B^T replacing the
+  // first zero_elems complex elements from cv.p (the whole output range)
+  void to_fp64(const Pieces &a, const Pieces &b, int M, int Nn, int K, const View &cv, int nb, double alpha,
+               i64 zero_elems = 0) {
     SplitGemmArgs g;
     g.M = M; g.N = Nn; g.K = K; g.nb = nb;
     g.A = a; g.B = b;
-    g.C = cv; g.alpha = alpha; g.accumulate = true;
+    g.C = cv; g.alpha = alpha;
+    g.accumulate = zero_elems == 0;
+    g.overwrite = zero_elems > 0;
+    g.zero_elems = zero_elems;
     split_gemm(g, s);
   }
   Pieces blk_pieces(Blocks b, bool transpose, void *buf, int np) {
@@ -329,10 +335,9 @@ struct DF {
       View v; v.rdiv = N; v.rs_hi = N; v.rs_lo = kpN; v.cdiv = N; v.cs_hi = (i64)N * kpN; v.cs_lo = 1; v.bs1 = es * kpN;
       to_pieces(vpieces(np), Mp, (int)es, (int)es, A, Sp, v, nu, (int)es);
     }
-    NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * nu * N2A, s));
     {
       View v; v.p = Q; v.rdiv = N; v.rs_hi = A; v.rs_lo = NA; v.cs_lo = 1; v.bs1 = N2A;
-      to_fp64(Sp, zs, (int)es, A, (int)es, v, nu, 1.0);
+      to_fp64(Sp, zs, (int)es, A, (int)es, v, nu, 1.0, (i64)nu * N2A);
     }
     Pieces Qp;
     Qp.p = (__nv_bfloat16 *)wsQ; Qp.rows = N; Qp.kpad = kpad64((int)NA); Qp.nb = nu; Qp.ncomp = 2; Qp.np = np;
@@ -381,13 +386,13 @@ struct DF {
       g.C.bs1 = es * kpN;
       split_gemm(g, s);
     }
-    NEDY_CUDA(cudaMemsetAsync(Q, 0, sizeof(double2) * nu * N2A, s));
-    {
+    {  // Q replaced (every element of the nu units stored once; cleared first under a K split)
       SplitGemmArgs g;
       g.M = (int)es; g.N = A; g.K = (int)es; g.nb = nu;
       g.A = Sp; g.B = Zp;
       g.C.p = Q; g.C.rdiv = N; g.C.rs_hi = A; g.C.rs_lo = NA; g.C.cs_lo = 1; g.C.bs1 = N2A;
-      g.accumulate = true;
+      g.overwrite = true;
+      g.zero_elems = (i64)nu * N2A;
       split_gemm(g, s);
     }
     {
@@ -590,12 +595,11 @@ void sigma_df(Ctx &c, int T, int nspin, DevGF *const *Sig, const DevGF *const *G
         }
         // bubble: P = sum_s VZa VYb^T (FP64), W pieces, Sigma_s += f VZn W
         double2 *P = c.ws.alloc<double2>((i64)nsl * A * A);
-        NEDY_CUDA(cudaMemsetAsync(P, 0, sizeof(double2) * nsl * A * A, c.stream));
         void *vyb = c.ws.get(big);
-        for (int s = 0; s < nspin; s++) {
+        for (int s = 0; s < nspin; s++) {  // the first spin replaces P, the second adds to it
           Pieces yb = d.VYb(ytp[s], vyb, np);
           View pv = rowmajor(P, A); pv.bs1 = (i64)A * A;
-          d.to_fp64(vza[s], yb, A, A, (int)es, pv, nsl, 1.0);
+          d.to_fp64(vza[s], yb, A, A, (int)es, pv, nsl, 1.0, s == 0 ? (i64)nsl * A * A : 0);
         }
         Pieces pp = d.arr(c.ws.get(DF::arr_bytes(A, A, nsl, np)), A, A, nsl, np);
         {

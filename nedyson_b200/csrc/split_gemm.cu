@@ -552,6 +552,195 @@ __global__ void __launch_bounds__(THREADS, (BN == 128 || (BN == 64 && STAGES <= 
   }
 }
 
+// ---- CTA-pair variant of the one-load kernel (tcgen05.mma.cta_group::2)
+// A cluster of two CTAs (adjacent row tiles, the same column tile) computes one 256 x BN
+// tile: each CTA stages its own 128 rows of A and half of the BN rows of B (rows
+// n0 + r BN/2 for pair rank r), so per K block a CTA moves A + B/2 instead of A + B, and
+// its TMEM holds its 128 rows x BN columns of both parts.  Rank 0 issues the MMAs
+// (M = 256, each operand read from the same shared-memory offset in both CTAs).
+// Barriers: every CTA's TMA loads complete on its own full barrier; the MMA warp of rank 1
+// (idle otherwise) waits for each of its stages and arrives remotely on rank 0's full
+// barrier, which therefore expects two arrivals (rank 0's expect_tx and rank 1's); the MMA
+// issuer's tcgen05.commit multicasts stage release (empty) and completion (done) to both
+// CTAs.  Both CTAs take the same path (a skip decided by either is taken by both), every
+// wait is bounded, every CTA drains the loads it issued itself, and a cluster barrier
+// before TMEM is released keeps each CTA's shared memory alive while the other still uses it.
+namespace pr {
+__device__ __forceinline__ uint32_t cta_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t map_to(uint32_t saddr, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(saddr), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ int ld_cluster(uint32_t caddr) {
+  int v;
+  asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(caddr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void arrive_remote(uint32_t caddr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(caddr) : "memory");
+}
+__device__ __forceinline__ void mma2(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+// arrive on the barrier at this shared-memory offset in every CTA of `mask` once the MMAs
+// this thread issued have finished
+__device__ __forceinline__ void commit2(uint32_t mbar, uint16_t mask) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::
+                   "r"(mbar), "h"(mask)
+               : "memory");
+}
+}  // namespace pr
+
+template <int BN, int STAGES, int BKT>
+__global__ void __launch_bounds__(THREADS, 1)
+    split_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                           const __grid_constant__ Params P) {
+  constexpr int A_TILE = BM * BKT * 2;
+  constexpr int BH = BN / 2;               // rows of B this CTA stages
+  constexpr int B_BYTES = BH * BKT * 2;
+  constexpr uint32_t TCOLS = 2 * BN;
+  constexpr uint32_t IDESC = idesc_bf16(2 * BM, BN);
+  extern __shared__ uint8_t sraw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)sraw + 1023) & ~(uintptr_t)1023);
+  uint64_t *bar = (uint64_t *)(smem + STAGES * P.stage_bytes);  // full[STAGES], empty[STAGES], done
+  uint32_t *tmem_slot = (uint32_t *)(bar + 2 * STAGES + 1);
+  __shared__ int s_skip, s_skip_pair;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = pr::cta_rank(), peer = rank ^ 1u, lead = rank & ~1u;
+  const bool leader = (rank & 1u) == 0;
+  const uint16_t mask = (uint16_t)(3u << lead);
+  // grid: x row tiles (pairs of consecutive x form the clusters), y column tiles, z batch x K split
+  const int b = blockIdx.z / P.ksplit, ks = blockIdx.z - (blockIdx.z / P.ksplit) * P.ksplit;
+  const int n0 = blockIdx.y * BN, m0 = blockIdx.x * BM;
+  const int kb0 = ks * P.kb_per_split;
+  const int nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
+  int iters = nkb;
+  const uint32_t full0 = smem_u32(bar), empty0 = smem_u32(bar + STAGES), done = smem_u32(bar + 2 * STAGES);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(full0 + 8 * s, leader ? 2 : 1);  // rank 0: its own expect_tx + rank 1's forward
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_skip = *(volatile int *)P.err != 0;  // an earlier CTA gave up: do nothing
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  pr::cluster_sync();  // barriers of both CTAs initialised, both skip flags written
+  tc_fence_after();
+  if (threadIdx.x == 0) s_skip_pair = s_skip | pr::ld_cluster(pr::map_to(smem_u32(&s_skip), peer));
+  __syncthreads();
+  const uint32_t tmem = *tmem_slot;
+  const bool skip = s_skip_pair != 0;
+  if (skip) iters = 0;
+
+  if (warp == 4 && lane == 0) {
+    // ---- TMA producer (both CTAs): own A rows, own half of the B rows, own full barrier
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    int issued = 0;
+    const int ab = P.a_nb > 1 ? P.a_b0 + b : 0, bb = P.b_nb > 1 ? P.b_b0 + b : 0;
+    const int nb0 = n0 + (int)(rank & 1u) * BH;
+    for (int it = 0; it < iters; it++) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (it >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) break;
+      const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+      mbar_expect_tx(full0 + 8 * s, P.stage_bytes);
+      issued = it + 1;
+      const int kb = kb0 + it;
+      const uint32_t bbase = base + P.np * P.nA * A_TILE;
+      for (int p = 0; p < P.np; p++) {
+        for (int i = 0; i < P.nA; i++)
+          tma_load_3d(base + (p * P.nA + i) * A_TILE, &tmA, full0 + 8 * s, kb * BKT, m0,
+                      (P.a_comp[i] * P.np + p) * P.a_nb + ab);
+        for (int j = 0; j < P.nB; j++)
+          tma_load_3d(bbase + (p * P.nB + j) * B_BYTES, &tmB, full0 + 8 * s, kb * BKT, nb0,
+                      (P.b_comp[j] * P.np + p) * P.b_nb + bb);
+      }
+    }
+    // loads of the last STAGES issued stages may still be in flight (the consumer may have
+    // given up): wait until each has landed, so that none reaches shared memory after exit
+    for (int j = max(0, issued - STAGES); j < issued; j++)
+      mbar_wait_drain(full0 + 8 * (j % STAGES), (uint32_t)(j / STAGES) & 1u, P.err, 4);
+  } else if (warp == 5 && lane == 0 && !leader) {
+    // ---- rank 1: tell rank 0 when each of its stages has landed
+    const uint32_t lfull0 = pr::map_to(full0, lead);
+    for (int it = 0; it < iters; it++) {
+      const int s = it % STAGES;
+      if (!mbar_wait(full0 + 8 * s, (uint32_t)(it / STAGES) & 1u, P.err, 2)) break;
+      pr::arrive_remote(lfull0 + 8 * s);
+    }
+  } else if (warp == 5 && lane == 0) {
+    // ---- rank 0: MMA issuer for the pair
+    bool started0 = false, started1 = false;
+    for (int it = 0; it < iters; it++) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+      if (!mbar_wait(full0 + 8 * s, ph, P.err, 2)) break;
+      tc_fence_after();
+      const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+      const uint32_t bbase = base + P.np * P.nA * A_TILE;
+      for (int pr_ = 0; pr_ < P.nprod; pr_++) {
+        const int sa0 = P.pa[pr_] * P.nA, sb0 = P.pb[pr_] * P.nB;
+        for (int q = 0; q < P.nmma; q++) {
+          const Mma mq = P.mma[q];
+          const uint64_t da = op_desc<BKT>(base + (sa0 + mq.sa) * A_TILE);
+          const uint64_t db = op_desc<BKT>(bbase + (sb0 + mq.sb) * B_BYTES);
+          const uint32_t idesc = IDESC | (mq.neg ? (1u << 13) : 0u);
+          const uint32_t tacc = tmem + (uint32_t)(mq.acc * BN);
+#pragma unroll
+          for (int k = 0; k < BKT / 16; k++)
+            pr::mma2(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                     ((mq.acc ? started1 : started0) || k > 0) ? 1u : 0u);
+          if (mq.acc)
+            started1 = true;
+          else
+            started0 = true;
+        }
+      }
+      pr::commit2(empty0 + 8 * s, mask);
+    }
+    pr::commit2(done, mask);
+  } else if (warp < 4) {
+    // ---- epilogue (both CTAs): this CTA's 128 rows from its own TMEM.  `done` follows
+    // every MMA rank 0 started, also when it gave up; incomplete accumulators are not stored.
+    int okl = 0;
+    if (lane == 0) okl = (mbar_wait_drain(done, 0, P.err, 3) && *(volatile int *)P.err == 0) ? 1 : 0;
+    __syncwarp();
+    const bool ok = __shfl_sync(0xffffffffu, okl, 0) != 0 && !skip;
+    tc_fence_after();
+    if (ok) epilogue_tile<BN>(P, m0, n0, b, warp, lane, tmem, iters == 0, smem + warp * STAGE_WARP_BYTES);
+  }
+  tc_fence_before();
+  __syncthreads();
+  pr::cluster_sync();  // neither CTA releases TMEM or exits while the other still works
+  if (warp == 5) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+  }
+}
+
 // Persistent variant of the one-load kernel: one CTA per SM walks a static list of tiles
 // (tile t, t + gridDim.x, ...), and TMEM holds two accumulators, so that the epilogue warps
 // store tile i while the MMA warp accumulates tile i+1 and the TMA warp loads ahead across
@@ -938,6 +1127,47 @@ void launch_persist(const Params &P, const CUtensorMap &ma, const CUtensorMap &m
   NEDY_CHECK_LAUNCH();
 }
 
+// CTA-pair kernel: grid (column tiles, row tiles, z) of the other kernels launched as
+// (row tiles, column tiles, z), clusters of two consecutive row tiles along x (an even count)
+template <int BN, int STAGES, int BKT>
+void launch_pair(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 grid, cudaStream_t s) {
+  static std::atomic<bool> attr[64];  // per device (host threads may race here)
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  NEDY_REQUIRE(grid.y % 2 == 0, "split_gemm: the pair kernel needs an even number of row tiles");
+  NEDY_REQUIRE(STAGES * P.stage_bytes <= SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  if (!attr[dev].load()) {
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_pair_kernel<BN, STAGES, BKT>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes(SMEM_LIMIT / STAGES, STAGES)));
+    attr[dev].store(true);
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid.y, grid.x, grid.z);
+  cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = (size_t)smem_bytes(P.stage_bytes, STAGES);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, split_gemm_pair_kernel<BN, STAGES, BKT>, ma, mb, P);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    int nclusters = -1;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, split_gemm_pair_kernel<BN, STAGES, BKT>, &cfg) != cudaSuccess)
+      (void)cudaGetLastError();
+    throw CudaError(std::string("split_gemm pair launch: ") + cudaGetErrorString(e) + " (grid " +
+                    std::to_string(cfg.gridDim.x) + "x" + std::to_string(cfg.gridDim.y) + "x" +
+                    std::to_string(cfg.gridDim.z) + ", " + std::to_string(cfg.dynamicSmemBytes) +
+                    " bytes of shared memory, at most " + std::to_string(nclusters) + " active clusters)");
+  }
+  NEDY_CHECK_LAUNCH();
+}
+
 // ---- autotuner: the tile shape (BN, stages) of each problem class is chosen by timing
 // the candidates on the live launches.  Every candidate computes the same result; the
 // first launches of a class cycle through the candidates with CUDA events around them,
@@ -947,6 +1177,7 @@ struct Cand {
   int bn, stages, kdiv;  // kdiv: divide the automatic K split by this (FP64-accumulating outputs)
   int bk;                // 0: per-product kernel (64-wide K blocks); 32 / 64: one-load kernel
   int persist = 0;       // 1: persistent one-load kernel (two TMEM accumulators)
+  int pair = 0;          // 1: CTA-pair one-load kernel (cta_group::2, 256-row tiles)
 };
 struct TuneKey {
   int dev, np, nA, nB, out_pieces, acc, M, N, kpad;
@@ -971,8 +1202,9 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
 bool g_tune_on = true;
 
-// shared memory of one stage
-int stage_bytes_for(int nA, int nB, int np, int bn, int bk) {
+// shared memory of one stage (a CTA of the pair kernel stages half of the B rows)
+int stage_bytes_for(int nA, int nB, int np, int bn, int bk, int pair = 0) {
+  if (pair) return np * (nA * BM * bk * 2 + nB * (bn / 2) * bk * 2);
   return bk == 0 ? nA * A_BYTES + nB * bn * BK * 2 : np * (nA * BM * bk * 2 + nB * bn * bk * 2);
 }
 
@@ -1014,6 +1246,20 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc, bool piece
         const int pst = std::min(bk == 32 ? 4 : 2, (P_SMEM_LIMIT - P_EPI_BYTES) / sb);
         if (pst >= 2) c.push_back({bn, pst, 1, bk, 1});
         if (pst >= 4) c.push_back({bn, 3, 1, bk, 1});
+      }
+    }
+  }
+  // CTA pairs (complex x complex): 256-row tiles, each CTA staging half of B
+  if (nA == 2 && nB == 2) {
+    for (int bn : {128, 256}) {
+      if (N <= 64 || (bn == 256 && N <= 128)) continue;
+      for (int bk : {32, 64}) {
+        const int sb = stage_bytes_for(nA, nB, np, bn, bk, 1);
+        // instances: 128-wide tiles 2-4 stages (K block 32) or 2 (64); 256-wide 2-3 (32)
+        const int st = std::min(bn == 256 ? 3 : bk == 64 ? 2 : 4, SMEM_LIMIT / sb);
+        if (st < 2 || (bn == 256 && bk == 64)) continue;
+        c.push_back({bn, st, 1, bk, 0, 1});
+        if (acc && bn == 256) c.push_back({bn, st, 2, bk, 0, 1});
       }
     }
   }
@@ -1074,7 +1320,8 @@ std::string split_tune_report() {
     for (size_t i = 0; i < e.cands.size(); i++) {
       char buf[96];
       char ol[16] = "";
-      if (e.cands[i].bk) snprintf(ol, sizeof(ol), "/ol%d%s", e.cands[i].bk, e.cands[i].persist ? "p" : "");
+      if (e.cands[i].bk)
+        snprintf(ol, sizeof(ol), "/ol%d%s", e.cands[i].bk, e.cands[i].persist ? "p" : e.cands[i].pair ? "x2" : "");
       snprintf(buf, sizeof(buf), " %d/%d/k%d%s=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv, ol,
                e.trials[i] ? e.best[i] * 1e3 : -1.0, (int)i == e.chosen ? "*" : "");
       r += buf;
@@ -1138,6 +1385,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   int KDsel = 1;
   int BKsel = 0;  // per-product kernel
   int PSsel = 0;  // persistent kernel
+  int PRsel = 0;  // CTA-pair kernel
   if (BNsel >= 128 && 2 * stage_bytes_for(P.nA, P.nB, P.np, BNsel, 32) <= SMEM_LIMIT) {
     BKsel = 32;
     STsel = 2;
@@ -1156,19 +1404,23 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
     NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && g.force_bn == 128 && g.out_pieces),
                  "split_gemm: the persistent kernel is the one-load kernel with 128-wide tiles and piece outputs");
+    NEDY_REQUIRE(!g.force_pair || (g.force_bk != 0 && !g.force_persist && ac && bc),
+                 "split_gemm: the pair kernel is a one-load kernel for complex x complex products");
     BNsel = g.force_bn;
     STsel = g.force_stages;
     KDsel = g.force_kdiv;
     BKsel = g.force_bk;
     PSsel = g.force_persist ? 1 : 0;
+    PRsel = g.force_pair ? 1 : 0;
   } else {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (g_tune_on) {
-      const TuneKey key{dev, P.np, P.nA, P.nB, g.out_pieces ? 1 : 0, g.accumulate ? 1 : 0, g.M, g.N, g.A.kpad};
+      const TuneKey key{dev, P.np, P.nA, P.nB, g.out_pieces ? 1 : 0, g.accumulate ? 1 : g.overwrite ? 2 : 0,
+                        g.M, g.N, g.A.kpad};
       auto it = g_tune.find(key);
       if (it == g_tune.end()) {
         TuneEntry e;
-        e.cands = candidates(P.nA, P.nB, P.np, g.N, g.accumulate && g.ksplit <= 0, g.out_pieces);
+        e.cands = candidates(P.nA, P.nB, P.np, g.N, (g.accumulate || g.overwrite) && g.ksplit <= 0, g.out_pieces);
         e.best.assign(e.cands.size(), 1e30);
         e.trials.assign(e.cands.size(), 0);
         e.inflight.assign(e.cands.size(), 0);
@@ -1191,39 +1443,45 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
         KDsel = e.cands[c].kdiv;
         BKsel = e.cands[c].bk;
         PSsel = e.cands[c].persist;
+        PRsel = e.cands[c].pair;
       }
     }
   }
   const int bkt = BKsel ? BKsel : BK;
-  P.stage_bytes = stage_bytes_for(P.nA, P.nB, P.np, BNsel, BKsel);
+  P.stage_bytes = stage_bytes_for(P.nA, P.nB, P.np, BNsel, BKsel, PRsel);
   // real x complex without conjugation: one N = 2 BN product writes both parts
-  P.fuse = (BKsel && !ac && bc && !g.conjB && 2 * BNsel <= 256) ? 1 : 0;
+  P.fuse = (BKsel && !PRsel && !ac && bc && !g.conjB && 2 * BNsel <= 256) ? 1 : 0;
   P.kblocks = g.A.kpad / 64;  // 64-wide blocks while the K split is chosen
-  const int ntn = (g.N + BNsel - 1) / BNsel, ntm = (g.M + BM - 1) / BM;
+  // row tiles: an even number for CTA pairs (the rows of a last odd tile are out of range:
+  // loaded as zeros, not stored)
+  const int ntn = (g.N + BNsel - 1) / BNsel, ntm = (g.M + BM - 1) / BM + (PRsel ? ((g.M + BM - 1) / BM) & 1 : 0);
   // K split: bounded FP32 accumulation length, and enough CTAs for the GPU
   int ksplit = g.ksplit;
   const i64 tiles = (i64)ntm * ntn * g.nb;
   if (ksplit <= 0) {
     ksplit = 1;
-    if (g.accumulate) {
+    if (g.accumulate || g.overwrite) {
       while (tiles * ksplit < 2 * 148 && P.kblocks / (ksplit * 2) >= 4) ksplit *= 2;
       ksplit = std::max(1, ksplit / KDsel);
       if (g.max_kblocks > 0)
         while ((P.kblocks + ksplit - 1) / ksplit > g.max_kblocks) ksplit++;
     }
   }
-  NEDY_REQUIRE(ksplit == 1 || (g.accumulate && !g.out_pieces), "split_gemm: K split needs an accumulating FP64 output");
+  NEDY_REQUIRE(!(g.accumulate && g.overwrite), "split_gemm: accumulate and overwrite exclude each other");
+  NEDY_REQUIRE(ksplit == 1 || ((g.accumulate || g.overwrite) && !g.out_pieces),
+               "split_gemm: K split needs an accumulating or overwritten FP64 output");
+  NEDY_REQUIRE(!g.overwrite || ksplit == 1 || g.zero_elems > 0, "split_gemm: overwrite with a K split needs zero_elems");
   P.ksplit = ksplit;
   // in units of the kernel's K block
   P.kb_per_split = (P.kblocks + ksplit - 1) / ksplit * (64 / bkt);
   P.kblocks *= 64 / bkt;
   NEDY_REQUIRE((i64)g.nb * ksplit <= 65535 && ntm <= 65535, "split_gemm: grid too large");
   P.out_pieces = g.out_pieces ? 1 : 0;
-  P.accumulate = g.accumulate ? 1 : 0;
+  P.accumulate = g.accumulate ? 1 : 0;  // overwrite without a K split: plain stores
   P.atomic = ksplit > 1 ? 1 : 0;
   P.alpha = g.alpha;
   if (g.out_pieces) {
-    NEDY_REQUIRE(g.Cp.p && g.Cp.ncomp == 2 && !g.accumulate, "split_gemm: bad piece output");
+    NEDY_REQUIRE(g.Cp.p && g.Cp.ncomp == 2 && !g.accumulate && !g.overwrite, "split_gemm: bad piece output");
     P.out = g.Cp.p;
     P.out_np = g.Cp.np;
     P.plane = g.Cp.plane();
@@ -1239,7 +1497,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   P.cdiv = g.C.cdiv;
   P.bs = g.C.bs1;
   P.err = err_word(s);
-  const CUtensorMap ma = make_map(g.A, BM, bkt), mb = make_map(g.B, BNsel, bkt);
+  const CUtensorMap ma = make_map(g.A, BM, bkt), mb = make_map(g.B, PRsel ? BNsel / 2 : BNsel, bkt);
   dim3 grid(ntn, ntm, g.nb * ksplit);
   cudaEvent_t ev[2] = {nullptr, nullptr};
   {
@@ -1266,6 +1524,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     int bk, bn, st;
     LaunchFn fn;
     int persist;
+    int pair = 0;
   };
   static const Inst insts[] = {
       {0, 64, 4, launch<64, 4>, 0},       {0, 64, 2, launch<64, 2>, 0},       {0, 128, 2, launch<128, 2>, 0},
@@ -1276,7 +1535,11 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       {32, 256, 3, launch<256, 3, 32, true>, 0}, {64, 128, 2, launch<128, 2, 64, true>, 0},
       {64, 128, 3, launch<128, 3, 64, true>, 0},
       {32, 128, 2, launch_persist<128, 2, 32>, 1}, {32, 128, 3, launch_persist<128, 3, 32>, 1},
-      {32, 128, 4, launch_persist<128, 4, 32>, 1}, {64, 128, 2, launch_persist<128, 2, 64>, 1}};
+      {32, 128, 4, launch_persist<128, 4, 32>, 1}, {64, 128, 2, launch_persist<128, 2, 64>, 1},
+      {32, 256, 2, launch_pair<256, 2, 32>, 0, 1}, {32, 256, 3, launch_pair<256, 3, 32>, 0, 1},
+      {32, 128, 2, launch_pair<128, 2, 32>, 0, 1}, {32, 128, 3, launch_pair<128, 3, 32>, 0, 1},
+      {32, 128, 4, launch_pair<128, 4, 32>, 0, 1},
+      {64, 128, 2, launch_pair<128, 2, 64>, 0, 1}};
   int st_run = stages;
   if (BKsel == 0) {  // per-product kernel: the instance nearest to the requested stages
     st_run = BNsel == 64 ? (stages <= 2 ? 2 : 4)
@@ -1284,8 +1547,10 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   }
   LaunchFn fn = nullptr;
   for (const Inst &x : insts)
-    if (x.bk == BKsel && x.bn == BNsel && x.st == st_run && x.persist == PSsel) fn = x.fn;
+    if (x.bk == BKsel && x.bn == BNsel && x.st == st_run && x.persist == PSsel && x.pair == PRsel) fn = x.fn;
   NEDY_REQUIRE(fn != nullptr, "split_gemm: no kernel instance for this tile shape");
+  if (g.overwrite && ksplit > 1)  // inside the timed region: part of what a K split costs
+    NEDY_CUDA(cudaMemsetAsync((void *)g.C.p, 0, sizeof(double2) * (size_t)g.zero_elems, s));
   fn(P, ma, mb, grid, s);
   if (te) {
     NEDY_CUDA(cudaEventRecord(tev[1], s));
@@ -1385,11 +1650,15 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
     double2 *C = (double2 *)dalloc(sizeof(double2) * nc), *ref = (double2 *)dalloc(sizeof(double2) * nc);
     check_fill_kernel<<<592, 256, 0, s>>>(na, k.seed * 3 + 1, A);
     check_fill_kernel<<<592, 256, 0, s>>>(nbv, k.seed * 3 + 2, B);
+    // accumulate 1: C += ...; 2: overwrite (C holds values that must not be read)
     if (k.accumulate)
       check_fill_kernel<<<592, 256, 0, s>>>(2 * nc, k.seed * 3 + 3, (double *)C);
     else
       NEDY_CUDA(cudaMemsetAsync(C, 0, sizeof(double2) * nc, s));
-    NEDY_CUDA(cudaMemcpyAsync(ref, C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, s));
+    if (k.accumulate == 2)
+      NEDY_CUDA(cudaMemsetAsync(ref, 0, sizeof(double2) * nc, s));
+    else
+      NEDY_CUDA(cudaMemcpyAsync(ref, C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, s));
     NEDY_CHECK_LAUNCH();
     check_ref_kernel<<<592, 256, 0, s>>>(k.M, k.N, k.K, k.nb, k.a_cplx, k.b_cplx, k.conjA, k.conjB, A, B, k.alpha,
                                          ref);
@@ -1409,7 +1678,8 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
     g.conjA = k.conjA != 0; g.conjB = k.conjB != 0;
     g.alpha = k.alpha;
     g.force_bn = k.bn; g.force_stages = k.stages; g.force_bk = k.bk; g.force_kdiv = k.kdiv;
-    g.force_persist = k.persist;
+    g.force_persist = k.persist == 1;
+    g.force_pair = k.persist == 2;
     double2 *got = C;
     if (k.out_pieces) {
       Pieces cp;
@@ -1424,7 +1694,9 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
       NEDY_CHECK_LAUNCH();
     } else {
       g.C = rowmajor(C, k.N); g.C.bs1 = (i64)k.M * k.N;
-      g.accumulate = k.accumulate != 0;
+      g.accumulate = k.accumulate == 1;
+      g.overwrite = k.accumulate == 2;
+      g.zero_elems = nc;
       split_gemm(g, s);
     }
     unsigned long long *mx = (unsigned long long *)dalloc(2 * sizeof(unsigned long long));
@@ -1434,7 +1706,8 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
     unsigned long long h[2] = {0, 0};
     NEDY_CUDA(cudaMemcpyAsync(h, mx, sizeof(h), cudaMemcpyDeviceToHost, s));
     NEDY_CUDA(cudaStreamSynchronize(s));
-    NEDY_REQUIRE(split_gemm_error(s) == 0, "split_gemm_check: a bounded device wait timed out");
+    if (split_gemm_error(s) != 0)  // NEDY_ERR_TIMEOUT at the C ABI, not an absent instance
+      throw CudaError("split_gemm_check: a bounded device wait timed out");
     double d, r;
     memcpy(&d, &h[0], 8);
     memcpy(&r, &h[1], 8);

@@ -46,12 +46,19 @@ struct SplitGemmArgs {
   View C;                 // FP64 output (C.bs1 = batch stride); element offsets for pieces
   Pieces Cp;              // piece output: planes [comp][piece] of Cp.plane() elements, offsets from C
   bool accumulate = false;  // FP64 output only: C += alpha * A B^T
-  int ksplit = 0;           // 0: choose; > 1 needs accumulate (FP64 atomics)
+  // FP64 output only: C = alpha * A B^T replaces the old contents, which are not read.
+  // Without a K split every element is stored once; with one, the first zero_elems complex
+  // elements from C.p (the whole output range) are cleared on the stream first and the
+  // partial sums are added atomically.
+  bool overwrite = false;
+  i64 zero_elems = 0;
+  int ksplit = 0;           // 0: choose; > 1 needs accumulate or overwrite (FP64 atomics)
   int max_kblocks = 0;      // upper bound on 64-wide K blocks accumulated in FP32 per tile (0: none)
   // a given kernel instance instead of the autotuner's (force_bn 0: autotuner); force_bk 0
   // is the per-product kernel, 32 / 64 the one-load kernel with that K block
   int force_bn = 0, force_stages = 0, force_bk = 0, force_kdiv = 1;
   int force_persist = 0;  // with force_bn: the persistent one-load kernel (force_bk 32 / 64, force_bn 128)
+  int force_pair = 0;     // with force_bn: the CTA-pair one-load kernel (complex x complex)
 };
 
 void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
@@ -62,7 +69,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
 struct SplitCheck {
   int M = 0, N = 0, K = 0, nb = 1;
   int a_cplx = 1, b_cplx = 1, conjA = 0, conjB = 0, np = 3, out_pieces = 0, accumulate = 0;
-  int bn = 128, stages = 2, bk = 0, kdiv = 1, persist = 0;
+  int bn = 128, stages = 2, bk = 0, kdiv = 1, persist = 0;  // persist 1: persistent kernel, 2: CTA pair
   double alpha = 1.0;
   unsigned long long seed = 1;
 };

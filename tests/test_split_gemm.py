@@ -25,15 +25,21 @@ SHAPES = {
     "cxc_acc": (384, 256, 1024, 2, 1, 1, 0, 0, 0, 1),      # FP64 accumulation with a K split
     "cxr_conjA": (256, 320, 128, 1, 1, 0, 1, 0, 0, 0),     # complex x real, ragged last tile
     "cxc_n64_acc": (64, 64, 2048, 3, 1, 1, 0, 1, 0, 1),    # one 64-wide tile per batch
+    "cxc_overwrite": (384, 256, 1024, 2, 1, 1, 0, 0, 0, 2),  # replaces C unread (cleared first under a K split)
+    "rxc_overwrite": (256, 320, 512, 2, 0, 1, 0, 0, 0, 2),   # ragged last tile
 }
 # (tile_n, stages, k_block, kdiv, persistent); k_block 0: per-product kernel, 32 / 64: one-load
-# kernel; persistent: the one-load kernel with one CTA per SM over a tile list and two TMEM
-# accumulators (the epilogue of one tile beside the MMAs of the next), BF16 piece outputs only
+# kernel; persistent 1: the one-load kernel with one CTA per SM over a tile list and two TMEM
+# accumulators (the epilogue of one tile beside the MMAs of the next), BF16 piece outputs only;
+# persistent 2: the CTA-pair one-load kernel (tcgen05.mma.cta_group::2, 256-row tiles over
+# two CTAs, each staging half of B), complex x complex products only
 INSTANCES = [(64, 4, 0, 1, 0), (64, 4, 0, 2, 0), (64, 4, 0, 4, 0), (64, 2, 0, 1, 0), (64, 2, 0, 2, 0), (128, 2, 0, 1, 0),
              (128, 3, 0, 1, 0), (128, 4, 0, 1, 0), (256, 2, 0, 1, 0), (256, 3, 0, 1, 0), (256, 2, 0, 2, 0),
              (128, 2, 32, 1, 0), (128, 3, 32, 1, 0), (128, 4, 32, 1, 0), (256, 2, 32, 1, 0), (256, 3, 32, 1, 0),
              (256, 2, 32, 2, 0), (128, 2, 64, 1, 0), (128, 3, 64, 1, 0),
-             (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 4, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1)]
+             (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 4, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1),
+             (256, 2, 32, 1, 2), (256, 3, 32, 1, 2), (256, 3, 32, 2, 2), (128, 2, 32, 1, 2), (128, 3, 32, 1, 2),
+             (128, 4, 32, 1, 2), (128, 2, 64, 1, 2)]
 
 
 @pytest.mark.parametrize("np_", [2, 3])
@@ -49,14 +55,16 @@ def test_split_gemm_instances(shape, np_):
         if rc == NEDY_ERR_ARG:  # instance absent or too large for shared memory
             continue
         assert rc == NEDY_OK, (shape, bn, st, bk, kd, ps, lib.nedy_last_error())
-        print(f"{shape} np={np_} {bn}/{st}/bk{bk}/k{kd}{'/persistent' if ps else ''}: {err.value:.3e}")
+        print(f"{shape} np={np_} {bn}/{st}/bk{bk}/k{kd}{['', '/persistent', '/pair'][ps]}: {err.value:.3e}")
         assert 0.0 < err.value < TOL[np_], (shape, np_, bn, st, bk, kd, ps, err.value)
         ran.append((bn, st, bk, kd, ps))
     assert len(ran) >= 3, ran
     if N > 64:
         assert any(bk for (_, _, bk, _, _) in ran), "no one-load instance ran"
         if op:  # the persistent kernel writes piece outputs
-            assert any(ps for (*_, ps) in ran), "no persistent instance ran"
+            assert any(ps == 1 for (*_, ps) in ran), "no persistent instance ran"
+        if ac and bc:  # CTA pairs for complex x complex products
+            assert any(ps == 2 for (*_, ps) in ran), "no CTA-pair instance ran"
 
 
 def test_split_gemm_check_rejects_missing_instance():
