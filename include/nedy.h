@@ -110,7 +110,8 @@ int nedy_sigma_chunk_plan(int nao, int naux, long long budget, int precision, in
  * per-product kernel or 32/64 for the one-load kernel, kdiv the K-split divisor, persistent
  * 1 the persistent one-load kernel (one CTA per SM over a tile list, two TMEM
  * accumulators; tile_n 128, out_pieces only), persistent 2 the CTA-pair one-load kernel
- * (clusters of two CTAs, 256-row tiles by tcgen05.mma.cta_group::2; complex x complex).  *rel_err = max |C - C_fp64| / max |C_fp64|; NEDY_ERR_ARG for
+ * (clusters of two CTAs, 256-row tiles by tcgen05.mma.cta_group::2; complex x complex),
+ * persistent 3 the persistent CTA-pair kernel (tile_n 128, out_pieces only).  *rel_err = max |C - C_fp64| / max |C_fp64|; NEDY_ERR_ARG for
  * an instance that does not exist or does not fit in shared memory. */
 int nedy_split_gemm_check(int device, int M, int N, int K, int nb, int a_cplx, int b_cplx, int conj_a, int conj_b,
                           int npieces, int out_pieces, int accumulate, int tile_n, int stages, int k_block, int kdiv,

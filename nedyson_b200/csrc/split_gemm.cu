@@ -941,6 +941,226 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   }
 }
 
+// Persistent CTA-pair kernel (BF16 piece outputs): clusters of two CTAs walk a static list of
+// 256 x BN pair tiles (cluster c takes tiles c, c + clusters, ...), each CTA with two TMEM
+// accumulators of its 128 rows, so the epilogue of one tile runs beside the MMAs of the next
+// as in the persistent kernel, while each CTA stages only its own A rows and half of B as in
+// the pair kernel.  Real x complex products (P.fuse): one MMA with N = 2 BN whose B rows are
+// the real plane tile (staged by rank 0) followed by the imaginary one (rank 1).
+// Barriers: full / empty per stage (rank 1's landings forwarded to rank 0's full barrier),
+// tfull per accumulator (multicast commit to both CTAs), tempty per accumulator on rank 0
+// with one arrival per epilogue warp of both CTAs (rank 1's remote).
+template <int BN, int STAGES, int BKT>
+__global__ void __launch_bounds__(P_THREADS, 1)
+    split_gemm_persist_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                                   const __grid_constant__ Params P, int ntn, int ntmp, int ntiles) {
+  static_assert(BN <= 128, "two accumulators of 2 BN TMEM columns must fit in 512 columns");
+  constexpr int A_TILE = BM * BKT * 2;
+  constexpr uint32_t TCOLS = 2 * BN;
+  constexpr uint32_t TALLOC = 2 * TCOLS;
+  constexpr uint32_t IDESC = idesc_bf16(2 * BM, BN);
+  constexpr uint32_t IDESC2 = idesc_bf16(2 * BM, 2 * BN);
+  extern __shared__ uint8_t sraw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)sraw + 1023) & ~(uintptr_t)1023);
+  uint8_t *epi = smem + STAGES * P.stage_bytes;
+  uint64_t *bar = (uint64_t *)(epi + P_EPI_BYTES);  // full[ST], empty[ST], tfull[2], tempty[2], done
+  uint32_t *tmem_slot = (uint32_t *)(bar + 2 * STAGES + 5);
+  __shared__ int s_skip, s_skip_pair;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = pr::cta_rank(), peer = rank ^ 1u, lead = rank & ~1u;
+  const bool leader = (rank & 1u) == 0;
+  const uint16_t mask = (uint16_t)(3u << lead);
+  // B rows this CTA stages per piece: fused, one plane tile of BN rows (rank r: plane r);
+  // else BN / 2 rows of every plane (rows n0 + r BN / 2)
+  const int brows = P.fuse ? BN : BN / 2;
+  const int b_bytes = brows * BKT * 2;
+  const uint32_t full0 = smem_u32(bar), empty0 = smem_u32(bar + STAGES), tfull0 = smem_u32(bar + 2 * STAGES),
+                 tempty0 = smem_u32(bar + 2 * STAGES + 2), done = smem_u32(bar + 2 * STAGES + 4);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(full0 + 8 * s, leader ? 2 : 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(tfull0 + 8 * i, 1);
+      mbar_init(tempty0 + 8 * i, 2 * P_EPI_WARPS);  // on rank 0: every epilogue warp of the pair
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_skip = *(volatile int *)P.err != 0;
+  }
+  if (warp == P_EPI_WARPS + 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TALLOC));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  pr::cluster_sync();
+  tc_fence_after();
+  if (threadIdx.x == 0) s_skip_pair = s_skip | pr::ld_cluster(pr::map_to(smem_u32(&s_skip), peer));
+  __syncthreads();
+  const uint32_t tmem = *tmem_slot;
+  const int cid = (int)(blockIdx.x >> 1), ncl = (int)(gridDim.x >> 1);
+  const int first = s_skip_pair ? ntiles : cid;
+  // pair tile t: column tile fastest, then pair of row tiles, then batch x K split
+  auto decode = [&](int t, int &n0, int &m0, int &b, int &kb0, int &nkb) {
+    const int nt = t % ntn, r = t / ntn, mp = r % ntmp, z = r / ntmp;
+    b = z / P.ksplit;
+    const int ks = z - b * P.ksplit;
+    n0 = nt * BN;
+    m0 = (2 * mp + (int)(rank & 1u)) * BM;
+    kb0 = ks * P.kb_per_split;
+    nkb = max(0, min(P.kblocks, kb0 + P.kb_per_split) - kb0);
+  };
+
+  if (warp == P_EPI_WARPS && lane == 0) {
+    // ---- TMA producer (both CTAs)
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    int g = 0;
+    bool stop = false;
+    for (int t = first; t < ntiles && !stop; t += ncl) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      const int ab = P.a_nb > 1 ? P.a_b0 + b : 0, bb = P.b_nb > 1 ? P.b_b0 + b : 0;
+      const int nb0 = P.fuse ? n0 : n0 + (int)(rank & 1u) * (BN / 2);
+      for (int it = 0; it < nkb; it++) {
+        const int s = g % STAGES;
+        const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+        if (g >= STAGES && !mbar_wait(empty0 + 8 * s, ph ^ 1u, P.err, 1)) {
+          stop = true;
+          break;
+        }
+        const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+        mbar_expect_tx(full0 + 8 * s, P.stage_bytes);
+        const int kb = kb0 + it;
+        const uint32_t bbase = base + P.np * P.nA * A_TILE;
+        for (int p = 0; p < P.np; p++) {
+          for (int i = 0; i < P.nA; i++)
+            tma_load_3d(base + (p * P.nA + i) * A_TILE, &tmA, full0 + 8 * s, kb * BKT, m0,
+                        (P.a_comp[i] * P.np + p) * P.a_nb + ab);
+          if (P.fuse) {
+            tma_load_3d(bbase + p * b_bytes, &tmB, full0 + 8 * s, kb * BKT, nb0,
+                        (P.b_comp[rank & 1u] * P.np + p) * P.b_nb + bb);
+          } else {
+            for (int j = 0; j < P.nB; j++)
+              tma_load_3d(bbase + (p * P.nB + j) * b_bytes, &tmB, full0 + 8 * s, kb * BKT, nb0,
+                          (P.b_comp[j] * P.np + p) * P.b_nb + bb);
+          }
+        }
+        g++;
+      }
+    }
+    for (int j = max(0, g - STAGES); j < g; j++)
+      mbar_wait_drain(full0 + 8 * (j % STAGES), (uint32_t)(j / STAGES) & 1u, P.err, 4);
+  } else if (warp == P_EPI_WARPS + 1 && lane == 0 && !leader) {
+    // ---- rank 1: forward each landed stage to rank 0
+    const uint32_t lfull0 = pr::map_to(full0, lead);
+    int g = 0;
+    bool stop = false;
+    for (int t = first; t < ntiles && !stop; t += ncl) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      for (int it = 0; it < nkb; it++, g++) {
+        const int s = g % STAGES;
+        if (!mbar_wait(full0 + 8 * s, (uint32_t)(g / STAGES) & 1u, P.err, 2)) {
+          stop = true;
+          break;
+        }
+        pr::arrive_remote(lfull0 + 8 * s);
+      }
+    }
+  } else if (warp == P_EPI_WARPS + 1 && lane == 0) {
+    // ---- rank 0: MMA issuer for the pair
+    int g = 0, lt = 0;
+    bool stop = false;
+    for (int t = first; t < ntiles && !stop; t += ncl, lt++) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      const int bi = lt & 1;
+      const uint32_t tacc = tmem + (uint32_t)bi * TCOLS;
+      if (lt >= 2 && !mbar_wait(tempty0 + 8 * bi, (uint32_t)((lt >> 1) - 1) & 1u, P.err, 5)) break;
+      tc_fence_after();
+      bool started0 = false, started1 = false;
+      for (int it = 0; it < nkb; it++) {
+        const int s = g % STAGES;
+        const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+        if (!mbar_wait(full0 + 8 * s, ph, P.err, 2)) {
+          stop = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t base = smem_u32(smem + s * P.stage_bytes);
+        const uint32_t bbase = base + P.np * P.nA * A_TILE;
+        for (int pr_ = 0; pr_ < P.nprod; pr_++) {
+          const int sa0 = P.pa[pr_] * P.nA;
+          if (P.fuse) {
+            const uint64_t da = op_desc<BKT>(base + sa0 * A_TILE);
+            const uint64_t db = op_desc<BKT>(bbase + P.pb[pr_] * b_bytes);
+#pragma unroll
+            for (int k = 0; k < BKT / 16; k++)
+              pr::mma2(tacc, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), IDESC2, (started0 || k > 0) ? 1u : 0u);
+            started0 = started1 = true;
+            continue;
+          }
+          const int sb0 = P.pb[pr_] * P.nB;
+          for (int q = 0; q < P.nmma; q++) {
+            const Mma mq = P.mma[q];
+            const uint64_t da = op_desc<BKT>(base + (sa0 + mq.sa) * A_TILE);
+            const uint64_t db = op_desc<BKT>(bbase + (sb0 + mq.sb) * b_bytes);
+            const uint32_t idesc = IDESC | (mq.neg ? (1u << 13) : 0u);
+            const uint32_t ta = tacc + (uint32_t)(mq.acc * BN);
+#pragma unroll
+            for (int k = 0; k < BKT / 16; k++)
+              pr::mma2(ta, da + (uint64_t)(2 * k), db + (uint64_t)(2 * k), idesc,
+                       ((mq.acc ? started1 : started0) || k > 0) ? 1u : 0u);
+            if (mq.acc)
+              started1 = true;
+            else
+              started0 = true;
+          }
+        }
+        pr::commit2(empty0 + 8 * s, mask);
+        g++;
+      }
+      if (stop) break;
+      pr::commit2(tfull0 + 8 * bi, mask);
+    }
+    // every MMA issued has finished before either CTA releases TMEM or shared memory
+    pr::commit2(done, mask);
+    mbar_wait_drain(done, 0, P.err, 3);
+  } else if (warp < P_EPI_WARPS) {
+    // ---- epilogue (both CTAs): this CTA's 128 rows of tile lt from accumulator lt & 1,
+    // then release the accumulator on rank 0
+    const int q = warp & 3, c_lo = (warp >> 2) * (BN / 2);
+    const uint32_t tempty_l = pr::map_to(tempty0, lead);
+    int lt = 0;
+    for (int t = first; t < ntiles; t += ncl, lt++) {
+      int n0, m0, b, kb0, nkb;
+      decode(t, n0, m0, b, kb0, nkb);
+      const int bi = lt & 1;
+      int okl = 0;
+      if (lane == 0) okl = mbar_wait(tfull0 + 8 * bi, (uint32_t)(lt >> 1) & 1u, P.err, 3) ? 1 : 0;
+      __syncwarp();
+      if (!__shfl_sync(0xffffffffu, okl, 0)) break;
+      tc_fence_after();
+      epilogue_tile<BN>(P, m0, n0, b, q, lane, tmem + (uint32_t)bi * TCOLS, nkb == 0, epi + warp * PIECE_WARP_BYTES,
+                        c_lo, c_lo + BN / 2);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) pr::arrive_remote(tempty_l + 8 * bi);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  pr::cluster_sync();  // neither CTA releases TMEM or exits while the other still works
+  if (warp == P_EPI_WARPS + 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TALLOC));
+  }
+}
+
 // ---------------------------------------------------------------------------------
 __global__ void split_pieces_kernel(int rows, int K, int kpad, int nb, int cplx, int np, const double *in, View v,
                                     double conj_sign, __nv_bfloat16 *out, i64 plane) {
@@ -1127,6 +1347,46 @@ void launch_persist(const Params &P, const CUtensorMap &ma, const CUtensorMap &m
   NEDY_CHECK_LAUNCH();
 }
 
+// persistent CTA-pair kernel: clusters of two CTAs (one per SM), at most one cluster per pair tile
+template <int BN, int STAGES, int BKT>
+void launch_persist_pair(const Params &P, const CUtensorMap &ma, const CUtensorMap &mb, dim3 grid, cudaStream_t s) {
+  static std::atomic<bool> attr[64];  // per device (host threads may race here)
+  static std::atomic<int> sms_of[64];
+  int dev = 0;
+  NEDY_CUDA(cudaGetDevice(&dev));
+  NEDY_REQUIRE(dev < 64, "device index out of range");
+  NEDY_REQUIRE(grid.y % 2 == 0, "split_gemm: the pair kernel needs an even number of row tiles");
+  NEDY_REQUIRE(STAGES * P.stage_bytes + P_EPI_BYTES <= P_SMEM_LIMIT, "split_gemm: stages exceed shared memory");
+  NEDY_REQUIRE(P.out_pieces, "split_gemm: the persistent kernels write BF16 piece outputs only");
+  if (!attr[dev].load()) {
+    int sms = 0;
+    NEDY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    sms_of[dev].store(sms);
+    NEDY_CUDA(cudaFuncSetAttribute(split_gemm_persist_pair_kernel<BN, STAGES, BKT>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_LIMIT + 1024 + 256));
+    attr[dev].store(true);
+  }
+  const int ntmp = (int)grid.y / 2;
+  const long long ntiles = (long long)grid.x * ntmp * grid.z;
+  NEDY_REQUIRE(ntiles < (1LL << 31), "split_gemm: too many tiles");
+  const int ncl = (int)std::min<long long>(ntiles, std::max(1, sms_of[dev].load() / 2));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * ncl);
+  cfg.blockDim = dim3(P_THREADS);
+  cfg.dynamicSmemBytes = (size_t)psmem_bytes(P.stage_bytes, STAGES);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  NEDY_CUDA(cudaLaunchKernelEx(&cfg, split_gemm_persist_pair_kernel<BN, STAGES, BKT>, ma, mb, P, (int)grid.x, ntmp,
+                               (int)ntiles));
+  NEDY_CHECK_LAUNCH();
+}
+
 // CTA-pair kernel: grid (column tiles, row tiles, z) of the other kernels launched as
 // (row tiles, column tiles, z), clusters of two consecutive row tiles along x (an even count)
 template <int BN, int STAGES, int BKT>
@@ -1246,6 +1506,9 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc, bool piece
         const int pst = std::min(bk == 32 ? 4 : 2, (P_SMEM_LIMIT - P_EPI_BYTES) / sb);
         if (pst >= 2) c.push_back({bn, pst, 1, bk, 1});
         if (pst >= 4) c.push_back({bn, 3, 1, bk, 1});
+        // persistent CTA pairs: each CTA stages half of B (instances: 3-4 stages of 32, 2-3 of 64)
+        const int ppst = std::min(bk == 32 ? 4 : 3, (P_SMEM_LIMIT - P_EPI_BYTES) / stage_bytes_for(nA, nB, np, bn, bk, 1));
+        if (ppst >= (bk == 32 ? 3 : 2)) c.push_back({bn, ppst, 1, bk, 1, 1});
       }
     }
   }
@@ -1321,7 +1584,7 @@ std::string split_tune_report() {
       char buf[96];
       char ol[16] = "";
       if (e.cands[i].bk)
-        snprintf(ol, sizeof(ol), "/ol%d%s", e.cands[i].bk, e.cands[i].persist ? "p" : e.cands[i].pair ? "x2" : "");
+        snprintf(ol, sizeof(ol), "/ol%d%s%s", e.cands[i].bk, e.cands[i].persist ? "p" : "", e.cands[i].pair ? "x2" : "");
       snprintf(buf, sizeof(buf), " %d/%d/k%d%s=%.1fus%s", e.cands[i].bn, e.cands[i].stages, e.cands[i].kdiv, ol,
                e.trials[i] ? e.best[i] * 1e3 : -1.0, (int)i == e.chosen ? "*" : "");
       r += buf;
@@ -1404,8 +1667,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
     NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && g.force_bn == 128 && g.out_pieces),
                  "split_gemm: the persistent kernel is the one-load kernel with 128-wide tiles and piece outputs");
-    NEDY_REQUIRE(!g.force_pair || (g.force_bk != 0 && !g.force_persist && ac && bc),
-                 "split_gemm: the pair kernel is a one-load kernel for complex x complex products");
+    NEDY_REQUIRE(!g.force_pair || (g.force_bk != 0 && (g.force_persist ? g.out_pieces : (ac && bc))),
+                 "split_gemm: the pair kernels are one-load kernels (complex x complex, or persistent with piece outputs)");
     BNsel = g.force_bn;
     STsel = g.force_stages;
     KDsel = g.force_kdiv;
@@ -1450,7 +1713,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   const int bkt = BKsel ? BKsel : BK;
   P.stage_bytes = stage_bytes_for(P.nA, P.nB, P.np, BNsel, BKsel, PRsel);
   // real x complex without conjugation: one N = 2 BN product writes both parts
-  P.fuse = (BKsel && !PRsel && !ac && bc && !g.conjB && 2 * BNsel <= 256) ? 1 : 0;
+  P.fuse = (BKsel && !(PRsel && !PSsel) && !ac && bc && !g.conjB && 2 * BNsel <= 256) ? 1 : 0;
   P.kblocks = g.A.kpad / 64;  // 64-wide blocks while the K split is chosen
   // row tiles: an even number for CTA pairs (the rows of a last odd tile are out of range:
   // loaded as zeros, not stored)
@@ -1497,7 +1760,9 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   P.cdiv = g.C.cdiv;
   P.bs = g.C.bs1;
   P.err = err_word(s);
-  const CUtensorMap ma = make_map(g.A, BM, bkt), mb = make_map(g.B, PRsel ? BNsel / 2 : BNsel, bkt);
+  // B rows per CTA: half of a tile in CTA pairs, except a fused real x complex product, where
+  // each CTA of the pair stages one whole plane tile
+  const CUtensorMap ma = make_map(g.A, BM, bkt), mb = make_map(g.B, PRsel && !P.fuse ? BNsel / 2 : BNsel, bkt);
   dim3 grid(ntn, ntm, g.nb * ksplit);
   cudaEvent_t ev[2] = {nullptr, nullptr};
   {
@@ -1539,7 +1804,9 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       {32, 256, 2, launch_pair<256, 2, 32>, 0, 1}, {32, 256, 3, launch_pair<256, 3, 32>, 0, 1},
       {32, 128, 2, launch_pair<128, 2, 32>, 0, 1}, {32, 128, 3, launch_pair<128, 3, 32>, 0, 1},
       {32, 128, 4, launch_pair<128, 4, 32>, 0, 1},
-      {64, 128, 2, launch_pair<128, 2, 64>, 0, 1}};
+      {64, 128, 2, launch_pair<128, 2, 64>, 0, 1},
+      {32, 128, 3, launch_persist_pair<128, 3, 32>, 1, 1}, {32, 128, 4, launch_persist_pair<128, 4, 32>, 1, 1},
+      {64, 128, 2, launch_persist_pair<128, 2, 64>, 1, 1}, {64, 128, 3, launch_persist_pair<128, 3, 64>, 1, 1}};
   int st_run = stages;
   if (BKsel == 0) {  // per-product kernel: the instance nearest to the requested stages
     st_run = BNsel == 64 ? (stages <= 2 ? 2 : 4)
@@ -1678,8 +1945,8 @@ double split_gemm_check(const SplitCheck &k, cudaStream_t s) {
     g.conjA = k.conjA != 0; g.conjB = k.conjB != 0;
     g.alpha = k.alpha;
     g.force_bn = k.bn; g.force_stages = k.stages; g.force_bk = k.bk; g.force_kdiv = k.kdiv;
-    g.force_persist = k.persist == 1;
-    g.force_pair = k.persist == 2;
+    g.force_persist = k.persist == 1 || k.persist == 3;
+    g.force_pair = k.persist == 2 || k.persist == 3;
     double2 *got = C;
     if (k.out_pieces) {
       Pieces cp;

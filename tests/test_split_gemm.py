@@ -32,14 +32,17 @@ SHAPES = {
 # kernel; persistent 1: the one-load kernel with one CTA per SM over a tile list and two TMEM
 # accumulators (the epilogue of one tile beside the MMAs of the next), BF16 piece outputs only;
 # persistent 2: the CTA-pair one-load kernel (tcgen05.mma.cta_group::2, 256-row tiles over
-# two CTAs, each staging half of B), complex x complex products only
+# two CTAs, each staging half of B), complex x complex products only; persistent 3: the
+# persistent CTA-pair kernel (clusters of two over a tile list, two accumulators per CTA),
+# BF16 piece outputs only
 INSTANCES = [(64, 4, 0, 1, 0), (64, 4, 0, 2, 0), (64, 4, 0, 4, 0), (64, 2, 0, 1, 0), (64, 2, 0, 2, 0), (128, 2, 0, 1, 0),
              (128, 3, 0, 1, 0), (128, 4, 0, 1, 0), (256, 2, 0, 1, 0), (256, 3, 0, 1, 0), (256, 2, 0, 2, 0),
              (128, 2, 32, 1, 0), (128, 3, 32, 1, 0), (128, 4, 32, 1, 0), (256, 2, 32, 1, 0), (256, 3, 32, 1, 0),
              (256, 2, 32, 2, 0), (128, 2, 64, 1, 0), (128, 3, 64, 1, 0),
              (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 4, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1),
              (256, 2, 32, 1, 2), (256, 3, 32, 1, 2), (256, 3, 32, 2, 2), (128, 2, 32, 1, 2), (128, 3, 32, 1, 2),
-             (128, 4, 32, 1, 2), (128, 2, 64, 1, 2)]
+             (128, 4, 32, 1, 2), (128, 2, 64, 1, 2),
+             (128, 3, 32, 1, 3), (128, 4, 32, 1, 3), (128, 2, 64, 1, 3), (128, 3, 64, 1, 3)]
 
 
 @pytest.mark.parametrize("np_", [2, 3])
@@ -55,14 +58,15 @@ def test_split_gemm_instances(shape, np_):
         if rc == NEDY_ERR_ARG:  # instance absent or too large for shared memory
             continue
         assert rc == NEDY_OK, (shape, bn, st, bk, kd, ps, lib.nedy_last_error())
-        print(f"{shape} np={np_} {bn}/{st}/bk{bk}/k{kd}{['', '/persistent', '/pair'][ps]}: {err.value:.3e}")
+        print(f"{shape} np={np_} {bn}/{st}/bk{bk}/k{kd}{['', '/persistent', '/pair', '/persistent-pair'][ps]}: {err.value:.3e}")
         assert 0.0 < err.value < TOL[np_], (shape, np_, bn, st, bk, kd, ps, err.value)
         ran.append((bn, st, bk, kd, ps))
     assert len(ran) >= 3, ran
     if N > 64:
         assert any(bk for (_, _, bk, _, _) in ran), "no one-load instance ran"
-        if op:  # the persistent kernel writes piece outputs
+        if op:  # the persistent kernels write piece outputs
             assert any(ps == 1 for (*_, ps) in ran), "no persistent instance ran"
+            assert any(ps == 3 for (*_, ps) in ran), "no persistent CTA-pair instance ran"
         if ac and bc:  # CTA pairs for complex x complex products
             assert any(ps == 2 for (*_, ps) in ran), "no CTA-pair instance ran"
 
