@@ -93,6 +93,7 @@ Ctx::~Ctx() {
   auto f = [](void *p) { if (p) cudaFree(p); };
   f(Vija); f(Viaj); f(Vaij); f(Vmbq); f(Vp); f(Vanj_p); f(Vjkb_p); f(Vila_p); f(rowcopy); f(d_maxdiff); f(pred_corr); f(U); f(Uexch); f(mixK); f(mixK_alt); f(Minv); f(greg); f(small);
   if (stream) cudaStreamDestroy(stream);
+  delete aux;
 }
 
 // full-U Hartree-Fock (molHFSolver.cpp:35-56): hmf_ij += sum_kl rho_kl (2 U_ijkl - U_ilkj)
@@ -931,10 +932,14 @@ void step_tol(nedy_ctx *ctx, int tstp, int nspin, nedy_gf *const *G, nedy_gf *co
     sigma_df(c, tstp, nspin, Ss, Gs);
     pt.mark(3);
     double d = 0.0;
-    for (int s = 0; s < nspin; s++) {
-      double e[3] = {0, 0, 0};
-      dyson_step(c, tstp, G[s]->g, S[s]->g, (const double2 *)hmf[s]->p, mu[s], e);
-      d = std::max(d, row_change(c, G[s]->g, tstp, s));
+    {
+      double e[2][3] = {{0, 0, 0}, {0, 0, 0}};
+      if (nspin == 2)
+        dyson_step_spins(c, tstp, G[0]->g, S[0]->g, (const double2 *)hmf[0]->p, mu[0], e[0], G[1]->g, S[1]->g,
+                         (const double2 *)hmf[1]->p, mu[1], e[1]);
+      else
+        dyson_step(c, tstp, G[0]->g, S[0]->g, (const double2 *)hmf[0]->p, mu[0], e[0]);
+      for (int s = 0; s < nspin; s++) d = std::max(d, row_change(c, G[s]->g, tstp, s));
     }
     if (err_hist) err_hist[it] = d;
     if (learned && it == 0) {
@@ -1226,8 +1231,8 @@ int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *Gu, nedy_gf *Gd, ned
       pt.mark(2);
       sigma_df(c, tstp, 2, Ss, Gs);
       pt.mark(3);
-      dyson_step(c, tstp, Gu->g, Su->g, (const double2 *)hu->p, mu_up, eu);
-      dyson_step(c, tstp, Gd->g, Sd->g, (const double2 *)hd->p, mu_dn, ed);
+      dyson_step_spins(c, tstp, Gu->g, Su->g, (const double2 *)hu->p, mu_up, eu, Gd->g, Sd->g,
+                       (const double2 *)hd->p, mu_dn, ed);
     }
     pt.mark(-1);
     NEDY_CUDA(cudaStreamSynchronize(c.stream));

@@ -15,6 +15,8 @@
 // change, so each step is a single block product instead of an LU solve.
 #include "sigma.cuh"
 #include <cooperative_groups.h>
+#include <exception>
+#include <thread>
 #include <atomic>
 #include <cmath>
 #include <algorithm>
@@ -1577,6 +1579,93 @@ void dyson_step(Ctx &c, int n, DevGF &G, const DevGF &Sig, const double2 *hmf, d
   double e3 = dyson_les(c, n, G, Sig, hmf, mu);
   check_status(c);
   if (err) { err[0] = e1; err[1] = e2; err[2] = e3; }
+}
+
+// Second context of c, created on first use: the same sizes, weights and collocation, its
+// own stream (ordered after c's by events), workspace, inverses and mixing kernel.
+static Ctx &aux_ctx(Ctx &c) {
+  if (!c.aux) {
+    Ctx *a = new Ctx;
+    a->device = c.device;
+    a->nt = c.nt; a->ntau = c.ntau; a->nao = c.nao; a->k = c.k;
+    a->beta = c.beta; a->dt = c.dt;
+    a->ws_budget = c.ws_budget;
+    a->W = c.W;
+    a->col = c.col;
+    const cudaError_t e = cudaStreamCreate(&a->stream);
+    if (e != cudaSuccess) {
+      delete a;
+      NEDY_CUDA(e);
+    }
+    a->ws.set_stream(a->stream);
+    c.aux = a;
+  }
+  return *c.aux;
+}
+
+// A mixing kernel that `from` holds for G's G^M moves to `to` (no second 16 ntau^2 nao^2
+// bytes for the same kernel).  Work already queued on from's stream that reads it comes
+// before to's stream by the event order of the caller.
+static void hand_over_mixing_kernel(Ctx &from, Ctx &to, const DevGF &G) {
+  const int N = G.nao;
+  if (to.mixK && to.mixK_src == G.mat && to.mixK_ver == G.mat_version && to.mixK_nao == N) return;
+  double2 **p = nullptr;
+  const double2 **src = nullptr;
+  unsigned long long *ver = nullptr;
+  int *nao = nullptr;
+  if (from.mixK && from.mixK_src == G.mat && from.mixK_ver == G.mat_version && from.mixK_nao == N) {
+    p = &from.mixK; src = &from.mixK_src; ver = &from.mixK_ver; nao = &from.mixK_nao;
+  } else if (from.mixK_alt && from.mixK_alt_src == G.mat && from.mixK_alt_ver == G.mat_version &&
+             from.mixK_alt_nao == N) {
+    p = &from.mixK_alt; src = &from.mixK_alt_src; ver = &from.mixK_alt_ver; nao = &from.mixK_alt_nao;
+  }
+  if (!p) return;
+  if (to.mixK) NEDY_CUDA(cudaFree(to.mixK));
+  to.mixK = *p; to.mixK_src = *src; to.mixK_ver = *ver; to.mixK_nao = *nao;
+  *p = nullptr; *src = nullptr; *ver = ~0ULL; *nao = 0;
+}
+
+void dyson_step_spins(Ctx &c, int n, DevGF &G0, const DevGF &S0, const double2 *h0, double mu0, double *e0,
+                      DevGF &G1, const DevGF &S1, const double2 *h1, double mu1, double *e1) {
+  // The two steps are independent; each is a chain of small dependent kernels (sequential
+  // sweeps, the pivot steps of the start blocks) with host round trips, which leaves most
+  // of the GPU idle, so they run side by side.
+  Ctx &a = aux_ctx(c);
+  hand_over_mixing_kernel(c, a, G1);
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  NEDY_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  const cudaError_t ce = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    NEDY_CUDA(ce);
+  }
+  std::exception_ptr ex0, ex1;
+  try {
+    NEDY_CUDA(cudaEventRecord(ev[0], c.stream));  // a's stream after everything queued on c's
+    NEDY_CUDA(cudaStreamWaitEvent(a.stream, ev[0], 0));
+    std::thread th([&] {
+      try {
+        NEDY_CUDA(cudaSetDevice(a.device));
+        dyson_step(a, n, G1, S1, h1, mu1, e1);
+      } catch (...) {
+        ex1 = std::current_exception();
+      }
+    });
+    try {
+      dyson_step(c, n, G0, S0, h0, mu0, e0);
+    } catch (...) {
+      ex0 = std::current_exception();
+    }
+    th.join();
+    NEDY_CUDA(cudaEventRecord(ev[1], a.stream));  // c's stream continues after spin 1's step
+    NEDY_CUDA(cudaStreamWaitEvent(c.stream, ev[1], 0));
+  } catch (...) {
+    if (!ex0) ex0 = std::current_exception();
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (ex0) std::rethrow_exception(ex0);
+  if (ex1) std::rethrow_exception(ex1);
 }
 
 } // namespace nedy

@@ -147,6 +147,9 @@ struct Ctx {
   // device time per phase of the whole-step entry points (ms): predictor, mean field, self-energy, Dyson
   bool timing = false;
   double phase_ms[4] = {0, 0, 0, 0};
+  // second context (own stream, workspace, inverses, mixing kernel; owned) on which the
+  // unrestricted whole steps run the second spin's Dyson step beside the first's
+  Ctx *aux = nullptr;
   ~Ctx();
 };
 

@@ -28,6 +28,11 @@ void ensure_tables(Ctx &c);
 // dyson::dyson_step (dyson_step.h:329-382); hmf: (nt+1) x nao x nao on the device.
 // Returns the sum of the three component errors (ret, tv, les) when err != nullptr.
 void dyson_step(Ctx &c, int n, DevGF &G, const DevGF &Sig, const double2 *hmf, double mu, double *err);
+// The Dyson steps of both spins of an unrestricted step, side by side: spin 0 on c's stream,
+// spin 1 on the stream of c's second context from a helper thread; c's stream continues
+// after both.
+void dyson_step_spins(Ctx &c, int n, DevGF &G0, const DevGF &S0, const double2 *h0, double mu0, double *e0,
+                      DevGF &G1, const DevGF &S1, const double2 *h1, double mu1, double *e1);
 // dyson::dyson_start (dyson_boot.h:195-230)
 double dyson_start(Ctx &c, DevGF &G, const DevGF &Sig, const double2 *hmf, double mu);
 // dyson::energy_conv (dyson_integrals.h:24-70)
