@@ -89,6 +89,9 @@ def parse():
     ap.add_argument("--window", type=int, default=0,
                     help="keep only the last W time steps of G^R and G^< on the device (Sigma whole); "
                          "with --state synthetic the history is built on the device")
+    ap.add_argument("--sigma-host", action="store_true",
+                    help="Sigma's two triangles in pinned host memory (nedy_gf_create_host_history), read by "
+                         "the kernels over the host link; with --window, runs whose history exceeds the device")
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--tight-tol", type=float, default=1e-10,
                     help="tolerance of the predictor ablation forms (0: skip them)")
@@ -437,12 +440,18 @@ def fill_synthetic_windowed(G, S, t_first, ntau, x, mu, F, beta, dt, window):
     for comp in (LES, RET, TV):
         check(lib().nedy_gf_device_pointer(S.h, comp, C.byref(ptr)))
         views[comp] = ptr.value
-    Sret = _dev_view(views[RET], (ntri, N, N), torch)
-    Sles = _dev_view(views[LES], (ntri, N, N), torch)
-    for t in range(t_first):
-        o = t * (t + 1) // 2
-        Sret[o:o + t + 1] = 0.02 * Eret[:t + 1].flip(0)
-        Sles[o:o + t + 1] = 0.02 * Eles[:t + 1].flip(0)
+    if S.host_history:  # Sigma's triangles in host memory: written through the row API
+        for t in range(t_first):
+            o = t * (t + 1) // 2
+            S.upload(RET, o, (0.02 * Eret[:t + 1].flip(0)).cpu().numpy())
+            S.upload(LES, o, (0.02 * Eles[:t + 1].flip(0)).cpu().numpy())
+    else:
+        Sret = _dev_view(views[RET], (ntri, N, N), torch)
+        Sles = _dev_view(views[LES], (ntri, N, N), torch)
+        for t in range(t_first):
+            o = t * (t + 1) // 2
+            Sret[o:o + t + 1] = 0.02 * Eret[:t + 1].flip(0)
+            Sles[o:o + t + 1] = 0.02 * Eles[:t + 1].flip(0)
     check(lib().nedy_gf_device_pointer(G.h, TV, C.byref(ptr)))
     Gtv = _dev_view(ptr.value, (t_first, ntau + 1, N, N), torch)
     Stv = _dev_view(views[TV], (t_first, ntau + 1, N, N), torch)
@@ -498,7 +507,7 @@ def run_engine(args, dist: Dist):
                       workspace_bytes=int(args.workspace_gb * (1 << 30)))
     x, _ = ctx.collocation()
     G = [api.green_func(ctx, nt, ntau, N, -1, window=args.window) for _ in range(ns)]
-    S = [api.green_func(ctx, nt, ntau, N, -1) for _ in range(ns)]
+    S = [api.green_func(ctx, nt, ntau, N, -1, host_history=args.sigma_host) for _ in range(ns)]
     solver = (api.molGF2SolverSpinDecomp if spin else api.molGF2SolverDecomp)(ctx, p.Vija)
     kk = 5
     traj = args.state == "trajectory"
@@ -580,6 +589,7 @@ def run_engine(args, dist: Dist):
             hmf.append(api.hmf_buffer(ctx, N, hm))
         torch.cuda.synchronize(dev)
         prep = {"state": "synthetic free propagation built on the device", "window": args.window,
+                "sigma_history": "pinned host memory" if args.sigma_host else "device",
                 "device_memory_used_gb": (lambda fr: (fr[1] - fr[0]) / 1e9)(torch.cuda.mem_get_info(dev))}
     else:
         for s in range(ns):
@@ -904,6 +914,10 @@ def main():
            "t_window": [args.t0 + W, args.t0 + W + K - 1], "corr_steps": args.corr,
            "l2": "inputs (G, Sigma histories, GBs) larger than L2; no flush needed",
            "parallelism": f"replicas x{dist.world}"}
+    if args.window:
+        cfg["g_window"] = args.window
+    if args.sigma_host:
+        cfg["sigma_history"] = "pinned host memory, read by the kernels over the host link"
     T_ref = args.t0 + W  # the first step of the window
     if args.impl == "reference":
         if dist.rank != 0:

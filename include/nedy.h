@@ -147,6 +147,16 @@ int nedy_gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **
  * of the lesser / retarded components must then lie in one row (column). */
 #define NEDY_GF_MIN_WINDOW 12
 int nedy_gf_create_windowed(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int window, nedy_gf **out);
+/* The same as nedy_gf_create with the lesser and retarded triangles in pinned host memory
+ * mapped into the device's address space (no reference counterpart: the reference holds
+ * every triangle in host memory, src/greens.cpp:44-45, and runs on the host).  For Sigma of
+ * runs whose two-time history exceeds the device: the kernels read and write it in place
+ * over the host link, so a Dyson step, which reads both of Sigma's triangles whole, then
+ * moves them across that link every step.  G^tv and G^M stay on the device; transfers and
+ * every entry point take it like any green_func. */
+int nedy_gf_create_host_history(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out);
+/* *host = 1 when the lesser and retarded triangles of g live in mapped host memory */
+int nedy_gf_host_history(const nedy_gf *g, int *host);
 int nedy_gf_window(const nedy_gf *g, int *window);
 /* Waits for the device; may be called before or after nedy_ctx_destroy of its context
  * (every other call on the handle needs a live context). */

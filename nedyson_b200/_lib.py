@@ -54,6 +54,8 @@ SIGNATURES = {
     "nedy_gf_create": ([_P, _I, _I, _I, _I, _PP], _I),
     "nedy_gf_create_windowed": ([_P, _I, _I, _I, _I, _I, _PP], _I),
     "nedy_gf_window": ([_P, C.POINTER(C.c_int)], _I),
+    "nedy_gf_create_host_history": ([_P, _I, _I, _I, _I, _PP], _I),
+    "nedy_gf_host_history": ([_P, C.POINTER(C.c_int)], _I),
     "nedy_gf_destroy": ([_P], _I),
     "nedy_gf_upload": ([_P, _I, _LL, _LL, _P], _I),
     "nedy_gf_download": ([_P, _I, _LL, _LL, _P], _I),

@@ -80,13 +80,20 @@ class Context:
 class green_func:
     """Device-resident contour Green's function (green_func, reference src/greens.h:17-112)."""
 
-    def __init__(self, ctx: Context, nt, ntau, nao, sig=-1, window: int = 0):
+    def __init__(self, ctx: Context, nt, ntau, nao, sig=-1, window: int = 0, host_history: bool = False):
         """window > 0: only the last `window` time steps of G^R and G^< on the device
-        (nedy_gf_create_windowed); rows are then read and written one time step at a time."""
+        (nedy_gf_create_windowed); rows are then read and written one time step at a time.
+        host_history: the lesser and retarded triangles in pinned host memory that the kernels
+        read over the host link (nedy_gf_create_host_history; for a Sigma whose history exceeds
+        the device)."""
         self.ctx = ctx
         self.nt, self.ntau, self.nao, self.sig = int(nt), int(ntau), int(nao), int(sig)
         h = C.c_void_p()
-        if window:
+        if host_history:
+            if window:
+                raise ValueError("green_func: a host-resident history is not windowed")
+            check(lib().nedy_gf_create_host_history(ctx.h, self.nt, self.ntau, self.nao, self.sig, C.byref(h)))
+        elif window:
             check(lib().nedy_gf_create_windowed(ctx.h, self.nt, self.ntau, self.nao, self.sig, int(window),
                                                 C.byref(h)))
         else:
@@ -95,6 +102,8 @@ class green_func:
         w = C.c_int()
         check(lib().nedy_gf_window(h, C.byref(w)))
         self.window = w.value
+        check(lib().nedy_gf_host_history(h, C.byref(w)))
+        self.host_history = bool(w.value)
 
     def close(self):
         if getattr(self, "h", None):

@@ -155,7 +155,7 @@ static void save_row(Ctx &c, const DevGF &g, int T, int slot = 0) {
   }
   i64 o = slot * tot;
   for (int k = 0; k < 3; k++) {
-    NEDY_CUDA(cudaMemcpyAsync(c.rowcopy + o, r.p[k], sizeof(double2) * r.n[k], cudaMemcpyDeviceToDevice, c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(c.rowcopy + o, r.p[k], sizeof(double2) * r.n[k], cudaMemcpyDefault, c.stream));
     o += r.n[k];
   }
 }
@@ -419,7 +419,8 @@ int nedy_collocation_nodes(const nedy_ctx *ctx, double *x, double *w) {
   });
 }
 
-static int gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int window, nedy_gf **out) {
+static int gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int window, nedy_gf **out,
+                     bool host_tri = false) {
   return guard([&] {
     NEDY_REQUIRE(ctx && out, "null argument");
     NEDY_REQUIRE(nao > 0 && nt >= -1 && ntau >= 0 && sig * sig == 1, "green_func: bad sizes (greens.cpp:35)");
@@ -432,6 +433,27 @@ static int gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int wind
     DevGF &d = g->g;
     d.nt = nt; d.ntau = ntau; d.nao = nao; d.sig = sig; d.es = (i64)nao * nao;
     d.win = window > nt ? 0 : window;  // a window as long as the run is the full triangle
+    g->host_tri = host_tri;
+    // triangle in pinned host memory mapped into the device's address space (unified
+    // addressing: the device pointer is the host pointer); cleared by the device
+    auto alloc_host = [&](double2 *&p, i64 nblk) {
+      if (nblk <= 0) { p = nullptr; return; }
+      void *h = nullptr;
+      cudaError_t e = cudaHostAlloc(&h, sizeof(double2) * nblk * d.es, cudaHostAllocMapped | cudaHostAllocPortable);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(std::string("green_func host history allocation failed: ") + cudaGetErrorString(e));
+      }
+      void *dp = nullptr;
+      e = cudaHostGetDevicePointer(&dp, h, 0);
+      if (e != cudaSuccess || dp != h) {
+        cudaGetLastError();
+        cudaFreeHost(h);
+        throw CudaError("green_func host history: the mapped pointer differs from the host pointer (no unified addressing)");
+      }
+      p = (double2 *)dp;
+      memset_sync(p, sizeof(double2) * nblk * d.es, ctx->c.stream);
+    };
     auto alloc = [&](double2 *&p, i64 nblk) {
       if (nblk <= 0) { p = nullptr; return; }
       cudaError_t e = cudaMalloc(&p, sizeof(double2) * nblk * d.es);
@@ -445,14 +467,20 @@ static int gf_create(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, int wind
     try {
       alloc(d.mat, ntau + 1);
       if (nt >= 0) {
-        alloc(d.les, d.nstore());
-        alloc(d.ret, d.nstore());
+        if (host_tri) {
+          alloc_host(d.les, d.nstore());
+          alloc_host(d.ret, d.nstore());
+        } else {
+          alloc(d.les, d.nstore());
+          alloc(d.ret, d.nstore());
+        }
         alloc(d.tv, (i64)(nt + 1) * (ntau + 1));
       }
     } catch (...) {
+      auto tri_free = [&](double2 *p) { if (p) { if (host_tri) cudaFreeHost(p); else cudaFree(p); } };
       if (d.mat) cudaFree(d.mat);
-      if (d.les) cudaFree(d.les);
-      if (d.ret) cudaFree(d.ret);
+      tri_free(d.les);
+      tri_free(d.ret);
       if (d.tv) cudaFree(d.tv);
       delete g;
       throw;
@@ -469,6 +497,17 @@ int nedy_gf_create_windowed(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, i
   return gf_create(ctx, nt, ntau, nao, sig, window, out);
 }
 
+int nedy_gf_create_host_history(nedy_ctx *ctx, int nt, int ntau, int nao, int sig, nedy_gf **out) {
+  return gf_create(ctx, nt, ntau, nao, sig, 0, out, true);
+}
+
+int nedy_gf_host_history(const nedy_gf *g, int *host) {
+  return guard([&] {
+    NEDY_REQUIRE(g && host, "null argument");
+    *host = g->host_tri ? 1 : 0;
+  });
+}
+
 int nedy_gf_window(const nedy_gf *g, int *window) {
   return guard([&] {
     NEDY_REQUIRE(g && window, "null argument");
@@ -482,8 +521,13 @@ int nedy_gf_destroy(nedy_gf *g) {
     // cudaFree waits for the device; the context may already be gone
     cudaSetDevice(g->device);
     if (g->g.mat) cudaFree(g->g.mat);
-    if (g->g.les) cudaFree(g->g.les);
-    if (g->g.ret) cudaFree(g->g.ret);
+    if (g->host_tri) {
+      if (g->g.les) cudaFreeHost(g->g.les);
+      if (g->g.ret) cudaFreeHost(g->g.ret);
+    } else {
+      if (g->g.les) cudaFree(g->g.les);
+      if (g->g.ret) cudaFree(g->g.ret);
+    }
     if (g->g.tv) cudaFree(g->g.tv);
     delete g;
   });
@@ -516,7 +560,7 @@ int nedy_gf_upload(nedy_gf *g, int comp, long long first, long long nb, const vo
     set_dev(g->ctx);
     NEDY_REQUIRE(first >= 0 && nb >= 0, "block range out of bounds");
     double2 *dst = range_ptr(g, comp, first, nb);
-    NEDY_CUDA(cudaMemcpyAsync(dst, host, sizeof(double2) * nb * g->g.es, cudaMemcpyHostToDevice, g->ctx->c.stream));
+    NEDY_CUDA(cudaMemcpyAsync(dst, host, sizeof(double2) * nb * g->g.es, cudaMemcpyDefault, g->ctx->c.stream));
     NEDY_CUDA(cudaStreamSynchronize(g->ctx->c.stream));
     if (comp == NEDY_MAT) g->g.mat_version++;
   });
@@ -528,7 +572,7 @@ int nedy_gf_download(const nedy_gf *g, int comp, long long first, long long nb, 
     set_dev(g->ctx);
     NEDY_REQUIRE(first >= 0 && nb >= 0, "block range out of bounds");
     const double2 *src = range_ptr(g, comp, first, nb);
-    NEDY_CUDA(cudaMemcpyAsync(host, src, sizeof(double2) * nb * g->g.es, cudaMemcpyDeviceToHost,
+    NEDY_CUDA(cudaMemcpyAsync(host, src, sizeof(double2) * nb * g->g.es, cudaMemcpyDefault,
                               g->ctx->c.stream));
     NEDY_CUDA(cudaStreamSynchronize(g->ctx->c.stream));
   });

@@ -1558,7 +1558,7 @@ static double dyson_les(Ctx &c, int n, DevGF &G, const DevGF &S, const double2 *
   }
   diffnorm_kernel<<<nblk((i64)(n + 1) * es), TPB, 0, c.stream>>>(N, n + 1, G.lesptr(0, n), X, err);
   NEDY_CHECK_LAUNCH();
-  NEDY_CUDA(cudaMemcpyAsync(G.lesptr(1, n), X + es, sizeof(double2) * n * es, cudaMemcpyDeviceToDevice, c.stream));
+  NEDY_CUDA(cudaMemcpyAsync(G.lesptr(1, n), X + es, sizeof(double2) * n * es, cudaMemcpyDefault, c.stream));
   return sum_dev(c, err, n + 2, true);
 }
 

@@ -14,6 +14,7 @@ struct nedy_gf {
   nedy_ctx *ctx;
   int device;
   nedy::DevGF g;
+  bool host_tri = false;  // les / ret in mapped pinned host memory (cudaFreeHost)
 };
 struct nedy_buf {
   nedy_ctx *ctx;

@@ -23,10 +23,12 @@ from .inputs import Problem, drive, g0_from_h0, hf_equilibrium, uhf_equilibrium
 class DecompSimulation:
     def __init__(self, p: Problem, nt: int, ntau: int, beta: float, dt: float, k: int = 5,
                  corr_steps: int = 5, drive_kind: str = "none", drive_kw: dict | None = None, device: int = 0,
-                 workspace_bytes: int = 0, g_window: int = 0):
+                 workspace_bytes: int = 0, g_window: int = 0, sigma_host: bool = False):
         """g_window > 0: G keeps only the last g_window time steps of G^R and G^< on the
         device (Sigma keeps its whole history); read each finished row with G.ret_row(t) /
-        G.les_col(t) while it is in the window."""
+        G.les_col(t) while it is in the window.  sigma_host: Sigma's two triangles in pinned
+        host memory read by the kernels over the host link (runs whose history exceeds the
+        device)."""
         self.p, self.nt, self.ntau, self.beta, self.dt, self.k = p, nt, ntau, beta, dt, k
         self.corr_steps = corr_steps
         self.drive_kind, self.drive_kw = drive_kind, dict(drive_kw or {})
@@ -34,7 +36,7 @@ class DecompSimulation:
         self.x, self.w = self.ctx.collocation()
         N = p.nao
         self.G = api.green_func(self.ctx, nt, ntau, N, -1, window=g_window)
-        self.Sigma = api.green_func(self.ctx, nt, ntau, N, -1)
+        self.Sigma = api.green_func(self.ctx, nt, ntau, N, -1, host_history=sigma_host)
         self.solver = api.molGF2SolverDecomp(self.ctx, p.Vija)
         self.dyson = api.dyson(self.ctx)
         self.hmf = api.hmf_buffer(self.ctx, N)
