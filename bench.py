@@ -777,19 +777,31 @@ def run_batch(args, dist: Dist):
     import torch
     from nedyson_b200._lib import PREC_SPLIT_BF16X2
     from nedyson_b200.simulation import BatchSimulation, batch_problems
+    import ctypes as C
+    from nedyson_b200._lib import check, lib
     n, Kb, Wb = args.batch, args.batch_steps, 2
     t_first = 6 + 2
-    nt = t_first + Wb + Kb
+    W_max = 24  # warm-up steps at most: the autotuner times the candidates of every instance's classes
+    nt = t_first + W_max + Kb
     probs = batch_problems(n, seed=rank_seed(args.seed + 1000, dist.rank))
     tp = time.time()
     b = BatchSimulation(probs, nt, 128, 10.0, 0.02, k=5, corr_steps=5, workers=16, workspace_bytes=1 << 30,
                         device=dist.local, precision=PREC_SPLIT_BF16X2)
     b.boot(max_iter=20)
-    for t in range(6, t_first + Wb):
+    pending = C.c_int(0)
+    t = 6
+    # warm up until every problem class has chosen its tile shape (a run of nt=500 steps spends
+    # its first few steps there), then time steady-state steps; every rank takes the same number
+    # of steps
+    while t < t_first + W_max:
         b.do_tstp(t, args.tol)
+        t += 1
+        check(lib().nedy_split_tune_pending(C.byref(pending)))
+        if t >= t_first + Wb and dist.max(float(pending.value)) == 0:
+            break
     torch.cuda.synchronize()
     prep = time.time() - tp
-    T_win = list(range(t_first + Wb, t_first + Wb + Kb))
+    T_win = list(range(t, t + Kb))
     out = {}
     for mode, workers in (("batched", 16), ("one_at_a_time", 1)):
         b.set_workers(workers)
@@ -813,7 +825,8 @@ def run_batch(args, dist: Dist):
                        f"self-energy (two BF16 pieces), residual exit at tol={args.tol:g}",
            "batched": out["batched"], "one_at_a_time": out["one_at_a_time"],
            "speedup_batched": out["batched"]["timesteps_s"] / out["one_at_a_time"]["timesteps_s"],
-           "workers": 16, "preparation_s": prep,
+           "workers": 16, "preparation_s": prep, "warmup_steps": T_win[0] - 6,
+           "tuning_classes_pending": pending.value,
            "note": "the window is short (nt=500 of the configuration needs about 0.6 TB of Green's-function history)"}
     b.close()
     return res

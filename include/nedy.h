@@ -95,6 +95,9 @@ int nedy_split_stats(int on, double *pipe_flops, double *ms);
  * computes the same result.  The report lists classes, candidate times and choices. */
 int nedy_split_autotune(int on);
 int nedy_split_tune_report(char *buf, int len);
+/* *classes = problem classes still timing their candidates (0: every class has chosen;
+ * from then on no launch runs a trial shape).  No reference counterpart. */
+int nedy_split_tune_pending(int *classes);
 /* Work partition of the density-fitted self-energy for a workspace budget (bytes):
  * *chunk slices per chunk and *sub exchange units per launch, as the solver chooses them
  * (planning helper, no reference counterpart; host arithmetic, no device access).

@@ -80,6 +80,7 @@ SIGNATURES = {
     "nedy_sigma_chunk_plan": ([_I, _I, _LL, _I, _I, _I, C.POINTER(_I), C.POINTER(_I)], _I),
     "nedy_split_gemm_check": ([_I] * 17 + [C.c_ulonglong, C.POINTER(C.c_double)], _I),
     "nedy_split_tune_report": ([C.c_char_p, _I], _I),
+    "nedy_split_tune_pending": ([C.POINTER(C.c_int)], _I),
     "nedy_predictor_create": ([_P, _LL, C.c_ulonglong, _PP], _I),
     "nedy_predictor_destroy": ([_P], _I),
     "nedy_predictor_collect": ([_P, _P, _I, _I], _I),

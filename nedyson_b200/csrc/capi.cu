@@ -316,6 +316,13 @@ int nedy_split_autotune(int on) {
   return guard([&] { split_autotune(on != 0); });
 }
 
+int nedy_split_tune_pending(int *classes) {
+  return guard([&] {
+    NEDY_REQUIRE(classes, "null argument");
+    *classes = split_tune_pending();
+  });
+}
+
 int nedy_split_tune_report(char *buf, int len) {
   return guard([&] {
     NEDY_REQUIRE(buf && len > 0, "bad argument");

@@ -1562,6 +1562,16 @@ void split_autotune(bool on) {
   g_tune_on = on;
 }
 
+int split_tune_pending() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  int n = 0;
+  for (auto &kv : g_tune) {
+    poll(kv.second);
+    if (kv.second.chosen == -1) n++;
+  }
+  return n;
+}
+
 std::string split_tune_report() {
   std::string r;
   {

@@ -69,7 +69,7 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s);
 struct SplitCheck {
   int M = 0, N = 0, K = 0, nb = 1;
   int a_cplx = 1, b_cplx = 1, conjA = 0, conjB = 0, np = 3, out_pieces = 0, accumulate = 0;
-  int bn = 128, stages = 2, bk = 0, kdiv = 1, persist = 0;  // persist 1: persistent kernel, 2: CTA pair
+  int bn = 128, stages = 2, bk = 0, kdiv = 1, persist = 0;  // persist 1: persistent kernel, 2: CTA pair, 3: both
   double alpha = 1.0;
   unsigned long long seed = 1;
 };
@@ -84,6 +84,8 @@ void split_stats(bool on, double *flops, double *ms);
 // fastest.  split_tune_report lists the classes, candidate timings and choices.
 void split_autotune(bool on);
 std::string split_tune_report();
+// problem classes whose candidates are still being timed
+int split_tune_pending();
 
 // Error word of the split kernels launched on stream s: non-zero after a bounded wait gave
 // up (1 producer, 2 MMA issuer, 3 epilogue, 4 drain); reading a non-zero word clears it.
