@@ -112,7 +112,7 @@ int nedy_sigma_chunk_plan(int nao, int naux, long long budget, int precision, in
  * given instance: tile_n 64/128/256 output columns per CTA, stages, k_block 0 for the
  * per-product kernel or 32/64 for the one-load kernel, kdiv the K-split divisor, persistent
  * 1 the persistent one-load kernel (one CTA per SM over a tile list, two TMEM
- * accumulators; tile_n 128, out_pieces only), persistent 2 the CTA-pair one-load kernel
+ * accumulators; tile_n 64 or 128, out_pieces only), persistent 2 the CTA-pair one-load kernel
  * (clusters of two CTAs, 256-row tiles by tcgen05.mma.cta_group::2; complex x complex),
  * persistent 3 the persistent CTA-pair kernel (tile_n 128, out_pieces only).  *rel_err = max |C - C_fp64| / max |C_fp64|; NEDY_ERR_ARG for
  * an instance that does not exist or does not fit in shared memory. */

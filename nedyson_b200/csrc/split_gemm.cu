@@ -1512,6 +1512,14 @@ std::vector<Cand> candidates(int nA, int nB, int np, int N, bool acc, bool piece
       }
     }
   }
+  // persistent 64-wide tiles for narrow piece outputs: with K often one block, the loads and
+  // MMAs of one tile overlap the stores of the previous one only in the persistent kernel
+  if (pieces && N <= 64) {
+    for (int bk : {32, 64}) {
+      const int pst = std::min(bk == 32 ? 4 : 3, (P_SMEM_LIMIT - P_EPI_BYTES) / stage_bytes_for(nA, nB, np, 64, bk));
+      if (pst >= (bk == 32 ? 4 : 2)) c.push_back({64, pst, 1, bk, 1});
+    }
+  }
   // CTA pairs (complex x complex): 256-row tiles, each CTA staging half of B
   if (nA == 2 && nB == 2) {
     for (int bn : {128, 256}) {
@@ -1670,13 +1678,15 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
   if (g.force_bn > 0) {  // a given instance (the candidate checks of the test suite)
     NEDY_REQUIRE(g.force_bn == 64 || g.force_bn == 128 || g.force_bn == 256, "split_gemm: bad forced tile width");
     NEDY_REQUIRE(g.force_bk == 0 || g.force_bk == 32 || g.force_bk == 64, "split_gemm: bad forced K block");
-    NEDY_REQUIRE(g.force_bk == 0 || g.force_bn >= 128, "split_gemm: the one-load kernel has 128 or 256 wide tiles");
+    NEDY_REQUIRE(g.force_bk == 0 || g.force_bn >= 128 || (g.force_bn == 64 && g.force_persist && !g.force_pair),
+                 "split_gemm: the one-load kernel has 128 or 256 wide tiles (64 persistent)");
     NEDY_REQUIRE(g.force_stages >= 2 && g.force_stages <= 4 && g.force_kdiv >= 1, "split_gemm: bad forced stages");
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 64 || g.force_stages == 4 || g.force_stages == 2,
                  "split_gemm: 64-wide tiles use 2 or 4 stages");
     NEDY_REQUIRE(g.force_bk != 0 || g.force_bn != 256 || g.force_stages <= 3, "split_gemm: 256-wide tiles use <= 3 stages");
-    NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && g.force_bn == 128 && g.out_pieces),
-                 "split_gemm: the persistent kernel is the one-load kernel with 128-wide tiles and piece outputs");
+    NEDY_REQUIRE(!g.force_persist || (g.force_bk != 0 && (g.force_bn == 128 || (g.force_bn == 64 && !g.force_pair)) &&
+                                      g.out_pieces),
+                 "split_gemm: the persistent kernel is the one-load kernel with 64- or 128-wide tiles and piece outputs");
     NEDY_REQUIRE(!g.force_pair || (g.force_bk != 0 && (g.force_persist ? g.out_pieces : (ac && bc))),
                  "split_gemm: the pair kernels are one-load kernels (complex x complex, or persistent with piece outputs)");
     BNsel = g.force_bn;
@@ -1811,6 +1821,8 @@ void split_gemm(const SplitGemmArgs &g, cudaStream_t s) {
       {64, 128, 3, launch<128, 3, 64, true>, 0},
       {32, 128, 2, launch_persist<128, 2, 32>, 1}, {32, 128, 3, launch_persist<128, 3, 32>, 1},
       {32, 128, 4, launch_persist<128, 4, 32>, 1}, {64, 128, 2, launch_persist<128, 2, 64>, 1},
+      {32, 64, 4, launch_persist<64, 4, 32>, 1}, {64, 64, 2, launch_persist<64, 2, 64>, 1},
+      {64, 64, 3, launch_persist<64, 3, 64>, 1},
       {32, 256, 2, launch_pair<256, 2, 32>, 0, 1}, {32, 256, 3, launch_pair<256, 3, 32>, 0, 1},
       {32, 128, 2, launch_pair<128, 2, 32>, 0, 1}, {32, 128, 3, launch_pair<128, 3, 32>, 0, 1},
       {32, 128, 4, launch_pair<128, 4, 32>, 0, 1},

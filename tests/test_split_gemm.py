@@ -30,7 +30,8 @@ SHAPES = {
 }
 # (tile_n, stages, k_block, kdiv, persistent); k_block 0: per-product kernel, 32 / 64: one-load
 # kernel; persistent 1: the one-load kernel with one CTA per SM over a tile list and two TMEM
-# accumulators (the epilogue of one tile beside the MMAs of the next), BF16 piece outputs only;
+# accumulators (the epilogue of one tile beside the MMAs of the next; 64- or 128-wide tiles),
+# BF16 piece outputs only;
 # persistent 2: the CTA-pair one-load kernel (tcgen05.mma.cta_group::2, 256-row tiles over
 # two CTAs, each staging half of B), complex x complex products only; persistent 3: the
 # persistent CTA-pair kernel (clusters of two over a tile list, two accumulators per CTA),
@@ -42,7 +43,8 @@ INSTANCES = [(64, 4, 0, 1, 0), (64, 4, 0, 2, 0), (64, 4, 0, 4, 0), (64, 2, 0, 1,
              (128, 2, 32, 1, 1), (128, 3, 32, 1, 1), (128, 4, 32, 1, 1), (128, 2, 64, 1, 1), (128, 2, 32, 2, 1),
              (256, 2, 32, 1, 2), (256, 3, 32, 1, 2), (256, 3, 32, 2, 2), (128, 2, 32, 1, 2), (128, 3, 32, 1, 2),
              (128, 4, 32, 1, 2), (128, 2, 64, 1, 2),
-             (128, 3, 32, 1, 3), (128, 4, 32, 1, 3), (128, 2, 64, 1, 3), (128, 3, 64, 1, 3)]
+             (128, 3, 32, 1, 3), (128, 4, 32, 1, 3), (128, 2, 64, 1, 3), (128, 3, 64, 1, 3),
+             (64, 4, 32, 1, 1), (64, 2, 64, 1, 1), (64, 3, 64, 1, 1)]
 
 
 @pytest.mark.parametrize("np_", [2, 3])
