@@ -91,3 +91,17 @@ def test_new_entry_points_reject_bad_arguments(libpath):
     assert L.nedy_matsubara_gf2(None, 1, arr, arr, arr, arr, arr, 1.0, 10, 1e-12, None, None) == 1
     assert L.nedy_ctx_inject_split_error(None, 2) == 1
     assert L.nedy_dense_solve(None, 4, 1, 1, None, None) == 1
+
+
+def test_tuner_and_host_history_entry_points_without_gpu(libpath):
+    """The tuner's pending-classes query answers without a device (no class has run yet);
+    the host-history Green's function and its query reject null handles."""
+    import ctypes as C
+    from nedyson_b200 import _lib
+    L = _lib.lib()
+    n = C.c_int(-1)
+    assert L.nedy_split_tune_pending(C.byref(n)) == 0 and n.value == 0
+    assert L.nedy_split_tune_pending(None) == 1
+    out = C.c_void_p()
+    assert L.nedy_gf_create_host_history(None, 8, 4, 2, -1, C.byref(out)) == 1
+    assert L.nedy_gf_host_history(None, C.byref(n)) == 1
