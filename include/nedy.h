@@ -307,7 +307,11 @@ int nedy_ctx_predictor_stats(const nedy_ctx *ctx, int *active, long long *judged
 int nedy_decomp_spin_tstp_tol(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
                               nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
                               double mu_up, double mu_dn, int max_corr, double tol, int *iters, double *err_hist);
-/* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122). */
+/* Spin-unrestricted step (DecompSpinSimulation::do_tstp, src/molNEsim_decomp_spin_impl.h:97-122).
+ * In this and in nedy_decomp_spin_tstp_tol the two spins' Dyson steps run side by side: the
+ * second on a stream of the context's own (created on first use, with its own workspace)
+ * from a short-lived helper thread; the call returns once both are done, and the context's
+ * stream is ordered after both. */
 int nedy_decomp_spin_tstp(nedy_ctx *ctx, int tstp, nedy_gf *G_up, nedy_gf *G_dn, nedy_gf *S_up, nedy_gf *S_dn,
                           nedy_buf *hmf_up, nedy_buf *hmf_dn, const nedy_buf *h_t_up, const nedy_buf *h_t_dn,
                           double mu_up, double mu_dn, int corr_steps, double *err);
