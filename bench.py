@@ -1008,7 +1008,9 @@ def main():
         # units of the step (les, tv and ret slices times the iterations)
         units = sum(nsp * (2 * (t + 1) + args.ntau + 1) * it for t, it in zip(r["T"], head["iters"])) / K
         per_unit = SPLIT_TRAFFIC_PER_UNIT if (args.nao, args.naux, args.split_mode) == (64, 256, "bf16x2") else None
-        line["roofline"] = {"bound": "tensor", "kernel": "split_gemm_kernel (BF16 piece products, tcgen05, TMEM)",
+        line["roofline"] = {"bound": "tensor", "kernel": "split GEMM kernels: split_gemm_kernel, split_gemm_persist_kernel, "
+                            "split_gemm_pair_kernel, split_gemm_persist_pair_kernel (BF16 piece products, "
+                            "tcgen05, TMEM; every launch of the step)",
                             "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
                             "frac": (ach / bf16_peak) if ach else None,
                             "traffic": per_unit * units if per_unit else None,
